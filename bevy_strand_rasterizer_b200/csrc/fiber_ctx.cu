@@ -1,0 +1,998 @@
+// fiber_ctx.cu — host runtime behind the C ABI (include/fiber.h).
+//
+// Mirrors the reference's plugin plumbing: slab allocation and the page
+// tables of bevy_gpu_paging_allocator (src/plugin.rs:1395-1440, 129-160), the
+// per-frame host preparation of use_prepass_buffers (src/plugin.rs:264-1209:
+// frustum table, capacities, queue resets), and the render-graph node order
+// (prepass -> shadows -> shading -> raster -> composite, src/plugin.rs:240-260).
+// Device counts never travel back to the host inside a frame: every stage
+// reads its item count from device memory, so a whole frame is one stream of
+// launches that can be replayed from a CUDA graph.
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "fiber_kernels.cuh"
+
+using namespace fiber;
+
+namespace {
+
+constexpr int kSpanCount = 14;
+const char* kSpanNames[kSpanCount] = {
+    "strand_prepass/broad_instances",     // broad + depth-warp LUT
+    "strand_prepass/fine",
+    "strand_prepass/mark_count_pages",
+    "strand_prepass/allocate_count_pages",
+    "strand_prepass/binning",              // count
+    "strand_prepass/prefix_fine_pages",
+    "strand_prepass/fill_segment_refs",
+    "strand_prepass/compact_active_tiles",
+    "strand_prepass/emit_raster_work",     // emit + canonical cell order
+    "strand_shadow_rasterizer/rasterize",  // incl. fused stampback
+    "strand_shading/shade",
+    "strand_rasterizer/rasterize",
+    "strand_composite/composite",
+    "frame/total",
+};
+
+struct Slab {
+    void* ptr = nullptr;
+    uint64_t bytes = 0;
+    bool live = false;
+};
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+};
+
+int kind_slot(uint32_t kind) {
+    switch (kind) {
+        case FIBER_SLAB_VERT: return 0;
+        case FIBER_SLAB_INDEX: return 1;
+        case FIBER_SLAB_MATERIAL: return 2;
+        case FIBER_SLAB_GEO: return 3;
+        case FIBER_SLAB_META: return 4;
+        default: return -1;
+    }
+}
+
+// Checks one instance's slabs on the device: every index < vertex count, every
+// strand range inside the index slab, every material index inside the material
+// slab (validate_cache, src/strand_cache.rs:174-209). out: [errors, segments
+// lo, segments hi, max count].
+__global__ void k_validate(InstanceView v, uint32_t* out) {
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+    for (uint32_t j = tid; j < v.n_indices; j += stride)
+        if (v.indices[j] >= v.n_vertices) atomicOr(out + 0, 1u);
+    unsigned long long segs = 0;
+    uint32_t maxc = 0;
+    for (uint32_t s = tid; s < v.n_meta; s += stride) {
+        fiber_strand_meta m = v.meta[s];
+        if (m.count < 2u) continue;
+        if ((uint64_t)m.offset + m.count > v.n_indices) atomicOr(out + 0, 2u);
+        if (m.material_idx >= v.n_materials) atomicOr(out + 0, 4u);
+        segs += m.count - 1u;
+        maxc = max(maxc, m.count);
+    }
+    atomicAdd(reinterpret_cast<unsigned long long*>(out + 1), segs);
+    atomicMax(out + 3, maxc);
+}
+
+}  // namespace
+
+struct fiber_ctx {
+    int device = 0;
+    uint64_t budget = 0, allocated = 0;
+    int sm_count = 148;
+    fiber_settings settings{};
+    std::vector<Slab> slabs[5];
+    // registered instances
+    std::vector<fiber_strand_instance> rows;
+    std::vector<InstanceView> views;
+    std::vector<uint64_t> inst_segments;
+    uint64_t total_segments = 0, total_points = 0, total_strands = 0;
+    uint32_t max_texels = 0, total_strand_count = 0, max_strand_count = 0;
+    // frame description
+    FrameParams P{};
+    std::vector<fiber_frustum_desc> frusta;
+    bool frame_ready = false;
+    uint32_t epoch = 0;
+    uint32_t lb_offset[kStageCount] = {0};
+    // device buffers
+    DevBuf d_params, d_inst, d_counters, d_lb, d_range_valid, d_ranges, d_keep, d_inst_visible, d_inst_keep;
+    DevBuf d_lut, d_tasks, d_projected, d_page_table, d_page_meta, d_counts, d_offsets, d_cursors;
+    DevBuf d_refs, d_ref_keys, d_active_flags, d_active_list, d_work, d_runs, d_big_cells;
+    DevBuf d_dom_depth, d_dom_opacity, d_shadow_map, d_atlas, d_history[2];
+    DevBuf d_color, d_depth, d_fragments, d_validate;
+    int hist_cur = 0;
+    // timing
+    cudaEvent_t ev[kSpanCount + 1] = {};
+    bool events_ok = false;
+    cudaStream_t last_stream = nullptr;
+    // graph replay of fiber_frame_fused
+    cudaGraphExec_t graph = nullptr;
+    uint64_t graph_key[8] = {0};
+    uint64_t buffer_generation = 0, graph_generation = ~0ull;
+    FrameCounters h_counters{};
+};
+
+namespace {
+
+#define FIBER_CUDA(expr)                                         \
+    do {                                                         \
+        cudaError_t _e = (expr);                                 \
+        if (_e != cudaSuccess) return FIBER_ECUDA;               \
+    } while (0)
+
+fiber_status ensure(fiber_ctx* c, DevBuf& b, size_t bytes, bool zero = false) {
+    if (bytes == 0) bytes = 16;
+    bytes = (bytes + 255) & ~size_t(255);
+    if (b.p && b.bytes >= bytes) return FIBER_OK;
+    if (c->budget && c->allocated - b.bytes + bytes > c->budget) return FIBER_ENOMEM;
+    if (b.p) {
+        cudaFree(b.p);
+        c->allocated -= b.bytes;
+        b.p = nullptr;
+        b.bytes = 0;
+    }
+    if (cudaMalloc(&b.p, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return FIBER_ENOMEM;
+    }
+    b.bytes = bytes;
+    c->allocated += bytes;
+    c->buffer_generation++;
+    if (zero) FIBER_CUDA(cudaMemset(b.p, 0, bytes));
+    return FIBER_OK;
+}
+
+void release(fiber_ctx* c, DevBuf& b) {
+    if (b.p) {
+        cudaFree(b.p);
+        c->allocated -= b.bytes;
+    }
+    b.p = nullptr;
+    b.bytes = 0;
+}
+
+template <typename T>
+T* dp(const DevBuf& b) { return static_cast<T*>(b.p); }
+
+void cfg_tiles(const fiber_froxel_config& cfg, uint32_t& tx, uint32_t& ty) {
+    tx = (cfg.screen_width + cfg.froxel_size_x - 1u) / cfg.froxel_size_x;
+    ty = (cfg.screen_height + cfg.froxel_size_y - 1u) / cfg.froxel_size_y;
+}
+
+LaunchCtx launch_ctx(fiber_ctx* c, cudaStream_t s) {
+    LaunchCtx L;
+    L.stream = s;
+    L.P = dp<FrameParams>(c->d_params);
+    L.inst = dp<InstanceView>(c->d_inst);
+    L.I = c->P.I;
+    L.total_coarse_tiles = c->P.total_coarse_tiles;
+    L.sm_count = c->sm_count;
+    return L;
+}
+
+PrepassArgs prepass_args(fiber_ctx* c) {
+    PrepassArgs A{};
+    A.counters = dp<FrameCounters>(c->d_counters);
+    A.range_valid = dp<uint32_t>(c->d_range_valid);
+    A.ranges = dp<fiber_coarse_asset_range>(c->d_ranges);
+    A.keep = dp<float>(c->d_keep);
+    A.inst_visible = dp<uint32_t>(c->d_inst_visible);
+    A.inst_keep = dp<float>(c->d_inst_keep);
+    A.lut = dp<fiber_coarse_depth_lut_entry>(c->d_lut);
+    A.tasks = dp<fiber_binning_task>(c->d_tasks);
+    A.projected = dp<fiber_projected_segment>(c->d_projected);
+    A.page_table = dp<uint32_t>(c->d_page_table);
+    A.page_meta = dp<fiber_fine_page_meta>(c->d_page_meta);
+    A.counts = dp<uint32_t>(c->d_counts);
+    A.offsets = dp<uint32_t>(c->d_offsets);
+    A.cursors = dp<uint32_t>(c->d_cursors);
+    A.refs = dp<fiber_fine_seg_ref>(c->d_refs);
+    A.ref_keys = dp<uint32_t>(c->d_ref_keys);
+    A.active_flags = dp<uint32_t>(c->d_active_flags);
+    A.active_list = dp<uint32_t>(c->d_active_list);
+    A.work = dp<fiber_raster_work_item>(c->d_work);
+    A.runs = dp<fiber_raster_tile_run>(c->d_runs);
+    A.big_cells = dp<uint2>(c->d_big_cells);
+    return A;
+}
+
+void set_stage(fiber_ctx* c, PrepassArgs& A, uint32_t stage) {
+    A.tile_counter = &dp<FrameCounters>(c->d_counters)->tile_counter[stage];
+    A.lb_status = dp<unsigned long long>(c->d_lb) + c->lb_offset[stage];
+}
+
+RenderArgs render_args(fiber_ctx* c) {
+    RenderArgs R{};
+    R.counters = dp<FrameCounters>(c->d_counters);
+    R.tasks = dp<fiber_binning_task>(c->d_tasks);
+    R.refs = dp<fiber_fine_seg_ref>(c->d_refs);
+    R.work = dp<fiber_raster_work_item>(c->d_work);
+    R.runs = dp<fiber_raster_tile_run>(c->d_runs);
+    R.dom_depth = dp<float>(c->d_dom_depth);
+    R.dom_opacity = dp<float>(c->d_dom_opacity);
+    R.shadow_map = dp<float>(c->d_shadow_map);
+    R.atlas = dp<__half>(c->d_atlas);
+    R.history[0] = dp<__half>(c->d_history[0]);
+    R.history[1] = dp<__half>(c->d_history[1]);
+    R.color = dp<__half>(c->d_color);
+    R.depth = dp<float>(c->d_depth);
+    R.fragments = dp<uint32_t>(c->d_fragments);
+    return R;
+}
+
+void record(fiber_ctx* c, int span, cudaStream_t s) {
+    if (c->events_ok) cudaEventRecord(c->ev[span], s);
+}
+
+fiber_status check_launch() {
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? FIBER_OK : FIBER_ECUDA;
+}
+
+fiber_status run_prepass(fiber_ctx* c, cudaStream_t s) {
+    LaunchCtx L = launch_ctx(c, s);
+    PrepassArgs A = prepass_args(c);
+    record(c, 0, s);
+    launch_broad(L, A);
+    launch_lut(L, A);
+    record(c, 1, s);
+    set_stage(c, A, kStageFine);
+    launch_fine(L, A);
+    record(c, 2, s);
+    launch_mark(L, A);
+    record(c, 3, s);
+    set_stage(c, A, kStageAlloc);
+    launch_alloc(L, A);
+    launch_zero_pages(L, A);
+    record(c, 4, s);
+    launch_count(L, A);
+    record(c, 5, s);
+    set_stage(c, A, kStagePrefix);
+    launch_prefix(L, A);
+    record(c, 6, s);
+    launch_fill(L, A);
+    record(c, 7, s);
+    set_stage(c, A, kStageActive);
+    launch_compact_active(L, A);
+    record(c, 8, s);
+    set_stage(c, A, kStageEmit);
+    launch_emit(L, A);
+    launch_sort_big(L, A);
+    return check_launch();
+}
+
+fiber_status run_shadows(fiber_ctx* c, cudaStream_t s) {
+    record(c, 9, s);
+    if (c->P.L) launch_shadow(launch_ctx(c, s), render_args(c));
+    return check_launch();
+}
+
+fiber_status run_shading(fiber_ctx* c, cudaStream_t s) {
+    record(c, 10, s);
+    launch_shade(launch_ctx(c, s), render_args(c));
+    c->hist_cur = 1 - c->hist_cur;  // shadow-history ping-pong flip (pipelines/shading.rs:564-566)
+    return check_launch();
+}
+
+fiber_status run_raster(fiber_ctx* c, cudaStream_t s) {
+    record(c, 11, s);
+    launch_raster(launch_ctx(c, s), render_args(c));
+    return check_launch();
+}
+
+uint32_t fmt_bytes(uint32_t fmt) {
+    return fmt == FIBER_FMT_RGBA16F ? 8u : (fmt == FIBER_FMT_R32F ? 4u : 16u);
+}
+
+fiber_status run_composite(fiber_ctx* c, const fiber_image* scene_color, const fiber_image* scene_depth,
+                           fiber_image* out, cudaStream_t s) {
+    record(c, 12, s);
+    if (!scene_color || !out || !scene_color->ptr || !out->ptr) return FIBER_EINVAL;
+    if (scene_color->width != c->P.width || scene_color->height != c->P.height || out->width != c->P.width ||
+        out->height != c->P.height)
+        return FIBER_EINVAL;
+    if (scene_color->format == FIBER_FMT_R32F || out->format == FIBER_FMT_R32F) return FIBER_EINVAL;
+    if (scene_depth && (scene_depth->format != FIBER_FMT_R32F || scene_depth->width != c->P.width ||
+                        scene_depth->height != c->P.height))
+        return FIBER_EINVAL;
+    CompositeArgs C{};
+    C.strand_color = dp<__half>(c->d_color);
+    C.strand_depth = dp<float>(c->d_depth);
+    C.scene_color = scene_color->ptr;
+    C.scene_pitch = scene_color->pitch ? scene_color->pitch : scene_color->width * fmt_bytes(scene_color->format);
+    C.scene_format = scene_color->format;
+    C.scene_depth = scene_depth ? static_cast<const float*>(scene_depth->ptr) : nullptr;
+    C.depth_pitch = scene_depth ? (scene_depth->pitch ? scene_depth->pitch : scene_depth->width * 4u) : 0u;
+    C.out = out->ptr;
+    C.out_pitch = out->pitch ? out->pitch : out->width * fmt_bytes(out->format);
+    C.out_format = out->format;
+    C.width = c->P.width;
+    C.height = c->P.height;
+    launch_composite(s, C);
+    return check_launch();
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+const char* fiber_status_string(fiber_status s) {
+    switch (s) {
+        case FIBER_OK: return "ok";
+        case FIBER_EINVAL: return "invalid argument";
+        case FIBER_ENOMEM: return "out of device memory or HBM budget";
+        case FIBER_EOVERFLOW: return "device queue overflow";
+        case FIBER_ETIMEDOUT: return "bounded device wait timed out";
+        case FIBER_ECUDA: return "CUDA runtime error";
+        case FIBER_ENOTREADY: return "inputs not ready";
+        default: return "unknown";
+    }
+}
+
+fiber_status fiber_settings_default(fiber_settings* s) {
+    if (!s) return FIBER_EINVAL;
+    std::memset(s, 0, sizeof(*s));
+    s->stochastic_cull_enabled = 1u;          // StochasticCullSettings::default (src/resources.rs:95-104)
+    s->target_strands_per_pixel = 2.0f;
+    s->min_keep_probability = 0.02f;
+    s->shadow_keep_probability = 1.0f;
+    s->telemetry_enabled = 0u;
+    s->fine_binning_backend = 0u;             // SegmentScatter
+    s->dom_slices = 12u;                      // NUM_DOM_SLICES (src/pipelines/shadows.rs:38)
+    s->shadow_map_size = 0u;
+    s->ambient_color[0] = s->ambient_color[1] = s->ambient_color[2] = 80.0f;  // AmbientLight default x brightness
+    s->ambient_color[3] = 80.0f;
+    s->history_enabled = 1u;
+    s->fragment_counts_enabled = 0u;
+    s->ref_capacity_factor = 4u;              // fine refs = 4 x binning (src/plugin.rs:536-540)
+    s->page_capacity_divisor = 1u;
+    return FIBER_OK;
+}
+
+fiber_status fiber_ctx_create(int device, uint64_t hbm_budget, fiber_ctx** out) {
+    if (!out) return FIBER_EINVAL;
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || device < 0 || device >= n) {
+        cudaGetLastError();
+        return FIBER_EINVAL;
+    }
+    FIBER_CUDA(cudaSetDevice(device));
+    fiber_ctx* c = new fiber_ctx();
+    c->device = device;
+    c->budget = hbm_budget;
+    cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device);
+    fiber_settings_default(&c->settings);
+    c->events_ok = true;
+    for (int i = 0; i <= kSpanCount; ++i)
+        if (cudaEventCreate(&c->ev[i]) != cudaSuccess) c->events_ok = false;
+    fiber_status st = ensure(c, c->d_counters, sizeof(FrameCounters), true);
+    if (st == FIBER_OK) st = ensure(c, c->d_validate, 64, true);
+    if (st != FIBER_OK) {
+        fiber_ctx_destroy(c);
+        return st;
+    }
+    *out = c;
+    return FIBER_OK;
+}
+
+fiber_status fiber_ctx_destroy(fiber_ctx* c) {
+    if (!c) return FIBER_EINVAL;
+    cudaSetDevice(c->device);
+    cudaDeviceSynchronize();
+    if (c->graph) cudaGraphExecDestroy(c->graph);
+    for (auto& v : c->slabs)
+        for (auto& s : v)
+            if (s.live && s.ptr) cudaFree(s.ptr);
+    DevBuf* bufs[] = {&c->d_params, &c->d_inst, &c->d_counters, &c->d_lb, &c->d_range_valid, &c->d_ranges,
+                      &c->d_keep, &c->d_inst_visible, &c->d_inst_keep, &c->d_lut, &c->d_tasks, &c->d_projected,
+                      &c->d_page_table, &c->d_page_meta, &c->d_counts, &c->d_offsets, &c->d_cursors, &c->d_refs,
+                      &c->d_ref_keys, &c->d_active_flags, &c->d_active_list, &c->d_work, &c->d_runs,
+                      &c->d_big_cells, &c->d_dom_depth, &c->d_dom_opacity, &c->d_shadow_map, &c->d_atlas,
+                      &c->d_history[0], &c->d_history[1], &c->d_color, &c->d_depth, &c->d_fragments,
+                      &c->d_validate};
+    for (DevBuf* b : bufs) release(c, *b);
+    for (int i = 0; i <= kSpanCount; ++i)
+        if (c->ev[i]) cudaEventDestroy(c->ev[i]);
+    delete c;
+    return FIBER_OK;
+}
+
+fiber_status fiber_settings_set(fiber_ctx* c, const fiber_settings* s) {
+    if (!c || !s) return FIBER_EINVAL;
+    if (s->dom_slices == 0u || s->dom_slices > 16u) return FIBER_EINVAL;
+    if (s->ref_capacity_factor == 0u || s->page_capacity_divisor == 0u) return FIBER_EINVAL;
+    if (s->fine_binning_backend != 0u) return FIBER_EINVAL;  // only SegmentScatter is built
+    c->settings = *s;
+    c->frame_ready = false;
+    return FIBER_OK;
+}
+
+fiber_status fiber_slab_alloc(fiber_ctx* c, uint32_t kind, uint64_t bytes, uint32_t* alloc_id, fiber_devptr* out) {
+    if (!c || !alloc_id || bytes == 0 || bytes > 0xFFFFFFFFull) return FIBER_EINVAL;
+    int k = kind_slot(kind);
+    if (k < 0) return FIBER_EINVAL;
+    if (kind == FIBER_SLAB_VERT && bytes % 16u) return FIBER_EINVAL;  // float4 vertex stride
+    if (c->budget && c->allocated + bytes > c->budget) return FIBER_ENOMEM;
+    cudaSetDevice(c->device);
+    Slab s;
+    if (cudaMalloc(&s.ptr, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return FIBER_ENOMEM;
+    }
+    s.bytes = bytes;
+    s.live = true;
+    c->allocated += bytes;
+    c->slabs[k].push_back(s);
+    *alloc_id = (uint32_t)(c->slabs[k].size() - 1);
+    if (out) *out = fiber_devptr{*alloc_id, 0u, (uint32_t)bytes};
+    return FIBER_OK;
+}
+
+fiber_status fiber_slab_upload(fiber_ctx* c, uint32_t kind, uint32_t alloc_id, uint64_t dst_offset, const void* host,
+                               uint64_t bytes, void* stream) {
+    if (!c || !host) return FIBER_EINVAL;
+    int k = kind_slot(kind);
+    if (k < 0 || alloc_id >= c->slabs[k].size() || !c->slabs[k][alloc_id].live) return FIBER_EINVAL;
+    const Slab& s = c->slabs[k][alloc_id];
+    if (dst_offset + bytes > s.bytes) return FIBER_EINVAL;
+    cudaSetDevice(c->device);
+    FIBER_CUDA(cudaMemcpyAsync(static_cast<char*>(s.ptr) + dst_offset, host, bytes, cudaMemcpyHostToDevice,
+                               (cudaStream_t)stream));
+    return FIBER_OK;
+}
+
+fiber_status fiber_slab_free(fiber_ctx* c, uint32_t kind, uint32_t alloc_id) {
+    if (!c) return FIBER_EINVAL;
+    int k = kind_slot(kind);
+    if (k < 0 || alloc_id >= c->slabs[k].size() || !c->slabs[k][alloc_id].live) return FIBER_EINVAL;
+    cudaSetDevice(c->device);
+    cudaDeviceSynchronize();
+    Slab& s = c->slabs[k][alloc_id];
+    cudaFree(s.ptr);
+    c->allocated -= s.bytes;
+    s = Slab{};
+    c->frame_ready = false;
+    return FIBER_OK;
+}
+
+fiber_status fiber_instance_set(fiber_ctx* c, const fiber_strand_instance* rows, uint32_t n) {
+    if (!c || (n && !rows)) return FIBER_EINVAL;
+    if (n >= 32768u) return FIBER_EINVAL;  // instance ids are 15 bits in the cell sort key
+    cudaSetDevice(c->device);
+    FIBER_CUDA(cudaDeviceSynchronize());
+    std::vector<InstanceView> views(n);
+    std::vector<uint64_t> segs(n, 0);
+    uint64_t tot_seg = 0, tot_pts = 0, tot_str = 0;
+    uint32_t max_tex = 0, strand_base = 0, max_strands = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+        const fiber_strand_instance& r = rows[i];
+        InstanceView& v = views[i];
+        std::memset(&v, 0, sizeof(v));
+        auto get = [&](uint32_t kind, uint32_t id) -> const Slab* {
+            int k = kind_slot(kind);
+            if (id >= c->slabs[k].size() || !c->slabs[k][id].live) return nullptr;
+            return &c->slabs[k][id];
+        };
+        const Slab *sv = get(FIBER_SLAB_VERT, r.vertex_id), *si = get(FIBER_SLAB_INDEX, r.index_id);
+        const Slab *sm = get(FIBER_SLAB_META, r.meta_id), *sg = get(FIBER_SLAB_GEO, r.geo_id);
+        const Slab* sa = get(FIBER_SLAB_MATERIAL, r.material_id);
+        if (!sv || !si || !sm || !sg || !sa || sg->bytes < sizeof(fiber_strand_geo) ||
+            sa->bytes < sizeof(fiber_strand_material))
+            return FIBER_EINVAL;
+        fiber_strand_geo geo;
+        FIBER_CUDA(cudaMemcpy(&geo, sg->ptr, sizeof(geo), cudaMemcpyDeviceToHost));
+        v.vertices = static_cast<const float4*>(sv->ptr);
+        v.indices = static_cast<const uint32_t*>(si->ptr);
+        v.meta = static_cast<const fiber_strand_meta*>(sm->ptr);
+        v.materials = static_cast<const fiber_strand_material*>(sa->ptr);
+        v.n_vertices = (uint32_t)(sv->bytes / 16u);
+        v.n_indices = (uint32_t)(si->bytes / 4u);
+        v.n_meta = (uint32_t)(sm->bytes / sizeof(fiber_strand_meta));
+        v.n_materials = (uint32_t)(sa->bytes / sizeof(fiber_strand_material));
+        v.strand_count = std::min(v.n_meta, geo.strand_count);
+        v.strand_base = strand_base;
+        v.valid = 1u;
+        v.aabb = geo.aabb;
+        std::memcpy(v.world_from_local, r.world_from_local, sizeof(v.world_from_local));
+        // Device-side validation.
+        FIBER_CUDA(cudaMemset(c->d_validate.p, 0, 16));
+        k_validate<<<std::max(1, c->sm_count * 2), 256>>>(v, dp<uint32_t>(c->d_validate));
+        uint32_t res[4];
+        FIBER_CUDA(cudaMemcpy(res, c->d_validate.p, 16, cudaMemcpyDeviceToHost));
+        if (res[0] != 0u) return FIBER_EINVAL;
+        segs[i] = (uint64_t)res[1] | ((uint64_t)res[2] << 32);
+        tot_seg += segs[i];
+        tot_pts += v.n_indices;
+        tot_str += v.strand_count;
+        strand_base += v.strand_count;
+        max_strands = std::max(max_strands, v.strand_count);
+        max_tex = std::max(max_tex, v.n_indices);
+    }
+    if (tot_str >= 0xFFFFFFFFull || tot_seg >= 0x3FFFFFFFull) return FIBER_EINVAL;
+    c->rows.assign(rows, rows + n);
+    c->views = views;
+    c->inst_segments = segs;
+    c->total_segments = tot_seg;
+    c->total_points = tot_pts;
+    c->total_strands = tot_str;
+    c->total_strand_count = strand_base;
+    c->max_strand_count = max_strands;
+    c->max_texels = max_tex;
+    c->frame_ready = false;
+    return FIBER_OK;
+}
+
+fiber_status fiber_frame_begin(fiber_ctx* c, const fiber_froxel_config* cam_cfg, const fiber_camera* cam,
+                               const fiber_froxel_config* light_cfgs, const fiber_light* lights, uint32_t n_lights,
+                               void* stream_) {
+    if (!c || !cam_cfg || !cam || (n_lights && (!light_cfgs || !lights))) return FIBER_EINVAL;
+    if (1u + n_lights > kMaxFrusta) return FIBER_EINVAL;
+    cudaStream_t s = (cudaStream_t)stream_;
+    cudaSetDevice(c->device);
+    auto cfg_ok = [](const fiber_froxel_config& g) {
+        return g.screen_width && g.screen_height && g.froxel_size_x && g.froxel_size_y && g.screen_width <= 16384u &&
+               g.screen_height <= 16384u;
+    };
+    if (!cfg_ok(*cam_cfg)) return FIBER_EINVAL;
+    for (uint32_t l = 0; l < n_lights; ++l) {
+        if (!cfg_ok(light_cfgs[l])) return FIBER_EINVAL;
+        // Dense deep-opacity layers: every light map is square and the same size.
+        if (light_cfgs[l].screen_width != light_cfgs[l].screen_height ||
+            light_cfgs[l].screen_width != light_cfgs[0].screen_width)
+            return FIBER_EINVAL;
+    }
+    const fiber_settings& st = c->settings;
+    FrameParams& P = c->P;
+    std::memset(&P, 0, sizeof(P));
+    // Frustum table (src/plugin.rs:386-482): camera first, then lights.
+    c->frusta.clear();
+    uint32_t bucket = 0, coarse = 0, fine = 0, cam_tiles = 0;
+    for (uint32_t f = 0; f < 1u + n_lights; ++f) {
+        const fiber_froxel_config& g = f == 0 ? *cam_cfg : light_cfgs[f - 1];
+        uint32_t tx, ty;
+        cfg_tiles(g, tx, ty);
+        uint32_t ctx_ = std::max(1u, (tx + 3u) / 4u), cty = std::max(1u, (ty + 3u) / 4u);
+        fiber_frustum_desc d{};
+        d.screen_width = g.screen_width;
+        d.screen_height = g.screen_height;
+        d.froxel_size_x = g.froxel_size_x;
+        d.froxel_size_y = g.froxel_size_y;
+        d.depth_slices = g.depth_slices;
+        d.bucket_base = bucket;
+        d.bucket_count = tx * ty * g.depth_slices;
+        d.kind = f == 0 ? 0u : 1u;
+        d.coarse_depth_tile_base = coarse;
+        d.coarse_depth_tile_count = ctx_ * cty;
+        d.coarse_tiles_x = ctx_;
+        d.coarse_tiles_y = cty;
+        d.cascade_index = 0u;
+        d.fine_depth_tile_base = fine;
+        c->frusta.push_back(d);
+        bucket += d.bucket_count;
+        coarse += d.coarse_depth_tile_count;
+        fine += tx * ty;
+        if (f == 0) cam_tiles = coarse;
+        P.frusta[f] = d;
+        std::memcpy(P.clip[f], f == 0 ? cam->clip_from_world : lights[f - 1].clip_from_world, 64);
+    }
+    for (uint32_t l = 0; l < n_lights; ++l) {
+        std::memcpy(P.light_dir[l], lights[l].direction_to_light, 12);
+        std::memcpy(P.light_color[l], lights[l].color, 16);
+    }
+    std::memcpy(P.camera_pos, cam->world_position, 12);
+    std::memcpy(P.ambient, st.ambient_color, 16);
+    const uint32_t I = (uint32_t)c->views.size();
+    P.F = 1u + n_lights;
+    P.I = I;
+    P.L = n_lights;
+    P.K = st.dom_slices;
+    P.total_coarse_tiles = coarse;
+    P.total_strands = c->total_strand_count;
+    P.max_strands = c->max_strand_count;
+    P.camera_frustum_end = 1u;
+    P.camera_tile_end = cam_tiles;
+    P.dom_size = n_lights ? light_cfgs[0].screen_width : 0u;
+    P.shadow_map_size = n_lights ? (st.shadow_map_size ? st.shadow_map_size : P.dom_size) : 0u;
+    // Shading atlas dims (create_shading_target_texture, src/pipelines/shading.rs:410-438).
+    uint32_t aw = std::min(std::max(c->max_texels, 1u), 8192u);
+    uint32_t ah = std::min(std::max((c->max_texels + aw - 1u) / aw, 1u), 8192u);
+    P.atlas_cap = aw * ah;
+    // Capacities (src/plugin.rs:483-576): prepass = next_pow2(strands) >= 2048,
+    // binning = next_pow2(next_pow2(segments) >= prepass, x frusta), refs =
+    // next_pow2(factor x binning). Pages and work items are sized so that only
+    // the reference list can overflow.
+    auto next_pow2 = [](uint64_t x) {
+        uint64_t p = 1;
+        while (p < x) p <<= 1;
+        return p;
+    };
+    const uint64_t table = (uint64_t)coarse * kDepthSlices;
+    const uint64_t prepass_cap = std::max<uint64_t>(next_pow2(c->total_strands), 2048);
+    const uint64_t base_binning = std::max<uint64_t>(next_pow2(c->total_segments), prepass_cap);
+    const uint64_t task_cap = std::max<uint64_t>(next_pow2(base_binning * P.F), base_binning);
+    const uint64_t page_cap = std::max<uint64_t>(1, table / st.page_capacity_divisor);
+    const uint64_t ref_cap = std::max<uint64_t>(next_pow2(task_cap * st.ref_capacity_factor), std::max<uint64_t>(task_cap, 1024));
+    const uint64_t fine_tiles = table;  // coarse tiles x 16 fine tiles
+    const uint64_t work_cap = std::max<uint64_t>(1, std::min<uint64_t>(ref_cap, 256ull * fine_tiles));
+    if (ref_cap >= 0xFFFFFFFFull || work_cap >= 0xFFFFFFFFull) return FIBER_ENOMEM;
+    P.task_capacity = (uint32_t)task_cap;
+    P.page_capacity = (uint32_t)page_cap;
+    P.ref_capacity = (uint32_t)ref_cap;
+    P.work_capacity = (uint32_t)work_cap;
+    P.stochastic_cull_enabled = st.stochastic_cull_enabled;
+    P.target_strands_per_pixel = st.target_strands_per_pixel;
+    P.min_keep_probability = st.min_keep_probability;
+    P.shadow_keep_probability = st.shadow_keep_probability;
+    P.history_valid = st.history_enabled ? 1u : 0u;
+    P.fragment_counts = st.fragment_counts_enabled;
+    P.width = cam_cfg->screen_width;
+    P.height = cam_cfg->screen_height;
+    // Look-back status regions.
+    uint64_t fine_tiles_lb = (uint64_t)P.F * ((P.total_strands + 7u) / 8u);
+    uint64_t lb_sizes[kStageCount] = {fine_tiles_lb + 1, table / 1024 + 2, page_cap + 1, table / 1024 + 2,
+                                      fine_tiles + 1};
+    uint64_t lb_total = 0;
+    for (int i = 0; i < kStageCount; ++i) {
+        c->lb_offset[i] = (uint32_t)lb_total;
+        lb_total += lb_sizes[i];
+    }
+    const uint64_t W = P.width, H = P.height, L = n_lights, D = P.dom_size, S = P.shadow_map_size, K = P.K;
+    const uint64_t FI = (uint64_t)I * P.F;
+    fiber_status e = FIBER_OK;
+#define ENSURE(buf, bytes, zero)                     \
+    do {                                             \
+        e = ensure(c, buf, (size_t)(bytes), zero);   \
+        if (e != FIBER_OK) return e;                 \
+    } while (0)
+    bool lb_new = !c->d_lb.p || c->d_lb.bytes < lb_total * 8;
+    ENSURE(c->d_params, sizeof(FrameParams), false);
+    ENSURE(c->d_inst, std::max<uint64_t>(1, I) * sizeof(InstanceView), false);
+    ENSURE(c->d_lb, lb_total * 8, true);
+    if (lb_new) c->epoch = 0;
+    ENSURE(c->d_range_valid, FI * 4, false);
+    ENSURE(c->d_ranges, FI * sizeof(fiber_coarse_asset_range), false);
+    ENSURE(c->d_keep, FI * 4, false);
+    ENSURE(c->d_inst_visible, (uint64_t)I * 4, false);
+    ENSURE(c->d_inst_keep, (uint64_t)I * 4, false);
+    ENSURE(c->d_lut, table * sizeof(fiber_coarse_depth_lut_entry), false);
+    ENSURE(c->d_tasks, task_cap * sizeof(fiber_binning_task), false);
+    ENSURE(c->d_projected, task_cap * sizeof(fiber_projected_segment), false);
+    ENSURE(c->d_page_table, table * 4, false);
+    ENSURE(c->d_page_meta, page_cap * sizeof(fiber_fine_page_meta), false);
+    ENSURE(c->d_counts, page_cap * kPageSize * 4, false);
+    ENSURE(c->d_offsets, page_cap * kPageSize * 4, false);
+    ENSURE(c->d_cursors, page_cap * kPageSize * 4, false);
+    ENSURE(c->d_refs, ref_cap * sizeof(fiber_fine_seg_ref), false);
+    ENSURE(c->d_ref_keys, ref_cap * 4, false);
+    ENSURE(c->d_active_flags, fine_tiles * 4, false);
+    ENSURE(c->d_active_list, fine_tiles * 4, false);
+    ENSURE(c->d_work, work_cap * sizeof(fiber_raster_work_item), false);
+    ENSURE(c->d_runs, fine_tiles * sizeof(fiber_raster_tile_run), false);
+    ENSURE(c->d_big_cells, (ref_cap / 33 + 1) * sizeof(uint2), false);
+    ENSURE(c->d_dom_depth, L * D * D * 4, false);
+    ENSURE(c->d_dom_opacity, L * K * D * D * 4, true);
+    ENSURE(c->d_shadow_map, L * S * S * 4, false);
+    const uint64_t atlas_texels = (uint64_t)std::max(I, 1u) * P.atlas_cap;
+    bool hist_new = !c->d_history[0].p || c->d_history[0].bytes < atlas_texels * 4;
+    ENSURE(c->d_atlas, atlas_texels * 8, true);
+    ENSURE(c->d_history[0], atlas_texels * 4, true);
+    ENSURE(c->d_history[1], atlas_texels * 4, true);
+    if (hist_new) {
+        // History is cleared on reallocation (src/pipelines/shading.rs:509-525).
+        cudaMemsetAsync(c->d_history[0].p, 0, c->d_history[0].bytes, s);
+        cudaMemsetAsync(c->d_history[1].p, 0, c->d_history[1].bytes, s);
+        c->hist_cur = 0;
+    }
+    ENSURE(c->d_color, W * H * 8, false);
+    ENSURE(c->d_depth, W * H * 4, false);
+    ENSURE(c->d_fragments, W * H * 4, false);
+#undef ENSURE
+    c->epoch = (c->epoch + 1u) & 0x3FFFFFFFu;
+    if (c->epoch == 0u) {  // epoch wrapped: old words could alias, clear them
+        cudaMemsetAsync(c->d_lb.p, 0, c->d_lb.bytes, s);
+        c->epoch = 1u;
+    }
+    P.epoch = c->epoch;
+    P.hist_in = (uint32_t)c->hist_cur;
+    // Per-frame uploads and resets (src/plugin.rs:1145-1208).
+    FIBER_CUDA(cudaMemcpyAsync(c->d_params.p, &P, sizeof(P), cudaMemcpyHostToDevice, s));
+    if (I) FIBER_CUDA(cudaMemcpyAsync(c->d_inst.p, c->views.data(), I * sizeof(InstanceView), cudaMemcpyHostToDevice, s));
+    FIBER_CUDA(cudaMemsetAsync(c->d_counters.p, 0, sizeof(FrameCounters), s));
+    FIBER_CUDA(cudaMemsetAsync(c->d_page_table.p, 0, table * 4, s));
+    FIBER_CUDA(cudaMemsetAsync(c->d_active_flags.p, 0, fine_tiles * 4, s));
+    FIBER_CUDA(cudaMemsetAsync(c->d_color.p, 0, W * H * 8, s));
+    FIBER_CUDA(cudaMemsetAsync(c->d_depth.p, 0, W * H * 4, s));
+    if (P.fragment_counts) FIBER_CUDA(cudaMemsetAsync(c->d_fragments.p, 0, W * H * 4, s));
+    if (L) {
+        FIBER_CUDA(cudaMemsetAsync(c->d_dom_depth.p, 0, L * D * D * 4, s));
+        FIBER_CUDA(cudaMemsetAsync(c->d_shadow_map.p, 0, L * S * S * 4, s));
+    }
+    c->last_stream = s;
+    c->frame_ready = true;
+    return FIBER_OK;
+}
+
+fiber_status fiber_prepass(fiber_ctx* c, void* stream) {
+    if (!c) return FIBER_EINVAL;
+    if (!c->frame_ready) return FIBER_ENOTREADY;
+    cudaSetDevice(c->device);
+    c->last_stream = (cudaStream_t)stream;
+    return run_prepass(c, (cudaStream_t)stream);
+}
+
+fiber_status fiber_shadows(fiber_ctx* c, void* stream) {
+    if (!c) return FIBER_EINVAL;
+    if (!c->frame_ready) return FIBER_ENOTREADY;
+    cudaSetDevice(c->device);
+    c->last_stream = (cudaStream_t)stream;
+    return run_shadows(c, (cudaStream_t)stream);
+}
+
+fiber_status fiber_shading(fiber_ctx* c, void* stream) {
+    if (!c) return FIBER_EINVAL;
+    if (!c->frame_ready) return FIBER_ENOTREADY;
+    cudaSetDevice(c->device);
+    c->last_stream = (cudaStream_t)stream;
+    return run_shading(c, (cudaStream_t)stream);
+}
+
+fiber_status fiber_raster(fiber_ctx* c, uint32_t view, void* stream) {
+    if (!c || view != 0u) return FIBER_EINVAL;
+    if (!c->frame_ready) return FIBER_ENOTREADY;
+    cudaSetDevice(c->device);
+    c->last_stream = (cudaStream_t)stream;
+    return run_raster(c, (cudaStream_t)stream);
+}
+
+fiber_status fiber_composite(fiber_ctx* c, uint32_t view, const fiber_image* scene_color,
+                             const fiber_image* scene_depth, fiber_image* out, void* stream) {
+    if (!c || view != 0u) return FIBER_EINVAL;
+    if (!c->frame_ready) return FIBER_ENOTREADY;
+    cudaSetDevice(c->device);
+    c->last_stream = (cudaStream_t)stream;
+    fiber_status st = run_composite(c, scene_color, scene_depth, out, (cudaStream_t)stream);
+    record(c, 13, (cudaStream_t)stream);
+    return st;
+}
+
+fiber_status fiber_frame_fused(fiber_ctx* c, const fiber_image* scene_color, const fiber_image* scene_depth,
+                               fiber_image* out, void* stream_) {
+    if (!c) return FIBER_EINVAL;
+    if (!c->frame_ready) return FIBER_ENOTREADY;
+    cudaSetDevice(c->device);
+    cudaStream_t s = (cudaStream_t)stream_;
+    c->last_stream = s;
+    const bool composite = scene_color && out;
+    if (!s) {  // the legacy stream cannot be captured: run the nodes directly
+        fiber_status st = run_prepass(c, s);
+        if (st == FIBER_OK) st = run_shadows(c, s);
+        if (st == FIBER_OK) st = run_shading(c, s);
+        if (st == FIBER_OK) st = run_raster(c, s);
+        if (st == FIBER_OK && composite) st = run_composite(c, scene_color, scene_depth, out, s);
+        record(c, 13, s);
+        return st;
+    }
+    // Every kernel argument is stable across frames (per-frame values live in
+    // the device FrameParams), so one captured graph serves every frame of the
+    // same shape and buffers.
+    uint64_t key[8] = {c->buffer_generation, (uint64_t)(composite ? 1 : 0),
+                       (uint64_t)(uintptr_t)(scene_color ? scene_color->ptr : nullptr),
+                       (uint64_t)(uintptr_t)(scene_depth ? scene_depth->ptr : nullptr),
+                       (uint64_t)(uintptr_t)(out ? out->ptr : nullptr), (uint64_t)(uintptr_t)s,
+                       (uint64_t)(composite ? scene_color->format : 0), (uint64_t)(composite ? out->format : 0)};
+    bool reuse = c->graph && std::memcmp(key, c->graph_key, sizeof(key)) == 0;
+    if (!reuse) {
+        if (c->graph) {
+            cudaGraphExecDestroy(c->graph);
+            c->graph = nullptr;
+        }
+        cudaGraph_t g = nullptr;
+        FIBER_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        const int hist_before = c->hist_cur;
+        fiber_status st = run_prepass(c, s);
+        if (st == FIBER_OK) st = run_shadows(c, s);
+        if (st == FIBER_OK) st = run_shading(c, s);
+        if (st == FIBER_OK) st = run_raster(c, s);
+        if (st == FIBER_OK && composite) st = run_composite(c, scene_color, scene_depth, out, s);
+        record(c, 13, s);
+        cudaError_t ce = cudaStreamEndCapture(s, &g);
+        if (st != FIBER_OK || ce != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            c->hist_cur = hist_before;
+            return st != FIBER_OK ? st : FIBER_ECUDA;
+        }
+        ce = cudaGraphInstantiate(&c->graph, g, 0);
+        cudaGraphDestroy(g);
+        if (ce != cudaSuccess) return FIBER_ECUDA;
+        std::memcpy(c->graph_key, key, sizeof(key));
+        c->hist_cur = hist_before;
+    }
+    FIBER_CUDA(cudaGraphLaunch(c->graph, s));
+    c->hist_cur = 1 - c->hist_cur;
+    return FIBER_OK;
+}
+
+fiber_status fiber_stats_get(fiber_ctx* c, fiber_stats* out) {
+    if (!c || !out) return FIBER_EINVAL;
+    cudaSetDevice(c->device);
+    FIBER_CUDA(cudaStreamSynchronize(c->last_stream));
+    FrameCounters h{};
+    FIBER_CUDA(cudaMemcpy(&h, c->d_counters.p, sizeof(h), cudaMemcpyDeviceToHost));
+    c->h_counters = h;
+    std::memset(out, 0, sizeof(*out));
+    out->frustum_count = c->P.F;
+    out->instance_count = c->P.I;
+    out->binning_tasks = std::min(h.tasks, c->P.task_capacity);
+    out->camera_tasks = h.frustum_task_base[c->P.camera_frustum_end];
+    out->allocated_pages = h.pages;
+    std::vector<fiber_fine_page_meta> pm(h.pages);
+    if (h.pages) FIBER_CUDA(cudaMemcpy(pm.data(), c->d_page_meta.p, h.pages * sizeof(fiber_fine_page_meta), cudaMemcpyDeviceToHost));
+    uint64_t refs = 0;
+    for (const auto& m : pm) {
+        refs += m.seg_ref_count;
+        uint32_t f = 0;
+        for (; f < c->P.F; ++f)
+            if (m.coarse_tile_id >= c->P.frusta[f].coarse_depth_tile_base &&
+                m.coarse_tile_id < c->P.frusta[f].coarse_depth_tile_base + c->P.frusta[f].coarse_depth_tile_count)
+                break;
+        if (f < 8) {
+            out->frustum_pages[f]++;
+            out->frustum_refs[f] += m.seg_ref_count;
+        }
+    }
+    out->fine_refs = (uint32_t)refs;
+    out->active_tiles = h.active_tiles;
+    out->camera_runs = h.camera_active;
+    out->shadow_runs = h.active_tiles - h.camera_active;
+    out->work_items = h.work_items;
+    out->overflow_flags = h.overflow;
+    out->timeout_flags = h.error;
+    for (uint32_t f = 0; f < c->P.F && f < 8; ++f) out->frustum_tasks[f] = h.frustum_task_base[f + 1] - h.frustum_task_base[f];
+    std::vector<fiber_raster_tile_run> runs(h.active_tiles);
+    if (h.active_tiles)
+        FIBER_CUDA(cudaMemcpy(runs.data(), c->d_runs.p, h.active_tiles * sizeof(fiber_raster_tile_run), cudaMemcpyDeviceToHost));
+    for (const auto& r : runs)
+        if (r.frustum_id < 8) {
+            out->frustum_work[r.frustum_id] += r.work_count;
+            out->frustum_runs[r.frustum_id]++;
+        }
+    out->total_segments = c->total_segments;
+    out->total_points = c->total_points;
+    out->total_strands = c->total_strands;
+    if (h.error) return FIBER_ETIMEDOUT;
+    if (h.overflow) return FIBER_EOVERFLOW;
+    return FIBER_OK;
+}
+
+fiber_status fiber_dump(fiber_ctx* c, uint32_t what, void* host, uint64_t capacity, uint64_t* written) {
+    if (!c) return FIBER_EINVAL;
+    cudaSetDevice(c->device);
+    FIBER_CUDA(cudaStreamSynchronize(c->last_stream));
+    FrameCounters h{};
+    FIBER_CUDA(cudaMemcpy(&h, c->d_counters.p, sizeof(h), cudaMemcpyDeviceToHost));
+    const FrameParams& P = c->P;
+    const uint64_t table = (uint64_t)P.total_coarse_tiles * kDepthSlices;
+    const uint64_t W = P.width, H = P.height, L = P.L, D = P.dom_size, S = P.shadow_map_size, K = P.K;
+    const void* src = nullptr;
+    uint64_t bytes = 0;
+    std::vector<uint32_t> tmp;
+    switch (what) {
+        case FIBER_DUMP_FRUSTA:
+            if (written) *written = c->frusta.size() * sizeof(fiber_frustum_desc);
+            if (host && capacity >= c->frusta.size() * sizeof(fiber_frustum_desc))
+                std::memcpy(host, c->frusta.data(), c->frusta.size() * sizeof(fiber_frustum_desc));
+            return FIBER_OK;
+        case FIBER_DUMP_RANGES: {
+            uint64_t n = (uint64_t)P.I * P.F;
+            std::vector<uint32_t> valid(n);
+            std::vector<fiber_coarse_asset_range> r(n);
+            if (n) {
+                FIBER_CUDA(cudaMemcpy(valid.data(), c->d_range_valid.p, n * 4, cudaMemcpyDeviceToHost));
+                FIBER_CUDA(cudaMemcpy(r.data(), c->d_ranges.p, n * sizeof(fiber_coarse_asset_range), cudaMemcpyDeviceToHost));
+            }
+            for (uint64_t i = 0; i < n; ++i) {
+                tmp.push_back(valid[i]);
+                const uint32_t* w = reinterpret_cast<const uint32_t*>(&r[i]);
+                if (valid[i]) tmp.insert(tmp.end(), w, w + 8);
+                else tmp.insert(tmp.end(), 8, 0u);
+            }
+            if (written) *written = tmp.size() * 4;
+            if (host && capacity >= tmp.size() * 4) std::memcpy(host, tmp.data(), tmp.size() * 4);
+            return FIBER_OK;
+        }
+        case FIBER_DUMP_KEEP: src = c->d_keep.p; bytes = (uint64_t)P.I * P.F * 4; break;
+        case FIBER_DUMP_LUT: src = c->d_lut.p; bytes = table * sizeof(fiber_coarse_depth_lut_entry); break;
+        case FIBER_DUMP_TASKS: src = c->d_tasks.p; bytes = (uint64_t)std::min(h.tasks, P.task_capacity) * 16; break;
+        case FIBER_DUMP_PROJECTED: src = c->d_projected.p; bytes = (uint64_t)std::min(h.tasks, P.task_capacity) * 12; break;
+        case FIBER_DUMP_PAGE_TABLE: src = c->d_page_table.p; bytes = table * 4; break;
+        case FIBER_DUMP_PAGE_META: src = c->d_page_meta.p; bytes = (uint64_t)h.pages * 32; break;
+        case FIBER_DUMP_COUNTS: src = c->d_counts.p; bytes = (uint64_t)h.pages * kPageSize * 4; break;
+        case FIBER_DUMP_OFFSETS: src = c->d_offsets.p; bytes = (uint64_t)h.pages * kPageSize * 4; break;
+        case FIBER_DUMP_REFS: src = c->d_refs.p; bytes = (uint64_t)std::min(h.refs, P.ref_capacity) * 12; break;
+        case FIBER_DUMP_ACTIVE_TILES: src = c->d_active_list.p; bytes = (uint64_t)h.active_tiles * 4; break;
+        case FIBER_DUMP_WORK: src = c->d_work.p; bytes = (uint64_t)std::min(h.work_items, P.work_capacity) * 32; break;
+        case FIBER_DUMP_RUNS: src = c->d_runs.p; bytes = (uint64_t)h.active_tiles * 32; break;
+        case FIBER_DUMP_DOM_DEPTH: src = c->d_dom_depth.p; bytes = L * D * D * 4; break;
+        case FIBER_DUMP_DOM_OPACITY: {
+            // Canonical form: opacity of texels without a depth (never written
+            // this frame) reads as 0.
+            std::vector<float> dep(L * D * D), op(L * K * D * D);
+            if (!op.empty()) {
+                FIBER_CUDA(cudaMemcpy(dep.data(), c->d_dom_depth.p, dep.size() * 4, cudaMemcpyDeviceToHost));
+                FIBER_CUDA(cudaMemcpy(op.data(), c->d_dom_opacity.p, op.size() * 4, cudaMemcpyDeviceToHost));
+                for (uint64_t l = 0; l < L; ++l)
+                    for (uint64_t k = 0; k < K; ++k)
+                        for (uint64_t p = 0; p < D * D; ++p)
+                            if (dep[l * D * D + p] == 0.0f) op[(l * K + k) * D * D + p] = 0.0f;
+            }
+            if (written) *written = op.size() * 4;
+            if (host && capacity >= op.size() * 4) std::memcpy(host, op.data(), op.size() * 4);
+            return FIBER_OK;
+        }
+        case FIBER_DUMP_SHADOW_MAP: src = c->d_shadow_map.p; bytes = L * S * S * 4; break;
+        case FIBER_DUMP_ATLAS: src = c->d_atlas.p; bytes = (uint64_t)P.I * P.atlas_cap * 8; break;
+        case FIBER_DUMP_HISTORY: src = c->d_history[c->hist_cur].p; bytes = (uint64_t)P.I * P.atlas_cap * 4; break;
+        case FIBER_DUMP_COLOR: src = c->d_color.p; bytes = W * H * 8; break;
+        case FIBER_DUMP_DEPTH: src = c->d_depth.p; bytes = W * H * 4; break;
+        case FIBER_DUMP_FRAGMENTS: src = c->d_fragments.p; bytes = W * H * 4; break;
+        default: return FIBER_EINVAL;
+    }
+    if (written) *written = bytes;
+    if (host && bytes) {
+        if (capacity < bytes) return FIBER_EINVAL;
+        FIBER_CUDA(cudaMemcpy(host, src, bytes, cudaMemcpyDeviceToHost));
+    }
+    return FIBER_OK;
+}
+
+fiber_status fiber_output_image(fiber_ctx* c, uint32_t what, fiber_image* out) {
+    if (!c || !out) return FIBER_EINVAL;
+    const FrameParams& P = c->P;
+    switch (what) {
+        case FIBER_DUMP_COLOR: *out = fiber_image{c->d_color.p, P.width, P.height, P.width * 8u, FIBER_FMT_RGBA16F}; break;
+        case FIBER_DUMP_DEPTH: *out = fiber_image{c->d_depth.p, P.width, P.height, P.width * 4u, FIBER_FMT_R32F}; break;
+        case FIBER_DUMP_DOM_DEPTH: *out = fiber_image{c->d_dom_depth.p, P.dom_size, P.dom_size * P.L, P.dom_size * 4u, FIBER_FMT_R32F}; break;
+        case FIBER_DUMP_DOM_OPACITY:
+            *out = fiber_image{c->d_dom_opacity.p, P.dom_size, P.dom_size * P.L * P.K, P.dom_size * 4u, FIBER_FMT_R32F};
+            break;
+        case FIBER_DUMP_SHADOW_MAP:
+            *out = fiber_image{c->d_shadow_map.p, P.shadow_map_size, P.shadow_map_size * P.L, P.shadow_map_size * 4u, FIBER_FMT_R32F};
+            break;
+        default: return FIBER_EINVAL;
+    }
+    return FIBER_OK;
+}
+
+uint32_t fiber_span_count(void) { return kSpanCount; }
+const char* fiber_span_name(uint32_t i) { return i < (uint32_t)kSpanCount ? kSpanNames[i] : ""; }
+
+fiber_status fiber_span_times(fiber_ctx* c, float* ms, uint32_t n) {
+    if (!c || !ms) return FIBER_EINVAL;
+    if (!c->events_ok) return FIBER_ENOTREADY;
+    cudaSetDevice(c->device);
+    FIBER_CUDA(cudaStreamSynchronize(c->last_stream));
+    for (uint32_t i = 0; i < n && i < (uint32_t)kSpanCount; ++i) {
+        float t = 0.0f;
+        if (i + 1 < (uint32_t)kSpanCount) {
+            if (cudaEventElapsedTime(&t, c->ev[i], c->ev[i + 1]) != cudaSuccess) { cudaGetLastError(); t = -1.0f; }
+        } else {
+            if (cudaEventElapsedTime(&t, c->ev[0], c->ev[13]) != cudaSuccess) { cudaGetLastError(); t = -1.0f; }
+        }
+        ms[i] = t;
+    }
+    return FIBER_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,278 @@
+// fiber_device.cuh — device-side building blocks of the strand raster path.
+//
+// Arithmetic follows the WGSL semantics of the reference shaders
+// (src/shaders/common.wgsl, strand_prepass.wgsl, strand_rasterizer.wgsl):
+// the library is compiled with --fmad=false and IEEE div/sqrt, so every
+// + - * / sqrt here is one correctly rounded binary32 operation in source
+// order and matrix-vector products are c0*x + c1*y + c2*z + c3*w left to
+// right. Float-to-integer conversions saturate like WGSL's.
+#pragma once
+
+#include <cuda/atomic>
+#include <stdint.h>
+
+#include "../../include/fiber.h"
+
+namespace fiber {
+
+constexpr uint32_t kCoarseExtent = 4;      // COARSE_FINE_TILE_EXTENT (src/plugin.rs:58)
+constexpr uint32_t kDepthSlices = 16;      // COARSE_DEPTH_SLICES (src/plugin.rs:59)
+constexpr uint32_t kPageSize = 256;        // COARSE_COUNT_PAGE_SIZE (src/plugin.rs:61)
+constexpr uint32_t kDepthQuantMax = 16777215u;
+constexpr uint32_t kInvalid = 0xFFFFFFFFu;
+constexpr uint32_t kMarked = 0xFFFFFFFEu;  // MARKED_COUNT_PAGE (strand_prepass.wgsl:69)
+constexpr uint32_t kMaxFrusta = 16;
+constexpr uint32_t kPixelSlots = 64;       // strand_rasterizer.wgsl:309,839
+
+// Error words written by device code (never trap).
+constexpr uint32_t kErrTimeout = 1u;
+
+// ---------------------------------------------------------------------------
+// Per-instance view resolved on the host once per frame from the slab tables.
+// ---------------------------------------------------------------------------
+struct InstanceView {
+    const float4* vertices;
+    const uint32_t* indices;
+    const fiber_strand_meta* meta;
+    const fiber_strand_material* materials;
+    uint32_t n_vertices, n_indices, n_meta, n_materials;
+    uint32_t strand_count;       // min(meta count, geo.strand_count)
+    uint32_t strand_base;        // prefix of strand_count over instances
+    uint32_t valid;              // all slab pointers resolved
+    uint32_t pad;
+    fiber_aabb aabb;
+    float world_from_local[16];
+};
+
+// Constant frame description shared by every kernel of a frame.
+struct FrameParams {
+    fiber_frustum_desc frusta[kMaxFrusta];
+    float clip[kMaxFrusta][16];
+    float light_dir[kMaxFrusta][4];
+    float light_color[kMaxFrusta][4];
+    float camera_pos[4];
+    float ambient[4];
+    uint32_t F, I, L, K;
+    uint32_t total_coarse_tiles;
+    uint32_t total_strands;       // sum of instance strand counts
+    uint32_t max_strands;         // max strand count of one instance
+    uint32_t camera_frustum_end;  // frusta [0, end) are cameras
+    uint32_t camera_tile_end;     // coarse tiles of camera frusta
+    uint32_t dom_size;            // D
+    uint32_t shadow_map_size;     // S
+    uint32_t atlas_cap;           // texels per instance layer
+    uint32_t task_capacity, page_capacity, ref_capacity, work_capacity;
+    uint32_t stochastic_cull_enabled;
+    float target_strands_per_pixel, min_keep_probability, shadow_keep_probability;
+    uint32_t history_valid;       // previous history holds a frame
+    uint32_t fragment_counts;     // count fragments per pixel
+    uint32_t width, height;       // camera resolution
+    uint32_t epoch;               // look-back status epoch of this frame
+    uint32_t hist_in;             // shadow-history buffer read this frame (0/1)
+};
+
+// Device counters of one frame (zeroed at frame start).
+struct FrameCounters {
+    uint32_t tasks;               // binning tasks written
+    uint32_t frustum_task_base[kMaxFrusta + 1];
+    uint32_t pages;               // allocated pages (<= capacity)
+    uint32_t refs;                // seg_ref tail (may exceed capacity)
+    uint32_t active_tiles;
+    uint32_t camera_active;       // active tiles that belong to camera frusta
+    uint32_t work_items;
+    uint32_t runs;
+    uint32_t overflow;            // bit0 tasks, bit1 pages, bit2 refs, bit3 work
+    uint32_t error;               // kErrTimeout when a bounded wait gave up
+    uint32_t big_cells;           // cells queued for the large-cell sort
+    uint32_t tile_counter[8];     // virtual block ids of the look-back stages
+    uint32_t pad[5];
+};
+
+// Look-back stages (index into FrameCounters::tile_counter and the status regions).
+enum LookbackStage : uint32_t { kStageFine = 0, kStageAlloc = 1, kStagePrefix = 2, kStageActive = 3, kStageEmit = 4, kStageCount = 5 };
+
+// ---------------------------------------------------------------------------
+// WGSL builtin semantics
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float wmin(float a, float b) { return fminf(a, b); }
+__device__ __forceinline__ float wmax(float a, float b) { return fmaxf(a, b); }
+__device__ __forceinline__ float wclamp(float e, float lo, float hi) { return fminf(fmaxf(e, lo), hi); }
+__device__ __forceinline__ int32_t iclamp(int32_t e, int32_t lo, int32_t hi) { return min(max(e, lo), hi); }
+__device__ __forceinline__ float wmix(float a, float b, float t) { return __fadd_rn(__fmul_rn(a, __fsub_rn(1.0f, t)), __fmul_rn(b, t)); }
+__device__ __forceinline__ uint32_t f2u(float f) { return __float2uint_rz(f); }   // saturating, NaN -> 0
+__device__ __forceinline__ int32_t f2i(float f) { return __float2int_rz(f); }     // saturating, NaN -> 0
+__device__ __forceinline__ float u2f(uint32_t u) { return __uint2float_rn(u); }
+__device__ __forceinline__ uint32_t ceil_div(uint32_t x, uint32_t y) { return (x + y - 1u) / y; }
+
+struct F3 { float x, y, z; };
+__device__ __forceinline__ F3 f3(float x, float y, float z) { return F3{x, y, z}; }
+
+__device__ __forceinline__ float4 matvec(const float* m, float x, float y, float z, float w) {
+    float4 r;
+    r.x = ((m[0] * x + m[4] * y) + m[8] * z) + m[12] * w;
+    r.y = ((m[1] * x + m[5] * y) + m[9] * z) + m[13] * w;
+    r.z = ((m[2] * x + m[6] * y) + m[10] * z) + m[14] * w;
+    r.w = ((m[3] * x + m[7] * y) + m[11] * z) + m[15] * w;
+    return r;
+}
+
+// common.wgsl:206-212
+__device__ __forceinline__ float normalize_depth01(float z) {
+    if (z >= 0.0f && z <= 1.0f) return z;
+    return wclamp(z * 0.5f + 0.5f, 0.0f, 1.0f);
+}
+// common.wgsl:93-107 -> (sx, sy, ndc z, clip w)
+__device__ __forceinline__ float4 world_to_screen_raw(float4 p, const float* clip, float vw, float vh) {
+    float4 c = matvec(clip, p.x, p.y, p.z, p.w);
+    if (c.w <= 0.0f) return make_float4(-1.0f, -1.0f, -1.0f, -1.0f);
+    float nx = c.x / c.w, ny = c.y / c.w, nz = c.z / c.w;
+    float sx = 0.0f + (nx * 0.5f + 0.5f) * vw;
+    float sy = 0.0f + (ny * -0.5f + 0.5f) * vh;
+    return make_float4(sx, sy, nz, c.w);
+}
+// common.wgsl:229-242
+__device__ __forceinline__ uint32_t wang_hash(uint32_t x) {
+    x = (x ^ 61u) ^ (x >> 16u);
+    x = x + (x << 3u);
+    x = x ^ (x >> 4u);
+    x = x * 0x27d4eb2du;
+    x = x ^ (x >> 15u);
+    return x;
+}
+__device__ __forceinline__ float hash_to_unit_float(uint32_t x) { return u2f(x) / 4294967296.0f; }
+// strand_prepass.wgsl:533-539 (WGSL round = half to even)
+__device__ __forceinline__ uint32_t quantize_depth01(float z) {
+    return f2u(rintf(wclamp(z, 0.0f, 1.0f) * (float)kDepthQuantMax));
+}
+__device__ __forceinline__ float dequantize_depth01(uint32_t q) { return u2f(q) / (float)kDepthQuantMax; }
+// WGSL pack2x16unorm: floor(0.5 + 65535 * clamp(e, 0, 1)), x in the low half.
+__device__ __forceinline__ uint32_t unorm16(float e) {
+    float t = 65535.0f * fminf(1.0f, fmaxf(0.0f, e));
+    return f2u(floorf(0.5f + t));
+}
+__device__ __forceinline__ uint32_t pack2x16unorm(float a, float b) { return unorm16(a) | (unorm16(b) << 16u); }
+__device__ __forceinline__ float2 unpack2x16unorm(uint32_t p) {
+    return make_float2(u2f(p & 0xFFFFu) / 65535.0f, u2f(p >> 16u) / 65535.0f);
+}
+__device__ __forceinline__ int32_t sgn_i32(float f) {
+    if (f > 1e-6f) return 1;
+    if (f < -1e-6f) return -1;
+    return 0;
+}
+
+// clip_axis_to_range / clip_segment_to_box (strand_prepass.wgsl:1356-1410)
+__device__ __forceinline__ bool clip_axis(float p, float d, float mn, float mx, float& tmin, float& tmax) {
+    if (fabsf(d) < 1e-6f) return !(p < mn || p > mx);
+    float inv_d = 1.0f / d;
+    float a = (mn - p) * inv_d;
+    float b = (mx - p) * inv_d;
+    if (a > b) { float t = a; a = b; b = t; }
+    tmin = wmax(tmin, a);
+    tmax = wmin(tmax, b);
+    return !(tmin > tmax);
+}
+__device__ __forceinline__ bool clip_segment(F3 p0, F3 p1, F3 bmin, F3 bmax, F3& o0, F3& o1) {
+    F3 d = f3(p1.x - p0.x, p1.y - p0.y, p1.z - p0.z);
+    float tmin = 0.0f, tmax = 1.0f;
+    if (!clip_axis(p0.x, d.x, bmin.x, bmax.x, tmin, tmax)) return false;
+    if (!clip_axis(p0.y, d.y, bmin.y, bmax.y, tmin, tmax)) return false;
+    if (!clip_axis(p0.z, d.z, bmin.z, bmax.z, tmin, tmax)) return false;
+    o0 = f3(p0.x + d.x * tmin, p0.y + d.y * tmin, p0.z + d.z * tmin);
+    o1 = f3(p0.x + d.x * tmax, p0.y + d.y * tmax, p0.z + d.z * tmax);
+    return true;
+}
+
+__device__ __forceinline__ uint32_t frustum_for_tile(const FrameParams& P, uint32_t tile) {
+    for (uint32_t f = 0; f < P.F; ++f) {
+        const fiber_frustum_desc& d = P.frusta[f];
+        if (tile >= d.coarse_depth_tile_base && tile < d.coarse_depth_tile_base + d.coarse_depth_tile_count) return f;
+    }
+    return kInvalid;
+}
+__device__ __forceinline__ uint32_t light_layer(const FrameParams& P, uint32_t f) {
+    if (f >= P.F || P.frusta[f].kind != 1u) return kInvalid;
+    uint32_t layer = 0;
+    for (uint32_t i = 0; i < f; ++i)
+        if (P.frusta[i].kind == 1u) ++layer;
+    return layer >= P.L ? kInvalid : layer;
+}
+
+// ---------------------------------------------------------------------------
+// Decoupled look-back (single-pass chained scan, Merrill & Garland 2016).
+// status[t] = (epoch << 2 | flag) << 32 | value; flag 1 = block aggregate,
+// 2 = inclusive prefix. Words stamped with another frame's epoch read as "not
+// ready", so the status arrays are never cleared between frames. Every wait is
+// bounded: after kSpinLimit polls the block records kErrTimeout and proceeds
+// with what it has, so a broken chain cannot hang the GPU.
+// ---------------------------------------------------------------------------
+constexpr uint32_t kSpinLimit = 1u << 22;
+
+__device__ __forceinline__ void lb_publish(unsigned long long* status, uint32_t tile, uint32_t epoch, uint32_t flag,
+                                           uint32_t value) {
+    cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> a(status[tile]);
+    a.store(((unsigned long long)((epoch << 2) | flag) << 32) | value, cuda::memory_order_release);
+}
+
+// Called by one thread. Returns the exclusive prefix of `tile`.
+__device__ __forceinline__ uint32_t lb_exclusive(unsigned long long* status, uint32_t tile, uint32_t epoch,
+                                                 uint32_t aggregate, uint32_t* error) {
+    if (tile == 0) {
+        lb_publish(status, 0, epoch, 2u, aggregate);
+        return 0u;
+    }
+    lb_publish(status, tile, epoch, 1u, aggregate);
+    uint32_t excl = 0;
+    int64_t pred = (int64_t)tile - 1;
+    uint32_t spins = 0;
+    while (pred >= 0) {
+        cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> a(status[pred]);
+        unsigned long long v = a.load(cuda::memory_order_acquire);
+        uint32_t hi = (uint32_t)(v >> 32);
+        uint32_t flag = (hi >> 2) == (epoch & 0x3FFFFFFFu) ? (hi & 3u) : 0u;
+        if (flag == 0u) {
+            if (++spins > kSpinLimit) {
+                atomicOr(error, kErrTimeout);
+                break;
+            }
+            __nanosleep(32);
+            continue;
+        }
+        excl += (uint32_t)v;
+        if (flag == 2u) break;
+        --pred;
+    }
+    lb_publish(status, tile, epoch, 2u, excl + aggregate);
+    return excl;
+}
+
+// Block-wide exclusive scan of one value per thread (blockDim multiple of 32).
+template <int kThreads>
+__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* smem_warp, uint32_t& total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) smem_warp[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t w = lane < kThreads / 32 ? smem_warp[lane] : 0u;
+        uint32_t s = w;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t y = __shfl_up_sync(0xFFFFFFFFu, s, o);
+            if (lane >= o) s += y;
+        }
+        if (lane < kThreads / 32) smem_warp[lane] = s - w;
+        if (lane == kThreads / 32 - 1) smem_warp[32] = s;
+    }
+    __syncthreads();
+    uint32_t r = smem_warp[warp] + x - v;
+    total = smem_warp[32];
+    __syncthreads();
+    return r;
+}
+
+}  // namespace fiber

@@ -1,0 +1,95 @@
+// fiber_kernels.cuh — kernel argument blocks and launch entry points.
+#pragma once
+
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include "fiber_device.cuh"
+
+namespace fiber {
+
+inline unsigned ceil_div_host(uint64_t x, uint64_t y) { return (unsigned)((x + y - 1) / y); }
+
+// Device buffers of the work-preparation stages.
+struct PrepassArgs {
+    uint32_t* tile_counter;          // virtual block ids of the current look-back stage
+    unsigned long long* lb_status;   // look-back status words of the current stage
+    FrameCounters* counters;
+    uint32_t* range_valid;           // [I * F]
+    fiber_coarse_asset_range* ranges;
+    float* keep;                     // [I * F]
+    uint32_t* inst_visible;          // [I]
+    float* inst_keep;                // [I] max(camera, shadow) keep probability
+    fiber_coarse_depth_lut_entry* lut;
+    fiber_binning_task* tasks;
+    fiber_projected_segment* projected;
+    uint32_t* page_table;
+    fiber_fine_page_meta* page_meta;
+    uint32_t* counts;
+    uint32_t* offsets;
+    uint32_t* cursors;
+    fiber_fine_seg_ref* refs;
+    uint32_t* ref_keys;
+    uint32_t* active_flags;
+    uint32_t* active_list;
+    fiber_raster_work_item* work;
+    fiber_raster_tile_run* runs;
+    uint2* big_cells;
+};
+
+// Device buffers of the shadow, shading, raster and composite stages.
+struct RenderArgs {
+    FrameCounters* counters;
+    const fiber_binning_task* tasks;
+    const fiber_fine_seg_ref* refs;
+    const fiber_raster_work_item* work;
+    const fiber_raster_tile_run* runs;
+    float* dom_depth;        // [L][D][D]
+    float* dom_opacity;      // [L][K][D][D]
+    float* shadow_map;       // [L][S][S] stampback target
+    __half* atlas;           // [I][cap][4]
+    __half* history[2];      // [I][cap][2] ping-pong; FrameParams::hist_in is read
+    __half* color;           // [H][W][4]
+    float* depth;            // [H][W]
+    uint32_t* fragments;     // [H][W]
+};
+
+struct CompositeArgs {
+    const __half* strand_color;
+    const float* strand_depth;
+    const void* scene_color;
+    uint32_t scene_pitch, scene_format;
+    const float* scene_depth;
+    uint32_t depth_pitch;
+    void* out;
+    uint32_t out_pitch, out_format;
+    uint32_t width, height;
+};
+
+struct LaunchCtx {
+    cudaStream_t stream;
+    const FrameParams* P;         // device copy
+    const InstanceView* inst;     // device copy
+    uint32_t I, total_coarse_tiles;
+    int sm_count;
+};
+
+void launch_broad(const LaunchCtx& L, const PrepassArgs& A);
+void launch_lut(const LaunchCtx& L, const PrepassArgs& A);
+void launch_fine(const LaunchCtx& L, const PrepassArgs& A);
+void launch_mark(const LaunchCtx& L, const PrepassArgs& A);
+void launch_alloc(const LaunchCtx& L, const PrepassArgs& A);
+void launch_zero_pages(const LaunchCtx& L, const PrepassArgs& A);
+void launch_count(const LaunchCtx& L, const PrepassArgs& A);
+void launch_prefix(const LaunchCtx& L, const PrepassArgs& A);
+void launch_fill(const LaunchCtx& L, const PrepassArgs& A);
+void launch_compact_active(const LaunchCtx& L, const PrepassArgs& A);
+void launch_emit(const LaunchCtx& L, const PrepassArgs& A);
+void launch_sort_big(const LaunchCtx& L, const PrepassArgs& A);
+
+void launch_shadow(const LaunchCtx& L, const RenderArgs& R);
+void launch_shade(const LaunchCtx& L, const RenderArgs& R);
+void launch_raster(const LaunchCtx& L, const RenderArgs& R);
+void launch_composite(cudaStream_t s, const CompositeArgs& C);
+
+}  // namespace fiber

@@ -1,0 +1,930 @@
+// fiber_prepass.cu — work preparation (the reference's work_preparation_pass,
+// src/nodes/prepass.rs:27-233 -> run_prepass, src/pipelines/prepass.rs:818-1397).
+//
+// Stage map (reference entry point -> kernel here):
+//   broad_prepass + broad_strand_prepass (strand_prepass.wgsl:684-782) -> k_broad, folded into k_fine
+//   coarse_interval_pass + build_depth_warp_lut (:835-1014)           -> k_lut
+//   fine_prepass (:1016-1140)                                           -> k_fine (single-pass compaction)
+//   mark_coarse_count_pages_pass (:1928-1932)                           -> k_traverse<kMark>
+//   allocate_coarse_count_pages (:1934-1969)                            -> k_alloc_pages (ordered)
+//   binning_queue_pass (:1986-1990)                                     -> k_traverse<kCount>
+//   prefix_fine_pages (:2051-2143)                                      -> k_prefix_pages
+//   fill_fine_seg_refs (:2190-2194)                                     -> k_traverse<kFill>
+//   prefix_active_tile_blocks + compact_active_tiles (:2581-2676)       -> k_compact_active
+//   emit_raster_work (:2678-2834)                                       -> k_emit (+ canonical cell order)
+// The finalize_* indirect-argument kernels disappear: every consumer is a
+// persistent or grid-stride kernel that reads its item count on the device.
+// Append orders that the reference takes from atomics are replaced by
+// decoupled look-back scans, so every output is deterministic.
+#include "fiber_kernels.cuh"
+
+namespace fiber {
+
+// ===========================================================================
+// K1 broad prepass: coarse range + keep probabilities per (instance, frustum)
+// ===========================================================================
+struct CornerScan {
+    float sminx, sminy, smaxx, smaxy, zmin, zmax;
+    bool any, near_clip;
+};
+
+__device__ CornerScan scan_corners(const float4* corners, const float* clip, float vw, float vh) {
+    CornerScan s{1e30f, 1e30f, -1e30f, -1e30f, 1.0f, 0.0f, false, false};
+    for (int i = 0; i < 8; ++i) {
+        float4 c = matvec(clip, corners[i].x, corners[i].y, corners[i].z, corners[i].w);
+        if (c.w <= 1e-6f) { s.near_clip = true; continue; }
+        float nx = c.x / c.w, ny = c.y / c.w, nz = c.z / c.w;
+        if (nz < 0.0f) s.near_clip = true;
+        float rx = 0.0f + (nx * 0.5f + 0.5f) * vw;
+        float ry = 0.0f + (ny * -0.5f + 0.5f) * vh;
+        s.any = true;
+        s.sminx = wmin(s.sminx, rx);
+        s.sminy = wmin(s.sminy, ry);
+        s.smaxx = wmax(s.smaxx, rx);
+        s.smaxy = wmax(s.smaxy, ry);
+        float z = normalize_depth01(nz);
+        s.zmin = wmin(s.zmin, z);
+        s.zmax = wmax(s.zmax, z);
+    }
+    return s;
+}
+
+__global__ void k_broad(const FrameParams* __restrict__ Pp, const InstanceView* __restrict__ inst, PrepassArgs A) {
+    const FrameParams& P = *Pp;
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P.I) return;
+    const InstanceView& in = inst[i];
+    float keep_max = 0.0f;
+    bool visible = false;
+    float cam_k = 0.0f, sh_k = 0.0f;
+    if (in.valid) {
+        const float* mn = in.aabb.min;
+        const float* mx = in.aabb.max;
+        const float cx[8][3] = {{mn[0], mn[1], mn[2]}, {mn[0], mn[1], mx[2]}, {mn[0], mx[1], mn[2]},
+                                {mn[0], mx[1], mx[2]}, {mx[0], mn[1], mn[2]}, {mx[0], mn[1], mx[2]},
+                                {mx[0], mx[1], mn[2]}, {mx[0], mx[1], mx[2]}};
+        float4 corners[8];
+        for (int c = 0; c < 8; ++c) corners[c] = matvec(in.world_from_local, cx[c][0], cx[c][1], cx[c][2], 1.0f);
+        for (uint32_t f = 0; f < P.F; ++f) {
+            const fiber_frustum_desc& d = P.frusta[f];
+            float k = 0.0f;
+            uint32_t slot = i * P.F + f;
+            A.range_valid[slot] = 0u;
+            if (d.kind <= 1u) {
+                // emit_coarse_asset_range_for_aabb (strand_prepass.wgsl:575-682)
+                bool vis = false;
+                float vw = u2f(d.screen_width), vh = u2f(d.screen_height);
+                if (d.coarse_depth_tile_count != 0u && !(d.kind == 1u && light_layer(P, f) == kInvalid)) {
+                    CornerScan s = scan_corners(corners, P.clip[f], vw, vh);
+                    if (s.near_clip) {
+                        s.sminx = 0.0f; s.sminy = 0.0f;
+                        s.smaxx = vw - 1.0f; s.smaxy = vh - 1.0f;
+                        s.zmax = 1.0f;
+                        if (!s.any) s.zmin = 0.0f;
+                        s.any = true;
+                    }
+                    if (s.any && !(s.smaxx < 0.0f || s.smaxy < 0.0f || s.sminx >= vw || s.sminy >= vh) &&
+                        !(s.zmax < 0.0f || s.zmin > 1.0f)) {
+                        uint32_t cpx = max(1u, d.froxel_size_x * kCoarseExtent);
+                        uint32_t cpy = max(1u, d.froxel_size_y * kCoarseExtent);
+                        float cminx = wclamp(s.sminx, 0.0f, vw - 1.0f), cminy = wclamp(s.sminy, 0.0f, vh - 1.0f);
+                        float cmaxx = wclamp(s.smaxx, 0.0f, vw - 1.0f), cmaxy = wclamp(s.smaxy, 0.0f, vh - 1.0f);
+                        fiber_coarse_asset_range r;
+                        r.geo_id = i;
+                        r.frustum_id = f;
+                        r.min_x = min(f2u(cminx) / cpx, d.coarse_tiles_x - 1u);
+                        r.max_x = min(f2u(cmaxx) / cpx, d.coarse_tiles_x - 1u);
+                        r.min_y = min(f2u(cminy) / cpy, d.coarse_tiles_y - 1u);
+                        r.max_y = min(f2u(cmaxy) / cpy, d.coarse_tiles_y - 1u);
+                        r.z_min_q = quantize_depth01(s.zmin);
+                        r.z_max_q = quantize_depth01(s.zmax);
+                        A.ranges[slot] = r;
+                        A.range_valid[slot] = 1u;
+                        vis = true;
+                    }
+                }
+                visible = vis || visible;
+                if (vis) {
+                    // aabb_projected_screen_area (:295-362)
+                    CornerScan s = scan_corners(corners, P.clip[f], vw, vh);
+                    float area;
+                    if (s.near_clip) area = vw * vh;
+                    else if (!s.any) area = -1.0f;
+                    else if (s.smaxx < 0.0f || s.smaxy < 0.0f || s.sminx >= vw || s.sminy >= vh) area = -1.0f;
+                    else if (s.zmax < 0.0f || s.zmin > 1.0f) area = -1.0f;
+                    else {
+                        float cminx = wclamp(s.sminx, 0.0f, vw - 1.0f), cminy = wclamp(s.sminy, 0.0f, vh - 1.0f);
+                        float cmaxx = wclamp(s.smaxx, 0.0f, vw - 1.0f), cmaxy = wclamp(s.smaxy, 0.0f, vh - 1.0f);
+                        area = wmax(cmaxx - cminx, 1.0f) * wmax(cmaxy - cminy, 1.0f);
+                    }
+                    // stochastic_{camera,shadow}_keep_probability (:364-392)
+                    if (P.stochastic_cull_enabled == 0u) k = 1.0f;
+                    else if (area < 0.0f) k = 0.0f;
+                    else {
+                        float density = wmax(P.target_strands_per_pixel, 1e-5f);
+                        float min_keep = wclamp(P.min_keep_probability, 0.0f, 1.0f);
+                        float area_keep = wclamp(area * density / wmax(u2f(in.strand_count), 1.0f), min_keep, 1.0f);
+                        if (d.kind == 0u) k = area_keep;
+                        else {
+                            float cap = wclamp(P.shadow_keep_probability, 0.0f, 1.0f);
+                            float curved = area_keep * area_keep;
+                            float scale = 1.0f / exp2f(u2f(d.cascade_index));
+                            k = wclamp(curved * scale * cap, min_keep, 1.0f);
+                        }
+                    }
+                    if (d.kind == 0u) cam_k = wmax(cam_k, k);
+                    else sh_k = wmax(sh_k, k);
+                }
+            }
+            A.keep[slot] = k;
+        }
+        keep_max = wmax(cam_k, sh_k);
+    } else {
+        for (uint32_t f = 0; f < P.F; ++f) {
+            A.range_valid[i * P.F + f] = 0u;
+            A.keep[i * P.F + f] = 0.0f;
+        }
+    }
+    A.inst_visible[i] = visible ? 1u : 0u;
+    A.inst_keep[i] = keep_max;
+}
+
+// ===========================================================================
+// K4 + K5: per coarse tile, merge the depth intervals of the ranges covering
+// it (instance order) and split 16 LUT slices across them.
+// ===========================================================================
+__global__ void k_lut(const FrameParams* __restrict__ Pp, PrepassArgs A) {
+    const FrameParams& P = *Pp;
+    uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= P.total_coarse_tiles) return;
+    fiber_coarse_depth_lut_entry* out = A.lut + (size_t)t * kDepthSlices;
+    uint32_t f = frustum_for_tile(P, t);
+    uint32_t mins[kDepthSlices], maxs[kDepthSlices];
+    uint32_t count = 0;
+    if (f != kInvalid) {
+        const fiber_frustum_desc& d = P.frusta[f];
+        uint32_t local = t - d.coarse_depth_tile_base;
+        uint32_t cx = local % d.coarse_tiles_x, cy = local / d.coarse_tiles_x;
+        for (uint32_t i = 0; i < P.I; ++i) {
+            uint32_t slot = i * P.F + f;
+            if (!A.range_valid[slot]) continue;
+            fiber_coarse_asset_range r = A.ranges[slot];
+            if (r.max_x < r.min_x || r.max_y < r.min_y) continue;
+            if (cx < r.min_x || cx > r.max_x || cy < r.min_y || cy > r.max_y) continue;
+            uint32_t zmin = min(r.z_min_q, r.z_max_q), zmax = max(r.z_min_q, r.z_max_q);
+            bool merged = false;
+            for (uint32_t k = 0; k < count; ++k) {
+                if (zmin <= maxs[k] + 1u && zmax + 1u >= mins[k]) {
+                    mins[k] = min(mins[k], zmin);
+                    maxs[k] = max(maxs[k], zmax);
+                    merged = true;
+                }
+            }
+            if (merged) continue;
+            if (count < kDepthSlices) {
+                mins[count] = zmin;
+                maxs[count] = zmax;
+                ++count;
+            } else {
+                uint32_t best = 0, best_gap = 0xFFFFFFFFu;
+                for (uint32_t k = 0; k < kDepthSlices; ++k) {
+                    uint32_t g = maxs[k] < zmin ? zmin - maxs[k] : (zmax < mins[k] ? mins[k] - zmax : 0u);
+                    if (g < best_gap) { best_gap = g; best = k; }
+                }
+                mins[best] = min(mins[best], zmin);
+                maxs[best] = max(maxs[best], zmax);
+            }
+        }
+    }
+    for (uint32_t k = 1; k < count; ++k) {
+        uint32_t j = k, kmin = mins[k], kmax = maxs[k];
+        while (j != 0 && mins[j - 1] > kmin) {
+            mins[j] = mins[j - 1];
+            maxs[j] = maxs[j - 1];
+            --j;
+        }
+        mins[j] = kmin;
+        maxs[j] = kmax;
+    }
+    uint32_t out_slice = 0;
+    for (uint32_t k = 0; k < count; ++k) {
+        uint32_t base_slices = max(1u, kDepthSlices / count);
+        uint32_t rem = kDepthSlices % count;
+        uint32_t slices = base_slices + (k < rem ? 1u : 0u);
+        uint32_t span = max(1u, maxs[k] - mins[k] + 1u);
+        for (uint32_t s = 0; s < slices && out_slice < kDepthSlices; ++s) {
+            uint32_t start = mins[k] + (span * s) / slices;
+            uint32_t excl_end = mins[k] + (span * (s + 1u)) / slices;
+            uint32_t end = min(excl_end > start ? excl_end - 1u : start, maxs[k]);
+            out[out_slice++] = fiber_coarse_depth_lut_entry{start, end, start, max(1u, end - start + 1u)};
+        }
+    }
+    for (; out_slice < kDepthSlices; ++out_slice) out[out_slice] = fiber_coarse_depth_lut_entry{0u, 0u, 0u, 0u};
+}
+
+// ===========================================================================
+// K2 + K6 fine prepass: one warp per strand, eight strands per block, one
+// block per (frustum, strand chunk) in frustum-major order. Each block counts
+// its clipped segments, takes its output offset from a decoupled look-back
+// and writes BinningTask + ProjectedSegment in (frustum, inst, strand, seg)
+// order — the binning queue's canonical order, produced without a sort.
+// ===========================================================================
+constexpr int kFineThreads = 256;
+constexpr int kFineWarps = kFineThreads / 32;
+
+struct SegOut {
+    uint32_t seg;
+    uint32_t p0, p1, dz;
+};
+
+__device__ __forceinline__ bool fine_segment(const FrameParams& P, const InstanceView& in, uint32_t f,
+                                             uint32_t seg, SegOut& o) {
+    const fiber_frustum_desc& d = P.frusta[f];
+    if (seg + 1u >= in.n_indices) return false;
+    uint32_t vi0 = __ldg(in.indices + seg), vi1 = __ldg(in.indices + seg + 1u);
+    float4 a = __ldg(in.vertices + vi0), b = __ldg(in.vertices + vi1);
+    const float* W = in.world_from_local;
+    float4 w0 = matvec(W, a.x, a.y, a.z, 1.0f), w1 = matvec(W, b.x, b.y, b.z, 1.0f);
+    float vw = u2f(d.screen_width), vh = u2f(d.screen_height);
+    float4 r0 = world_to_screen_raw(w0, P.clip[f], vw, vh), r1 = world_to_screen_raw(w1, P.clip[f], vw, vh);
+    F3 p0 = f3(r0.x, r0.y, normalize_depth01(r0.z)), p1 = f3(r1.x, r1.y, normalize_depth01(r1.z));
+    F3 c0, c1;
+    if (!clip_segment(p0, p1, f3(0.0f, 0.0f, 0.0f), f3(wmax(0.0f, vw - 1e-3f), wmax(0.0f, vh - 1e-3f), 1.0f), c0, c1))
+        return false;
+    float ssx = wmax(1.0f, vw), ssy = wmax(1.0f, vh);
+    o.seg = seg;
+    o.p0 = pack2x16unorm(wclamp(c0.x / ssx, 0.0f, 1.0f), wclamp(c0.y / ssy, 0.0f, 1.0f));
+    o.p1 = pack2x16unorm(wclamp(c1.x / ssx, 0.0f, 1.0f), wclamp(c1.y / ssy, 0.0f, 1.0f));
+    o.dz = pack2x16unorm(wclamp(c0.z, 0.0f, 1.0f), wclamp(c1.z, 0.0f, 1.0f));
+    return true;
+}
+
+__global__ void __launch_bounds__(kFineThreads) k_fine(const FrameParams* __restrict__ Pp,
+                                                       const InstanceView* __restrict__ inst, PrepassArgs A) {
+    const FrameParams& P = *Pp;
+    __shared__ uint32_t s_tile;
+    __shared__ uint32_t s_warp_count[kFineWarps];
+    __shared__ uint32_t s_base;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t tiles_per_f = ceil_div(P.total_strands, kFineWarps);
+    const uint32_t n_tiles = tiles_per_f * P.F;
+    for (;;) {
+        if (threadIdx.x == 0) s_tile = atomicAdd(A.tile_counter, 1u);
+        __syncthreads();
+        const uint32_t tile = s_tile;
+        if (tile >= n_tiles) break;
+        const uint32_t f = tile / tiles_per_f;
+        const uint32_t g = (tile % tiles_per_f) * kFineWarps + warp;
+        // Resolve the strand (instance, local strand) and the K2/K6 keep tests.
+        uint32_t nseg = 0, i = 0, s = 0, meta_offset = 0, packed = 0;
+        if (g < P.total_strands) {
+            uint32_t lo = 0, hi = P.I;  // last instance with strand_base <= g
+            while (hi - lo > 1u) {
+                uint32_t mid = (lo + hi) >> 1;
+                if (inst[mid].strand_base <= g) lo = mid; else hi = mid;
+            }
+            i = lo;
+            s = g - inst[i].strand_base;
+            const InstanceView& in = inst[i];
+            const fiber_frustum_desc& d = P.frusta[f];
+            float r = hash_to_unit_float(wang_hash((i * 16777619u) ^ s));
+            bool ok = in.valid && A.inst_visible[i] != 0u && s < in.strand_count && !(r > A.inst_keep[i]);
+            ok = ok && d.kind <= 1u && s < in.n_meta;
+            if (ok) {
+                fiber_strand_meta m = in.meta[s];
+                ok = m.count >= 2u && !(r > A.keep[i * P.F + f]) && !(d.kind == 1u && light_layer(P, f) == kInvalid);
+                if (ok) {
+                    nseg = m.count - 1u;
+                    meta_offset = m.offset;
+                    packed = ((d.kind == 1u ? 1u : 0u) << 2u) | (f << 3u);
+                }
+            }
+        }
+        // Pass A: count (results of the first 32 segments stay in registers).
+        uint32_t count = 0;
+        SegOut first{};
+        bool first_ok = false;
+        for (uint32_t c = 0; c < nseg; c += 32u) {
+            SegOut o;
+            bool ok = (c + lane < nseg) && fine_segment(P, inst[i], f, meta_offset + c + lane, o);
+            if (c == 0u) { first = o; first_ok = ok; }
+            count += __popc(__ballot_sync(0xFFFFFFFFu, ok));
+        }
+        if (lane == 0) s_warp_count[warp] = count;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            uint32_t agg = 0;
+            for (int w = 0; w < kFineWarps; ++w) agg += s_warp_count[w];
+            uint32_t base = lb_exclusive(A.lb_status, tile, P.epoch, agg, &A.counters->error);
+            s_base = base;
+            if (tile % tiles_per_f == 0u) A.counters->frustum_task_base[f] = base;
+            if (tile == n_tiles - 1u) {
+                A.counters->tasks = base + agg;
+                A.counters->frustum_task_base[P.F] = base + agg;
+            }
+        }
+        __syncthreads();
+        uint32_t out = s_base;
+        for (int w = 0; w < warp; ++w) out += s_warp_count[w];
+        // Pass B: write in segment order.
+        for (uint32_t c = 0; c < nseg; c += 32u) {
+            SegOut o = first;
+            bool ok = first_ok;
+            if (c != 0u) ok = (c + lane < nseg) && fine_segment(P, inst[i], f, meta_offset + c + lane, o);
+            uint32_t mask = __ballot_sync(0xFFFFFFFFu, ok);
+            if (ok) {
+                uint32_t dst = out + __popc(mask & ((1u << lane) - 1u));
+                if (dst < P.task_capacity) {
+                    reinterpret_cast<uint4*>(A.tasks)[dst] = make_uint4(i, s, o.seg, packed);
+                    fiber_projected_segment ps{o.p0, o.p1, o.dz};
+                    A.projected[dst] = ps;
+                } else {
+                    atomicOr(&A.counters->overflow, 1u);
+                }
+            }
+            out += __popc(mask);
+        }
+        __syncthreads();
+    }
+}
+
+// ===========================================================================
+// K7 / K9 / K11 traversal: coarse-tile 2-D DDA, LUT slices, then the fine
+// 3-D DDA inside each page (strand_prepass.wgsl:1251-1696,1894-1926).
+// ===========================================================================
+enum : int { kMark = 0, kCount = 1, kFill = 2 };
+
+__device__ __forceinline__ uint32_t lut_slice(const fiber_coarse_depth_lut_entry* e, float z) {
+    uint32_t zq = quantize_depth01(z);
+    uint32_t best = kInvalid, best_d = 0xFFFFFFFFu;
+    for (uint32_t i = 0; i < kDepthSlices; ++i) {
+        fiber_coarse_depth_lut_entry x = e[i];
+        if (x.virtual_count_q == 0u) continue;
+        if (zq >= x.z_min_q && zq <= x.z_max_q) return i;
+        uint32_t dist = zq > x.z_max_q ? zq - x.z_max_q : x.z_min_q - zq;
+        if (dist < best_d) { best_d = dist; best = i; }
+    }
+    return best;
+}
+
+template <int PASS>
+__device__ __forceinline__ void emit_cell(const PrepassArgs& A, uint32_t page, uint32_t cell, uint32_t ref_seg,
+                                          uint32_t ref_inst, uint32_t ref_mat, uint32_t key) {
+    size_t g = (size_t)page * kPageSize + cell;
+    if (PASS == kCount) {
+        atomicAdd(A.counts + g, 1u);
+    } else {
+        fiber_fine_page_meta pm = A.page_meta[page];
+        if (pm.seg_ref_count == 0u) return;
+        uint32_t lw = atomicAdd(A.cursors + g, 1u);
+        uint64_t dst = (uint64_t)pm.seg_ref_base + A.offsets[g] + lw;
+        if (dst >= (uint64_t)(pm.seg_ref_base) + pm.seg_ref_count) return;
+        A.refs[dst] = fiber_fine_seg_ref{ref_inst, ref_seg, ref_mat};
+        A.ref_keys[dst] = key;
+    }
+}
+
+template <int PASS>
+__device__ void trace_page(const FrameParams& P, const PrepassArgs& A, F3 p0, F3 p1, const fiber_frustum_desc& d,
+                           uint32_t tile, uint32_t local, uint32_t ref_inst, uint32_t ref_seg, uint32_t ref_mat,
+                           uint32_t key) {
+    uint32_t ccx = local % d.coarse_tiles_x, ccy = local / d.coarse_tiles_x;
+    uint32_t cpx = max(1u, d.froxel_size_x * kCoarseExtent);
+    uint32_t cpy = max(1u, d.froxel_size_y * kCoarseExtent);
+    float ox = u2f(ccx * cpx), oy = u2f(ccy * cpy);
+    float tmx = wmin(ox + u2f(cpx), u2f(d.screen_width)) - 1e-3f;
+    float tmy = wmin(oy + u2f(cpy), u2f(d.screen_height)) - 1e-3f;
+    F3 bmax = f3(wmax(ox, tmx), wmax(oy, tmy), 1.0f);
+    F3 c0, c1;
+    if (!clip_segment(p0, p1, f3(ox, oy, 0.0f), bmax, c0, c1)) return;
+    const fiber_coarse_depth_lut_entry* lut = A.lut + (size_t)tile * kDepthSlices;
+    uint32_t z0s = lut_slice(lut, c0.z), z1s = lut_slice(lut, c1.z);
+    if (z0s == kInvalid || z1s == kInvalid) return;
+    for (uint32_t cz = min(z0s, z1s); cz <= max(z0s, z1s); ++cz) {
+        fiber_coarse_depth_lut_entry e = lut[cz];
+        if (e.virtual_count_q == 0u) continue;
+        float zmin = dequantize_depth01(e.z_min_q), zmax = dequantize_depth01(e.z_max_q);
+        F3 d0, d1;
+        if (!clip_segment(c0, c1, f3(ox, oy, zmin), f3(bmax.x, bmax.y, zmax), d0, d1)) continue;
+        uint32_t pti = tile * kDepthSlices + cz;
+        if (PASS == kMark) {
+            A.page_table[pti] = kMarked;
+            continue;
+        }
+        uint32_t handle = A.page_table[pti];
+        if (handle == 0u || handle == kMarked) continue;
+        uint32_t page = handle - 1u;
+        float zspan = wmax(zmax - zmin, 1.0f / (float)kDepthQuantMax);
+        float fsx = u2f(d.froxel_size_x), fsy = u2f(d.froxel_size_y);
+        float l0[3] = {(d0.x - ox) / fsx, (d0.y - oy) / fsy, wclamp((d0.z - zmin) / zspan, 0.0f, 0.999999f) * 16.0f};
+        float l1[3] = {(d1.x - ox) / fsx, (d1.y - oy) / fsy, wclamp((d1.z - zmin) / zspan, 0.0f, 0.999999f) * 16.0f};
+        int32_t f1[3], fc[3], step[3];
+        float tm[3], dd[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            int32_t hi = a == 2 ? 15 : 3;
+            fc[a] = iclamp(f2i(floorf(l0[a])), 0, hi);
+            f1[a] = iclamp(f2i(floorf(l1[a])), 0, hi);
+            float dir = l1[a] - l0[a];
+            step[a] = sgn_i32(dir);
+            float sd = fabsf(dir) < 1e-6f ? 1e-6f : dir;
+            dd[a] = fabsf(1.0f / sd);
+            float fl = floorf(l0[a]);
+            tm[a] = step[a] > 0 ? ((fl + 1.0f) - l0[a]) / sd : (fl - l0[a]) / sd;
+            if (fabsf(dir) < 1e-6f) tm[a] = 1e38f;
+        }
+        uint32_t safety = 0;
+        for (;;) {
+            if (safety > kCoarseExtent + kCoarseExtent + kDepthSlices + 3u) break;
+            // fine_tile_occluded_by_opaque (:551-573): no opaque depth tiles are
+            // bound on this path, so the cull never fires.
+            emit_cell<PASS>(A, page, (uint32_t)((fc[2] * 4 + fc[1]) * 4 + fc[0]), ref_seg, ref_inst, ref_mat, key);
+            if (fc[0] == f1[0] && fc[1] == f1[1] && fc[2] == f1[2]) break;
+            float m = wmin(wmin(tm[0], tm[1]), tm[2]);  // canonical_min_mask
+            int a = tm[0] == m ? 0 : (tm[1] == m ? 1 : 2);
+            if (a == 0) { fc[0] += step[0]; tm[0] += dd[0]; }
+            else if (a == 1) { fc[1] += step[1]; tm[1] += dd[1]; }
+            else { fc[2] += step[2]; tm[2] += dd[2]; }
+            if (fc[0] < 0 || fc[1] < 0 || fc[2] < 0 || fc[0] >= 4 || fc[1] >= 4 || fc[2] >= 16) break;
+            ++safety;
+        }
+    }
+}
+
+template <int PASS>
+__global__ void __launch_bounds__(256) k_traverse(const FrameParams* __restrict__ Pp,
+                                                  const InstanceView* __restrict__ inst, PrepassArgs A) {
+    const FrameParams& P = *Pp;
+    const uint32_t n = *((volatile uint32_t*)&A.counters->tasks);
+    const uint32_t n_cap = min(n, P.task_capacity);
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n_cap; k += gridDim.x * blockDim.x) {
+        uint4 t = reinterpret_cast<const uint4*>(A.tasks)[k];
+        uint32_t f = t.w >> 3u;
+        if (f >= P.F) continue;
+        uint32_t i = t.x;
+        if (i >= P.I) continue;
+        const fiber_frustum_desc& d = P.frusta[f];
+        fiber_projected_segment pr = A.projected[k];
+        float sw = u2f(d.screen_width), sh = u2f(d.screen_height);
+        float2 a = unpack2x16unorm(pr.p0_xy), b = unpack2x16unorm(pr.p1_xy), z = unpack2x16unorm(pr.depths);
+        F3 p0 = f3(a.x * sw, a.y * sh, z.x), p1 = f3(b.x * sw, b.y * sh, z.y);
+        uint32_t slot = i * P.F + f;
+        if (!A.range_valid[slot]) continue;
+        fiber_coarse_asset_range r = A.ranges[slot];
+        uint32_t ref_mat = 0, key = 0;
+        if (PASS == kFill) {
+            // make_fine_seg_ref (:1313-1327)
+            const InstanceView& in = inst[i];
+            if (t.y < in.n_meta) ref_mat = in.meta[t.y].material_idx;
+            key = (pr.depths & 0xFFFFu) + (pr.depths >> 16u);
+        }
+        uint32_t cpx = max(1u, d.froxel_size_x * kCoarseExtent);
+        uint32_t cpy = max(1u, d.froxel_size_y * kCoarseExtent);
+        uint32_t min_cx = max(r.min_x, min(f2u(wmax(wmin(p0.x, p1.x), 0.0f)) / cpx, d.coarse_tiles_x - 1u));
+        uint32_t max_cx = min(r.max_x, min(f2u(wmax(wmax(p0.x, p1.x), 0.0f)) / cpx, d.coarse_tiles_x - 1u));
+        uint32_t min_cy = max(r.min_y, min(f2u(wmax(wmin(p0.y, p1.y), 0.0f)) / cpy, d.coarse_tiles_y - 1u));
+        uint32_t max_cy = min(r.max_y, min(f2u(wmax(wmax(p0.y, p1.y), 0.0f)) / cpy, d.coarse_tiles_y - 1u));
+        if (max_cx < min_cx || max_cy < min_cy) continue;
+        F3 bmin = f3(u2f(min_cx * cpx), u2f(min_cy * cpy), 0.0f);
+        F3 bmax = f3(wmin(u2f((max_cx + 1u) * cpx), sw) - 1e-3f, wmin(u2f((max_cy + 1u) * cpy), sh) - 1e-3f, 1.0f);
+        F3 c0, c1;
+        if (!clip_segment(p0, p1, bmin, bmax, c0, c1)) continue;
+        float x0 = c0.x / u2f(cpx), y0 = c0.y / u2f(cpy), x1 = c1.x / u2f(cpx), y1 = c1.y / u2f(cpy);
+        int32_t fx = iclamp(f2i(floorf(x0)), (int32_t)min_cx, (int32_t)max_cx);
+        int32_t fy = iclamp(f2i(floorf(y0)), (int32_t)min_cy, (int32_t)max_cy);
+        int32_t ex = iclamp(f2i(floorf(x1)), (int32_t)min_cx, (int32_t)max_cx);
+        int32_t ey = iclamp(f2i(floorf(y1)), (int32_t)min_cy, (int32_t)max_cy);
+        float dx = x1 - x0, dy = y1 - y0;
+        int32_t sx = sgn_i32(dx), sy = sgn_i32(dy);
+        float sdx = fabsf(dx) < 1e-6f ? 1e-6f : dx, sdy = fabsf(dy) < 1e-6f ? 1e-6f : dy;
+        float ddx = fabsf(1.0f / sdx), ddy = fabsf(1.0f / sdy);
+        float flx = floorf(x0), fly = floorf(y0);
+        float tx = sx > 0 ? ((flx + 1.0f) - x0) / sdx : (flx - x0) / sdx;
+        float ty = sy > 0 ? ((fly + 1.0f) - y0) / sdy : (fly - y0) / sdy;
+        if (fabsf(dx) < 1e-6f) tx = 1e38f;
+        if (fabsf(dy) < 1e-6f) ty = 1e38f;
+        uint32_t safety = 0, max_steps = (max_cx - min_cx + 1u) + (max_cy - min_cy + 1u) + 2u;
+        for (;;) {
+            if (safety > max_steps) break;
+            if (fx < (int32_t)min_cx || fx > (int32_t)max_cx || fy < (int32_t)min_cy || fy > (int32_t)max_cy) break;
+            uint32_t local = (uint32_t)fy * d.coarse_tiles_x + (uint32_t)fx;
+            if (local < d.coarse_depth_tile_count)
+                trace_page<PASS>(P, A, p0, p1, d, d.coarse_depth_tile_base + local, local, i, t.z, ref_mat, key);
+            if (fx == ex && fy == ey) break;
+            if (tx <= ty) { fx += sx; tx += ddx; } else { fy += sy; ty += ddy; }
+            ++safety;
+        }
+    }
+}
+
+// ===========================================================================
+// K8: allocate marked pages in page-table order.
+// ===========================================================================
+constexpr int kScanThreads = 256;
+constexpr int kScanItems = 4;
+
+__global__ void __launch_bounds__(kScanThreads) k_alloc_pages(const FrameParams* __restrict__ Pp, PrepassArgs A) {
+    const FrameParams& P = *Pp;
+    __shared__ uint32_t s_tile, s_base;
+    __shared__ uint32_t s_warp[33];
+    const uint32_t n = P.total_coarse_tiles * kDepthSlices;
+    const uint32_t per_tile = kScanThreads * kScanItems;
+    const uint32_t n_tiles = ceil_div(n, per_tile);
+    for (;;) {
+        if (threadIdx.x == 0) s_tile = atomicAdd(A.tile_counter, 1u);
+        __syncthreads();
+        const uint32_t tile = s_tile;
+        if (tile >= n_tiles) break;
+        const uint32_t e0 = tile * per_tile + threadIdx.x * kScanItems;
+        uint32_t flags[kScanItems], cnt = 0;
+#pragma unroll
+        for (int j = 0; j < kScanItems; ++j) {
+            flags[j] = (e0 + j < n && A.page_table[e0 + j] == kMarked) ? 1u : 0u;
+            cnt += flags[j];
+        }
+        uint32_t total;
+        uint32_t excl = block_exclusive_scan<kScanThreads>(cnt, s_warp, total);
+        if (threadIdx.x == 0) {
+            uint32_t base = lb_exclusive(A.lb_status, tile, P.epoch, total, &A.counters->error);
+            s_base = base;
+            if (tile == n_tiles - 1u) A.counters->pages = min(base + total, P.page_capacity);
+        }
+        __syncthreads();
+        uint32_t idx = s_base + excl;
+#pragma unroll
+        for (int j = 0; j < kScanItems; ++j) {
+            if (!flags[j]) continue;
+            uint32_t pti = e0 + j;
+            if (idx >= P.page_capacity) {
+                A.page_table[pti] = 0u;
+                atomicOr(&A.counters->overflow, 2u);
+            } else {
+                A.page_meta[idx] = fiber_fine_page_meta{0u, 0u, 0u, 0u, pti / kDepthSlices, pti % kDepthSlices, 0u, 0u};
+                A.page_table[pti] = idx + 1u;
+            }
+            ++idx;
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void k_zero_pages(PrepassArgs A) {
+    const uint32_t pages = *((volatile uint32_t*)&A.counters->pages);
+    const uint32_t n = pages * (kPageSize / 4u);
+    uint4* c = reinterpret_cast<uint4*>(A.counts);
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
+        c[k] = make_uint4(0u, 0u, 0u, 0u);
+}
+
+// ===========================================================================
+// K10: per page exclusive scan of the 256 cell counts; page ref bases from a
+// look-back over pages (page order); active fine-tile flags.
+// ===========================================================================
+__global__ void __launch_bounds__(256) k_prefix_pages(const FrameParams* __restrict__ Pp, PrepassArgs A) {
+    const FrameParams& P = *Pp;
+    __shared__ uint32_t s_tile, s_base;
+    __shared__ uint32_t s_warp[33];
+    __shared__ uint32_t s_counts[kPageSize];
+    const uint32_t pages = *((volatile uint32_t*)&A.counters->pages);
+    for (;;) {
+        if (threadIdx.x == 0) s_tile = atomicAdd(A.tile_counter, 1u);
+        __syncthreads();
+        const uint32_t page = s_tile;
+        if (page >= pages) break;
+        const size_t g = (size_t)page * kPageSize + threadIdx.x;
+        uint32_t c = A.counts[g];
+        s_counts[threadIdx.x] = c;
+        uint32_t total;
+        uint32_t excl = block_exclusive_scan<256>(c, s_warp, total);
+        A.offsets[g] = excl;
+        A.cursors[g] = 0u;
+        if (threadIdx.x == 0) {
+            uint32_t base = lb_exclusive(A.lb_status, page, P.epoch, total, &A.counters->error);
+            fiber_fine_page_meta pm = A.page_meta[page];
+            uint32_t flags = 0u;
+            if (total > 0u && (uint64_t)base + total > (uint64_t)P.ref_capacity) {
+                flags = 1u;
+                atomicOr(&A.counters->overflow, 4u);
+            }
+            pm.seg_ref_base = total > 0u ? base : 0u;
+            pm.seg_ref_count = flags ? 0u : total;
+            pm.flags = flags;
+            A.page_meta[page] = pm;
+            s_base = flags;
+            if (page == pages - 1u) A.counters->refs = base + total;
+        }
+        __syncthreads();
+        if (threadIdx.x < 16u && s_base == 0u) {
+            const uint32_t lt = threadIdx.x;
+            bool has = false;
+            for (uint32_t z = 0; z < kDepthSlices; ++z) has = has || s_counts[z * 16u + lt] > 0u;
+            if (has) {
+                fiber_fine_page_meta pm = A.page_meta[page];
+                uint32_t f = frustum_for_tile(P, pm.coarse_tile_id);
+                if (f != kInvalid) {
+                    const fiber_frustum_desc& d = P.frusta[f];
+                    uint32_t lc = pm.coarse_tile_id - d.coarse_depth_tile_base;
+                    uint32_t fx = (lc % d.coarse_tiles_x) * kCoarseExtent + lt % kCoarseExtent;
+                    uint32_t fy = (lc / d.coarse_tiles_x) * kCoarseExtent + lt / kCoarseExtent;
+                    if (fx < ceil_div(d.screen_width, d.froxel_size_x) && fy < ceil_div(d.screen_height, d.froxel_size_y))
+                        A.active_flags[(size_t)pm.coarse_tile_id * 16u + lt] = 1u;
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// ===========================================================================
+// K13: ordered compaction of the active fine-tile flags.
+// ===========================================================================
+__global__ void __launch_bounds__(kScanThreads) k_compact_active(const FrameParams* __restrict__ Pp, PrepassArgs A) {
+    const FrameParams& P = *Pp;
+    __shared__ uint32_t s_tile, s_base;
+    __shared__ uint32_t s_warp[33];
+    const uint32_t n = P.total_coarse_tiles * 16u;
+    const uint32_t cam_end = P.camera_tile_end * 16u;
+    const uint32_t per_tile = kScanThreads * kScanItems;
+    const uint32_t n_tiles = ceil_div(n, per_tile);
+    for (;;) {
+        if (threadIdx.x == 0) s_tile = atomicAdd(A.tile_counter, 1u);
+        __syncthreads();
+        const uint32_t tile = s_tile;
+        if (tile >= n_tiles) break;
+        const uint32_t e0 = tile * per_tile + threadIdx.x * kScanItems;
+        uint32_t flags[kScanItems], cnt = 0, cam = 0;
+#pragma unroll
+        for (int j = 0; j < kScanItems; ++j) {
+            flags[j] = (e0 + j < n && A.active_flags[e0 + j] != 0u) ? 1u : 0u;
+            cnt += flags[j];
+            cam += (flags[j] && e0 + j < cam_end) ? 1u : 0u;
+        }
+        uint32_t total;
+        uint32_t excl = block_exclusive_scan<kScanThreads>(cnt, s_warp, total);
+        for (int o = 16; o > 0; o >>= 1) cam += __shfl_xor_sync(0xFFFFFFFFu, cam, o);
+        if ((threadIdx.x & 31) == 0 && cam) atomicAdd(&A.counters->camera_active, cam);
+        if (threadIdx.x == 0) {
+            uint32_t base = lb_exclusive(A.lb_status, tile, P.epoch, total, &A.counters->error);
+            s_base = base;
+            if (tile == n_tiles - 1u) A.counters->active_tiles = base + total;
+        }
+        __syncthreads();
+        uint32_t idx = s_base + excl;
+#pragma unroll
+        for (int j = 0; j < kScanItems; ++j)
+            if (flags[j]) A.active_list[idx++] = e0 + j;
+        __syncthreads();
+    }
+}
+
+// ===========================================================================
+// K14: emit raster work per active fine tile (256 lanes = 16 coarse z x 16
+// fine z, near to far), and put every cell's references into canonical order
+// (projected depth key descending, then instance, then segment). Cells of up
+// to 32 references are sorted by one warp in registers; larger cells are
+// queued for k_sort_big_cells.
+// ===========================================================================
+__device__ __forceinline__ unsigned long long ref_sort_key(uint32_t key17, uint32_t inst, uint32_t seg) {
+    return ((unsigned long long)(0x1FFFFu - (key17 & 0x1FFFFu)) << 47) |
+           ((unsigned long long)(inst & 0x7FFFu) << 32) | (unsigned long long)seg;
+}
+
+__device__ __forceinline__ void warp_sort_cell(const PrepassArgs& A, uint32_t base, uint32_t n, int lane) {
+    unsigned long long k = ~0ull;
+    uint32_t mat = 0u;
+    if ((uint32_t)lane < n) {
+        fiber_fine_seg_ref r = A.refs[base + lane];
+        k = ref_sort_key(A.ref_keys[base + lane], r.inst_id, r.seg_id);
+        mat = r.material_idx;
+    }
+    // Bitonic sort over 32 lanes, ascending by k.
+#pragma unroll
+    for (int size = 2; size <= 32; size <<= 1) {
+#pragma unroll
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            unsigned long long ok = __shfl_xor_sync(0xFFFFFFFFu, k, stride);
+            uint32_t om = __shfl_xor_sync(0xFFFFFFFFu, mat, stride);
+            bool up = ((lane & size) == 0);
+            bool lower = (lane & stride) == 0;
+            bool take_other = lower == up ? (ok < k) : (ok > k);
+            if (take_other) { k = ok; mat = om; }
+        }
+    }
+    if ((uint32_t)lane < n) {
+        uint32_t key17 = 0x1FFFFu - (uint32_t)(k >> 47);
+        A.refs[base + lane] = fiber_fine_seg_ref{(uint32_t)(k >> 32) & 0x7FFFu, (uint32_t)k, mat};
+        A.ref_keys[base + lane] = key17;
+    }
+}
+
+__global__ void __launch_bounds__(256) k_emit(const FrameParams* __restrict__ Pp, PrepassArgs A) {
+    const FrameParams& P = *Pp;
+    __shared__ uint32_t s_tile, s_base;
+    __shared__ uint32_t s_warp[33];
+    __shared__ uint32_t s_load[8];
+    __shared__ uint32_t s_sort_n;
+    __shared__ uint2 s_sort[256];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t n_active = *((volatile uint32_t*)&A.counters->active_tiles);
+    for (;;) {
+        if (threadIdx.x == 0) { s_tile = atomicAdd(A.tile_counter, 1u); s_sort_n = 0u; }
+        __syncthreads();
+        const uint32_t a = s_tile;
+        if (a >= n_active) break;
+        const uint32_t packed = A.active_list[a];
+        const uint32_t lt = packed % 16u, tile = packed / 16u;
+        const uint32_t f = frustum_for_tile(P, tile);
+        const fiber_frustum_desc& d = P.frusta[f < P.F ? f : 0];
+        const uint32_t lc = tile - d.coarse_depth_tile_base;
+        const uint32_t lx = lt % kCoarseExtent, ly = lt / kCoarseExtent;
+        const uint32_t fx = (lc % d.coarse_tiles_x) * kCoarseExtent + lx;
+        const uint32_t fy = (lc / d.coarse_tiles_x) * kCoarseExtent + ly;
+        const uint32_t screen_tile = fy * ceil_div(d.screen_width, d.froxel_size_x) + fx;
+        const uint32_t depth_lane = kPageSize - 1u - threadIdx.x;
+        const uint32_t cz = depth_lane / kDepthSlices, fz = depth_lane % kDepthSlices;
+        const uint32_t pti = tile * kDepthSlices + cz;
+        uint32_t cnt = 0, base = 0, page = kInvalid, cell = 0;
+        if (f != kInvalid) {
+            uint32_t handle = A.page_table[pti];
+            if (handle != 0u && handle != kMarked) {
+                page = handle - 1u;
+                fiber_fine_page_meta pm = A.page_meta[page];
+                cell = (fz * kCoarseExtent + ly) * kCoarseExtent + lx;
+                if (pm.seg_ref_count > 0u && pm.flags == 0u) {
+                    cnt = A.counts[(size_t)page * kPageSize + cell];
+                    if (cnt > 0u) base = pm.seg_ref_base + A.offsets[(size_t)page * kPageSize + cell];
+                }
+            }
+        }
+        // Canonical order inside each cell.
+        if (cnt > 32u) {
+            uint32_t slot = atomicAdd(&A.counters->big_cells, 1u);
+            A.big_cells[slot] = make_uint2(base, cnt);
+        } else if (cnt >= 2u) {
+            uint32_t slot = atomicAdd(&s_sort_n, 1u);
+            s_sort[slot] = make_uint2(base, cnt);
+        }
+        const uint32_t has = cnt > 0u ? 1u : 0u;
+        uint32_t load = cnt;
+        for (int o = 16; o > 0; o >>= 1) load += __shfl_xor_sync(0xFFFFFFFFu, load, o);
+        if (lane == 0) s_load[warp] = load;
+        uint32_t n_work;
+        uint32_t excl = block_exclusive_scan<256>(has, s_warp, n_work);
+        if (threadIdx.x == 0) {
+            uint32_t wb = lb_exclusive(A.lb_status, a, P.epoch, n_work, &A.counters->error);
+            s_base = wb;
+            uint32_t total_load = 0;
+            for (int w = 0; w < 8; ++w) total_load += s_load[w];
+            A.runs[a] = fiber_raster_tile_run{wb, n_work, f, screen_tile, total_load, 0u, 0u, 0u};
+            if (a == n_active - 1u) A.counters->work_items = wb + n_work;
+        }
+        __syncthreads();
+        if (has) {
+            uint32_t lutk = pti;
+            fiber_coarse_depth_lut_entry lut = A.lut[lutk];
+            uint32_t dkey = lut.virtual_count_q == 0u ? fz : lut.virtual_start_q + (lut.virtual_count_q * fz) / kDepthSlices;
+            uint32_t dst = s_base + excl;
+            if (dst < P.work_capacity)
+                A.work[dst] = fiber_raster_work_item{base, cnt, f, screen_tile, dkey, cnt, page, cell};
+            else
+                atomicOr(&A.counters->overflow, 8u);
+        }
+        const uint32_t n_sort = s_sort_n;
+        for (uint32_t j = warp; j < n_sort; j += 8u) warp_sort_cell(A, s_sort[j].x, s_sort[j].y, lane);
+        __syncthreads();
+    }
+}
+
+// Large cells: one block per cell. Bitonic sort in the ascending-only form
+// (each stage starts with a "flip" compare i <-> i ^ (size - 1)), which never
+// moves the virtual +inf padding below n, so the padding needs no storage.
+// Up to kBigSmem entries sort in shared memory; longer cells sort in place in
+// global memory with the same network.
+constexpr uint32_t kBigSmem = 8192;
+constexpr size_t kBigSmemBytes = kBigSmem * (sizeof(unsigned long long) + sizeof(uint32_t));
+
+__device__ __forceinline__ void big_load(const PrepassArgs& A, uint32_t base, uint32_t n, uint32_t i,
+                                         unsigned long long& k, uint32_t& m) {
+    if (i < n) {
+        fiber_fine_seg_ref r = A.refs[base + i];
+        k = ref_sort_key(A.ref_keys[base + i], r.inst_id, r.seg_id);
+        m = r.material_idx;
+    } else {
+        k = ~0ull;
+        m = 0u;
+    }
+}
+__device__ __forceinline__ void big_store(const PrepassArgs& A, uint32_t base, uint32_t i, unsigned long long k,
+                                          uint32_t m) {
+    A.refs[base + i] = fiber_fine_seg_ref{(uint32_t)(k >> 32) & 0x7FFFu, (uint32_t)k, m};
+    A.ref_keys[base + i] = 0x1FFFFu - (uint32_t)(k >> 47);
+}
+// Pair t of a stage: (i, j) with i < j.
+__device__ __forceinline__ void bitonic_pair(uint32_t t, uint32_t size, uint32_t stride, bool flip, uint32_t& i,
+                                             uint32_t& j) {
+    if (flip) {
+        uint32_t half = size >> 1, blk = t / half, off = t % half;
+        i = blk * size + off;
+        j = blk * size + size - 1u - off;
+    } else {
+        i = (t / stride) * 2u * stride + (t % stride);
+        j = i + stride;
+    }
+}
+
+__global__ void __launch_bounds__(256) k_sort_big_cells(PrepassArgs A) {
+    extern __shared__ unsigned char s_raw[];
+    unsigned long long* s_k = reinterpret_cast<unsigned long long*>(s_raw);
+    uint32_t* s_m = reinterpret_cast<uint32_t*>(s_raw + kBigSmem * sizeof(unsigned long long));
+    const uint32_t n_cells = *((volatile uint32_t*)&A.counters->big_cells);
+    for (uint32_t c = blockIdx.x; c < n_cells; c += gridDim.x) {
+        const uint2 bc = A.big_cells[c];
+        const uint32_t base = bc.x, n = bc.y;
+        uint32_t np = 1;
+        while (np < n) np <<= 1;
+        const bool in_smem = np <= kBigSmem;
+        if (in_smem) {
+            for (uint32_t i = threadIdx.x; i < np; i += blockDim.x) big_load(A, base, n, i, s_k[i], s_m[i]);
+            __syncthreads();
+        }
+        for (uint32_t size = 2; size <= np; size <<= 1) {
+            for (uint32_t stride = size >> 1; stride > 0; stride >>= 1) {
+                const bool flip = stride == (size >> 1);
+                for (uint32_t t = threadIdx.x; t < np / 2u; t += blockDim.x) {
+                    uint32_t i, j;
+                    bitonic_pair(t, size, stride, flip, i, j);
+                    if (in_smem) {
+                        unsigned long long ki = s_k[i], kj = s_k[j];
+                        if (ki > kj) {
+                            s_k[i] = kj; s_k[j] = ki;
+                            uint32_t tm = s_m[i]; s_m[i] = s_m[j]; s_m[j] = tm;
+                        }
+                    } else if (j < n) {
+                        unsigned long long ki, kj;
+                        uint32_t mi, mj;
+                        big_load(A, base, n, i, ki, mi);
+                        big_load(A, base, n, j, kj, mj);
+                        if (ki > kj) {
+                            big_store(A, base, i, kj, mj);
+                            big_store(A, base, j, ki, mi);
+                        }
+                    }
+                }
+                __syncthreads();
+            }
+        }
+        if (in_smem) {
+            for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) big_store(A, base, i, s_k[i], s_m[i]);
+            __syncthreads();
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Launch wrappers
+// ---------------------------------------------------------------------------
+void launch_broad(const LaunchCtx& L, const PrepassArgs& A) {
+    k_broad<<<ceil_div_host(L.I, 64), 64, 0, L.stream>>>(L.P, L.inst, A);
+}
+void launch_lut(const LaunchCtx& L, const PrepassArgs& A) {
+    if (L.total_coarse_tiles) k_lut<<<ceil_div_host(L.total_coarse_tiles, 128), 128, 0, L.stream>>>(L.P, A);
+}
+void launch_fine(const LaunchCtx& L, const PrepassArgs& A) {
+    k_fine<<<L.sm_count * 6, kFineThreads, 0, L.stream>>>(L.P, L.inst, A);
+}
+void launch_mark(const LaunchCtx& L, const PrepassArgs& A) {
+    k_traverse<kMark><<<L.sm_count * 8, 256, 0, L.stream>>>(L.P, L.inst, A);
+}
+void launch_alloc(const LaunchCtx& L, const PrepassArgs& A) {
+    k_alloc_pages<<<L.sm_count * 4, kScanThreads, 0, L.stream>>>(L.P, A);
+}
+void launch_zero_pages(const LaunchCtx& L, const PrepassArgs& A) {
+    k_zero_pages<<<L.sm_count * 4, 256, 0, L.stream>>>(A);
+}
+void launch_count(const LaunchCtx& L, const PrepassArgs& A) {
+    k_traverse<kCount><<<L.sm_count * 8, 256, 0, L.stream>>>(L.P, L.inst, A);
+}
+void launch_prefix(const LaunchCtx& L, const PrepassArgs& A) {
+    k_prefix_pages<<<L.sm_count * 6, 256, 0, L.stream>>>(L.P, A);
+}
+void launch_fill(const LaunchCtx& L, const PrepassArgs& A) {
+    k_traverse<kFill><<<L.sm_count * 8, 256, 0, L.stream>>>(L.P, L.inst, A);
+}
+void launch_compact_active(const LaunchCtx& L, const PrepassArgs& A) {
+    k_compact_active<<<L.sm_count * 4, kScanThreads, 0, L.stream>>>(L.P, A);
+}
+void launch_emit(const LaunchCtx& L, const PrepassArgs& A) {
+    k_emit<<<L.sm_count * 6, 256, 0, L.stream>>>(L.P, A);
+}
+void launch_sort_big(const LaunchCtx& L, const PrepassArgs& A) {
+    static bool configured[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64 || !configured[dev]) {
+        cudaFuncSetAttribute(k_sort_big_cells, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBigSmemBytes);
+        if (dev >= 0 && dev < 64) configured[dev] = true;
+    }
+    k_sort_big_cells<<<L.sm_count * 2, 256, kBigSmemBytes, L.stream>>>(A);
+}
+
+}  // namespace fiber

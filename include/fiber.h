@@ -1,0 +1,378 @@
+/*
+ * fiber.h — C ABI of the B200-native strand software-raster path.
+ *
+ * This library replaces the per-frame GPU work of the Fiber Bevy plugin
+ * (RostigerDagmer/bevy_strand_rasterizer): work preparation (broad + fine
+ * prepass, froxel binning), deep-opacity shadow maps with shadow-map
+ * stampback, per-segment hair shading, tile-binned strand rasterisation and
+ * compositing.  Every struct below is byte-for-byte the layout of the
+ * reference's `#[repr(C)]` host mirrors (src/shader_types.rs,
+ * src/pipelines/task_contract.rs, src/components.rs, src/plugin.rs) so a Rust
+ * host can hand its own buffers across the FFI without repacking.
+ *
+ * Conventions
+ *  - All entry points return fiber_status; nothing aborts or traps.
+ *  - `stream` arguments are cudaStream_t passed as void* (NULL = legacy stream).
+ *  - A context is single-threaded (callers synchronise externally); several
+ *    contexts may share one device.
+ *  - Matrices are column-major float[16] (glam Mat4 layout); a matrix-vector
+ *    product is c0*x + c1*y + c2*z + c3*w evaluated left to right.
+ */
+#ifndef FIBER_H
+#define FIBER_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------------ */
+/* Status codes                                                              */
+/* ------------------------------------------------------------------------ */
+typedef enum fiber_status {
+    FIBER_OK = 0,
+    FIBER_EINVAL = 1,     /* bad argument, malformed slab or instance         */
+    FIBER_ENOMEM = 2,     /* device allocation failed or HBM budget exceeded  */
+    FIBER_EOVERFLOW = 3,  /* a device queue overflowed; work was dropped      */
+    FIBER_ETIMEDOUT = 4,  /* a bounded device wait gave up                    */
+    FIBER_ECUDA = 5,      /* a CUDA runtime call failed                       */
+    FIBER_ENOTREADY = 6   /* a node ran before its inputs existed             */
+} fiber_status;
+
+/* ------------------------------------------------------------------------ */
+/* Slab format (bevy_gpu_paging_allocator replacement)                       */
+/* ------------------------------------------------------------------------ */
+/* Slab kinds and their bind ids: src/plugin.rs:129-140 (Vert 0, Index 1,
+ * StrandMaterial 5, StrandGeo 6, StrandMeta 7). */
+typedef enum fiber_slab_kind {
+    FIBER_SLAB_VERT = 0,
+    FIBER_SLAB_INDEX = 1,
+    FIBER_SLAB_MATERIAL = 5,
+    FIBER_SLAB_GEO = 6,
+    FIBER_SLAB_META = 7
+} fiber_slab_kind;
+
+/* DevicePtr: src/shaders/types.wgsl:23-27 ({slab, byte offset, byte size}). */
+typedef struct fiber_devptr {
+    uint32_t slab;
+    uint32_t offset;
+    uint32_t size;
+} fiber_devptr;
+
+/* StrandMeta: src/shader_types.rs:24-31 (16 B). */
+typedef struct fiber_strand_meta {
+    uint32_t count;        /* vertices in the strand                    */
+    uint32_t offset;       /* first position in the index slab          */
+    uint32_t material_idx; /* index into the instance's material slab   */
+    uint32_t pad;
+} fiber_strand_meta;
+
+/* Aabb: src/shader_types.rs:44-51 (32 B). */
+typedef struct fiber_aabb {
+    float min[3];
+    float pad_a;
+    float max[3];
+    float pad_b;
+} fiber_aabb;
+
+/* StrandGeo: src/shader_types.rs:64-73 (64 B). */
+typedef struct fiber_strand_geo {
+    uint32_t strand_count;
+    uint32_t max_segments_in_strand;
+    uint32_t offset;
+    uint32_t pad_b;
+    fiber_aabb aabb;
+    uint32_t pad_c[4];
+} fiber_strand_geo;
+
+/* StrandMaterial: src/components.rs:61-72 (64 B); defaults :74-89. */
+typedef struct fiber_strand_material {
+    float absorption_color[4];
+    float specular_color[4];
+    float ambient_factor;
+    float ao_factor;
+    float eta;
+    float beta;
+    float alpha;
+    float shift;
+    float min_radius_pixels;
+    float max_radius_pixels;
+} fiber_strand_material;
+
+/* StrandInstance: src/shader_types.rs:75-88 (160 B). The *_id fields are
+ * allocation ids returned by fiber_slab_alloc for the matching slab kind. */
+typedef struct fiber_strand_instance {
+    uint32_t vertex_id;
+    uint32_t index_id;
+    uint32_t meta_id;
+    uint32_t geo_id;
+    uint32_t material_id;
+    uint32_t pad0;
+    uint32_t pad1;
+    uint32_t pad2;
+    float world_from_local[16];
+    float local_from_world[16];
+} fiber_strand_instance;
+
+/* ------------------------------------------------------------------------ */
+/* Views, lights and the frustum table                                       */
+/* ------------------------------------------------------------------------ */
+/* FroxelConfig: src/components.rs:93-110 (20 B). */
+typedef struct fiber_froxel_config {
+    uint32_t screen_width;
+    uint32_t screen_height;
+    uint32_t froxel_size_x;
+    uint32_t froxel_size_y;
+    uint32_t depth_slices;
+} fiber_froxel_config;
+
+/* GpuFrustumDesc: src/plugin.rs:1545-1562 (64 B). kind 0 = camera, 1 = light. */
+typedef struct fiber_frustum_desc {
+    uint32_t screen_width;
+    uint32_t screen_height;
+    uint32_t froxel_size_x;
+    uint32_t froxel_size_y;
+    uint32_t depth_slices;
+    uint32_t bucket_base;
+    uint32_t bucket_count;
+    uint32_t kind;
+    uint32_t coarse_depth_tile_base;
+    uint32_t coarse_depth_tile_count;
+    uint32_t coarse_tiles_x;
+    uint32_t coarse_tiles_y;
+    uint32_t cascade_index;
+    uint32_t fine_depth_tile_base;
+    uint32_t pad1;
+    uint32_t pad2;
+} fiber_frustum_desc;
+
+/* The camera fields the path reads from Bevy's View uniform
+ * (view.unjittered_clip_from_world, view.world_position:
+ * src/shaders/strand_prepass.wgsl:446, src/shaders/strand_shading.wgsl:653). */
+typedef struct fiber_camera {
+    float clip_from_world[16];
+    float world_position[3];
+    float pad;
+} fiber_camera;
+
+/* The directional-light fields the path reads from Bevy's Lights uniform:
+ * cascades[c].clip_from_world (one authoritative cascade per light),
+ * direction_to_light and color (linear colour x illuminance)
+ * (src/shaders/strand_prepass.wgsl:443, src/shaders/strand_shading.wgsl:684-688). */
+typedef struct fiber_light {
+    float clip_from_world[16];
+    float direction_to_light[3];
+    float pad0;
+    float color[4];
+} fiber_light;
+
+/* ------------------------------------------------------------------------ */
+/* Queue / task ABI (src/pipelines/task_contract.rs:45-135)                  */
+/* ------------------------------------------------------------------------ */
+typedef struct fiber_queue_header { uint32_t head, tail; } fiber_queue_header;
+typedef struct fiber_fine_prepass_task { uint32_t inst_id, strand_local; } fiber_fine_prepass_task;
+/* packed_field bits: [0..1] level, [2] is_shadow, [3..31] frustum. */
+typedef struct fiber_binning_task { uint32_t id_info, chunk_id, seg_idx, packed_field; } fiber_binning_task;
+typedef struct fiber_projected_segment { uint32_t p0_xy, p1_xy, depths; } fiber_projected_segment;
+typedef struct fiber_raster_work_item {
+    uint32_t seg_ref_base, seg_ref_count, frustum_id, screen_tile_id;
+    uint32_t depth_key, load_score, page_idx, cell_idx;
+} fiber_raster_work_item;
+typedef struct fiber_raster_tile_run {
+    uint32_t work_base, work_count, frustum_id, screen_tile_id;
+    uint32_t load_score, flags, raster_run_reserved_a, raster_run_reserved_b;
+} fiber_raster_tile_run;
+typedef struct fiber_fine_seg_ref { uint32_t inst_id, seg_id, material_idx; } fiber_fine_seg_ref;
+typedef struct fiber_fine_page_meta {
+    uint32_t seg_ref_base, seg_ref_count, work_base, work_count;
+    uint32_t coarse_tile_id, coarse_z, first_depth_key, flags;
+} fiber_fine_page_meta;
+/* GpuCoarseDepthLutEntry: src/plugin.rs:1566-1571. */
+typedef struct fiber_coarse_depth_lut_entry {
+    uint32_t z_min_q, z_max_q, virtual_start_q, virtual_count_q;
+} fiber_coarse_depth_lut_entry;
+/* GpuCoarseAssetRange: src/plugin.rs:1575-1584. */
+typedef struct fiber_coarse_asset_range {
+    uint32_t geo_id, frustum_id, min_x, max_x, min_y, max_y, z_min_q, z_max_q;
+} fiber_coarse_asset_range;
+
+/* ------------------------------------------------------------------------ */
+/* Settings (StochasticCullSettings, PrepassTelemetrySettings,               */
+/* FineBinningBackend: src/resources.rs:70-104; PushConstants                */
+/* src/shader_types.rs:7-22)                                                 */
+/* ------------------------------------------------------------------------ */
+typedef struct fiber_settings {
+    uint32_t stochastic_cull_enabled;   /* default 1                        */
+    float target_strands_per_pixel;     /* default 2.0                      */
+    float min_keep_probability;         /* default 0.02                     */
+    float shadow_keep_probability;      /* default 1.0                      */
+    uint32_t telemetry_enabled;         /* default 0                        */
+    uint32_t fine_binning_backend;      /* 0 = SegmentScatter (only one)    */
+    uint32_t dom_slices;                /* deep-opacity layers K (ref 12)   */
+    uint32_t shadow_map_size;           /* stampback target side; 0 = DOM   */
+    float ambient_color[4];             /* Lights.ambient_color (linear)    */
+    uint32_t history_enabled;           /* temporal shadow history (1)      */
+    uint32_t fragment_counts_enabled;   /* per-pixel fragment counter (0)   */
+    uint32_t ref_capacity_factor;       /* refs = factor x tasks (4)        */
+    uint32_t page_capacity_divisor;     /* pages = table / divisor (1)      */
+} fiber_settings;
+
+/* ------------------------------------------------------------------------ */
+/* Images (headless replacements for the swapchain / view targets)          */
+/* ------------------------------------------------------------------------ */
+typedef enum fiber_format {
+    FIBER_FMT_RGBA16F = 0,  /* 8 B / px  */
+    FIBER_FMT_R32F = 1,     /* 4 B / px  */
+    FIBER_FMT_RGBA32F = 2   /* 16 B / px */
+} fiber_format;
+
+typedef struct fiber_image {
+    void* ptr;          /* device pointer                */
+    uint32_t width;
+    uint32_t height;
+    uint32_t pitch;     /* bytes per row                 */
+    uint32_t format;    /* fiber_format                  */
+} fiber_image;
+
+/* ------------------------------------------------------------------------ */
+/* Per-frame statistics (telemetry counters + overflow words)               */
+/* ------------------------------------------------------------------------ */
+typedef struct fiber_stats {
+    uint32_t frustum_count;
+    uint32_t instance_count;
+    uint32_t binning_tasks;         /* N = sum_f N_f                          */
+    uint32_t camera_tasks;          /* shading queue length                   */
+    uint32_t allocated_pages;
+    uint32_t fine_refs;
+    uint32_t active_tiles;
+    uint32_t camera_runs;
+    uint32_t shadow_runs;
+    uint32_t work_items;
+    uint32_t overflow_flags;        /* bit0 tasks, bit1 pages, bit2 refs, bit3 work */
+    uint32_t timeout_flags;         /* non-zero: a bounded device wait gave up */
+    uint32_t frustum_tasks[8];      /* N_f per frustum (first 8)              */
+    uint32_t frustum_pages[8];
+    uint32_t frustum_refs[8];
+    uint32_t frustum_work[8];
+    uint32_t frustum_runs[8];
+    uint64_t total_segments;        /* segments of all registered instances   */
+    uint64_t total_points;
+    uint64_t total_strands;
+} fiber_stats;
+
+/* What fiber_dump copies back (canonical forms used by parity tests). */
+typedef enum fiber_dump_what {
+    FIBER_DUMP_FRUSTA = 0,        /* fiber_frustum_desc[F]                      */
+    FIBER_DUMP_RANGES = 1,        /* (valid u32 + fiber_coarse_asset_range)[I*F] */
+    FIBER_DUMP_KEEP = 2,          /* float[I*F] per-frustum keep probability    */
+    FIBER_DUMP_LUT = 3,           /* fiber_coarse_depth_lut_entry[T*16]         */
+    FIBER_DUMP_TASKS = 4,         /* fiber_binning_task[N]                      */
+    FIBER_DUMP_PROJECTED = 5,     /* fiber_projected_segment[N]                 */
+    FIBER_DUMP_PAGE_TABLE = 6,    /* u32[T*16] (0 empty, idx+1 allocated)       */
+    FIBER_DUMP_PAGE_META = 7,     /* fiber_fine_page_meta[pages]                */
+    FIBER_DUMP_COUNTS = 8,        /* u32[pages*256] froxel counts               */
+    FIBER_DUMP_OFFSETS = 9,       /* u32[pages*256] exclusive prefix offsets    */
+    FIBER_DUMP_REFS = 10,         /* fiber_fine_seg_ref[R] (canonical order)    */
+    FIBER_DUMP_ACTIVE_TILES = 11, /* u32[A] packed coarse_tile*16+local         */
+    FIBER_DUMP_WORK = 12,         /* fiber_raster_work_item[W]                  */
+    FIBER_DUMP_RUNS = 13,         /* fiber_raster_tile_run[runs] camera then shadow */
+    FIBER_DUMP_DOM_DEPTH = 14,    /* float[L*D*D]                               */
+    FIBER_DUMP_DOM_OPACITY = 15,  /* float[L*K*D*D]                             */
+    FIBER_DUMP_SHADOW_MAP = 16,   /* float[L*S*S] stampback target              */
+    FIBER_DUMP_ATLAS = 17,        /* half[I*cap*4] shading atlas                */
+    FIBER_DUMP_HISTORY = 18,      /* half[I*cap*2] shadow history (next)        */
+    FIBER_DUMP_COLOR = 19,        /* half[W*H*4] strand colour (RGBA16F)        */
+    FIBER_DUMP_DEPTH = 20,        /* float[W*H] strand depth                    */
+    FIBER_DUMP_FRAGMENTS = 21     /* u32[W*H] per-pixel fragment counts         */
+} fiber_dump_what;
+
+typedef struct fiber_ctx fiber_ctx;
+
+/* ------------------------------------------------------------------------ */
+/* Plugin API (StrandRasterizerPlugin::build/finish, src/plugin.rs:162-262)  */
+/* ------------------------------------------------------------------------ */
+/* Create a context on `device`. hbm_budget bytes caps the context's device
+ * allocations (0 = no cap). */
+fiber_status fiber_ctx_create(int device, uint64_t hbm_budget, fiber_ctx** out);
+fiber_status fiber_ctx_destroy(fiber_ctx* ctx);
+/* Mirrors StochasticCullSettings / PrepassTelemetrySettings /
+ * FineBinningBackend (src/resources.rs:70-104). */
+fiber_status fiber_settings_default(fiber_settings* out);
+fiber_status fiber_settings_set(fiber_ctx* ctx, const fiber_settings* settings);
+
+/* ------------------------------------------------------------------------ */
+/* Slabs (VirtualShaderStorageBuffer per SlabKind, src/plugin.rs:1395-1440)  */
+/* ------------------------------------------------------------------------ */
+/* Allocates `bytes` of slab `kind`; returns the allocation id (the id a
+ * StrandInstance stores) and its DevicePtr. */
+fiber_status fiber_slab_alloc(fiber_ctx* ctx, uint32_t kind, uint64_t bytes,
+                              uint32_t* alloc_id, fiber_devptr* out);
+fiber_status fiber_slab_upload(fiber_ctx* ctx, uint32_t kind, uint32_t alloc_id,
+                               uint64_t dst_offset, const void* host, uint64_t bytes,
+                               void* stream);
+fiber_status fiber_slab_free(fiber_ctx* ctx, uint32_t kind, uint32_t alloc_id);
+
+/* Registers the StrandInstance table (src/plugin.rs:284-315). Validates every
+ * referenced slab on the device (indices < vertices, strand ranges inside the
+ * index slab, material indices) and rejects malformed instances with EINVAL,
+ * mirroring validate_cache (src/strand_cache.rs:174-209). */
+fiber_status fiber_instance_set(fiber_ctx* ctx, const fiber_strand_instance* rows, uint32_t n);
+
+/* ------------------------------------------------------------------------ */
+/* Per-frame host preparation (use_prepass_buffers, src/plugin.rs:264-1209)  */
+/* ------------------------------------------------------------------------ */
+/* Builds the frustum table (camera first, then one frustum per light, in the
+ * order given), sizes every queue, and uploads the frame tables on `stream`. */
+fiber_status fiber_frame_begin(fiber_ctx* ctx,
+                               const fiber_froxel_config* camera_cfg,
+                               const fiber_camera* camera,
+                               const fiber_froxel_config* light_cfgs,
+                               const fiber_light* lights, uint32_t n_lights,
+                               void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Render-graph node contracts (src/nodes/<node>.rs)                         */
+/* ------------------------------------------------------------------------ */
+/* work_preparation_pass (src/nodes/prepass.rs:27-233). */
+fiber_status fiber_prepass(fiber_ctx* ctx, void* stream);
+/* strand_shadow_rasterizer_pass incl. stampback (src/nodes/shadows.rs:29-221). */
+fiber_status fiber_shadows(fiber_ctx* ctx, void* stream);
+/* strand_shading_pass (src/nodes/shading.rs:25-155); flips the history. */
+fiber_status fiber_shading(fiber_ctx* ctx, void* stream);
+/* strand_rasterizer_pass (src/nodes/raster.rs:26-179). */
+fiber_status fiber_raster(fiber_ctx* ctx, uint32_t view, void* stream);
+/* composition_pass (src/nodes/composite.rs:19-131): per-pixel depth test and
+ * alpha mix of the strand image into scene_color, ALPHA_BLENDING onto `out`
+ * (loaded). scene_depth may be NULL (no opaque scene: depth 0). */
+fiber_status fiber_composite(fiber_ctx* ctx, uint32_t view, const fiber_image* scene_color,
+                             const fiber_image* scene_depth, fiber_image* out, void* stream);
+/* All nodes of one frame in order, replayed from a CUDA graph after the first
+ * call with the same frame shape. */
+fiber_status fiber_frame_fused(fiber_ctx* ctx, const fiber_image* scene_color,
+                               const fiber_image* scene_depth, fiber_image* out, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Readback                                                                  */
+/* ------------------------------------------------------------------------ */
+/* Synchronises the context's last stream and returns the frame counters
+ * (telemetry words, src/pipelines/prepass.rs:1345-1396). */
+fiber_status fiber_stats_get(fiber_ctx* ctx, fiber_stats* out);
+/* Copies one canonical buffer to host memory. With host == NULL only
+ * *written receives the byte size. */
+fiber_status fiber_dump(fiber_ctx* ctx, uint32_t what, void* host, uint64_t capacity,
+                        uint64_t* written);
+/* Device pointers of the context-owned outputs (strand colour RGBA16F, strand
+ * depth R32F, DOM layers, stampback target) for zero-copy consumers. */
+fiber_status fiber_output_image(fiber_ctx* ctx, uint32_t what, fiber_image* out);
+/* Per-stage device times of the last frame in ms, named like the reference's
+ * diagnostic spans; returns the number of spans written. */
+uint32_t fiber_span_count(void);
+const char* fiber_span_name(uint32_t i);
+fiber_status fiber_span_times(fiber_ctx* ctx, float* ms, uint32_t n);
+const char* fiber_status_string(fiber_status s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FIBER_H */

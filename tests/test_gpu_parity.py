@@ -1,0 +1,125 @@
+"""CUDA path vs the oracle on identical seeded inputs, through the C ABI.
+
+Integer and index outputs (frustum table, coarse ranges, keep probabilities,
+depth-warp LUT, binning tasks, projected segments, page table and metadata,
+froxel counts, prefix offsets, canonical fine refs, active tiles, raster work
+items, tile runs, per-pixel fragment counts) must match bit for bit. Shaded
+colour, shading atlas and deep-shadow opacity must agree within max-abs 2e-3
+and PSNR >= 50 dB in FP32 (the DOM stages use no transcendental functions and
+are compared exactly).
+"""
+import numpy as np
+import pytest
+
+from bevy_strand_rasterizer_b200 import abi
+from common import build_scene, psnr, run_gpu, run_ref
+
+pytestmark = pytest.mark.gpu
+
+TOL_ABS = 2e-3
+TOL_PSNR = 50.0
+
+EXACT = [
+    abi.DUMP_FRUSTA, abi.DUMP_RANGES, abi.DUMP_KEEP, abi.DUMP_LUT, abi.DUMP_TASKS, abi.DUMP_PROJECTED,
+    abi.DUMP_PAGE_TABLE, abi.DUMP_PAGE_META, abi.DUMP_COUNTS, abi.DUMP_OFFSETS, abi.DUMP_REFS,
+    abi.DUMP_ACTIVE_TILES, abi.DUMP_WORK, abi.DUMP_RUNS, abi.DUMP_DOM_DEPTH, abi.DUMP_DOM_OPACITY,
+    abi.DUMP_SHADOW_MAP, abi.DUMP_FRAGMENTS,
+]
+NAMES = {v: k for k, v in vars(abi).items() if k.startswith("DUMP_") and isinstance(v, int)}
+
+
+def _exact(gpu, ref, what):
+    g = gpu.view(np.uint8)
+    r = ref.view(np.uint8)
+    assert g.shape == r.shape, f"{NAMES[what]}: size {g.shape} vs oracle {r.shape}"
+    if not np.array_equal(g, r):
+        gv, rv = gpu.reshape(-1), ref.reshape(-1)
+        bad = np.nonzero(gv != rv)[0]
+        raise AssertionError(f"{NAMES[what]}: {bad.size} of {gv.size} records differ; first {bad[:5]}: "
+                             f"gpu {gv[bad[:3]]} oracle {rv[bad[:3]]}")
+
+
+def _close(gpu, ref, what, mask=None):
+    g = gpu.astype(np.float32).reshape(-1)
+    r = ref.astype(np.float32).reshape(-1)
+    assert g.shape == r.shape
+    if mask is not None:
+        g, r = g[mask], r[mask]
+    assert np.array_equal(np.isnan(g), np.isnan(r)), f"{NAMES[what]}: NaN pattern differs"
+    ok = ~np.isnan(g)
+    err = float(np.max(np.abs(g[ok] - r[ok]))) if ok.any() else 0.0
+    p = psnr(g[ok], r[ok]) if ok.any() else float("inf")
+    assert err <= TOL_ABS and p >= TOL_PSNR, f"{NAMES[what]}: max abs {err:.3g}, PSNR {p:.1f} dB"
+    return err, p
+
+
+def _compare(scene, fused=False):
+    plugin = run_gpu(scene, fused=fused)
+    ref = run_ref(scene)
+    s = plugin.stats()
+    rs = ref.stats()
+    for k in ("binning_tasks", "camera_tasks", "allocated_pages", "fine_refs", "active_tiles", "camera_runs",
+              "shadow_runs", "work_items", "overflow_flags"):
+        assert getattr(s, k) == getattr(rs, k), f"stat {k}: gpu {getattr(s, k)} oracle {getattr(rs, k)}"
+    for what in EXACT:
+        if what == abi.DUMP_FRAGMENTS and not scene.settings.fragment_counts_enabled:
+            continue
+        _exact(plugin.dump(what), ref.get(what), what)
+    # Shading atlas / history: compare the texels this frame wrote.
+    ga, ra = plugin.dump(abi.DUMP_ATLAS).reshape(-1, 4), ref.get(abi.DUMP_ATLAS).reshape(-1, 4)
+    written = ra.astype(np.float32)[:, 3] > 0
+    _close(ga[written], ra[written], abi.DUMP_ATLAS)
+    gh, rh = plugin.dump(abi.DUMP_HISTORY).reshape(-1, 2), ref.get(abi.DUMP_HISTORY).reshape(-1, 2)
+    _close(gh[written], rh[written], abi.DUMP_HISTORY)
+    _close(plugin.dump(abi.DUMP_COLOR), ref.get(abi.DUMP_COLOR), abi.DUMP_COLOR)
+    _close(plugin.dump(abi.DUMP_DEPTH), ref.get(abi.DUMP_DEPTH), abi.DUMP_DEPTH)
+    plugin.close()
+    return s
+
+
+@pytest.mark.parametrize("name", ["tiny", "small"])
+def test_parity_default(name):
+    scene = build_scene(name, settings_overrides={"fragment_counts_enabled": 1})
+    s = _compare(scene)
+    assert s.binning_tasks > 0 and s.fine_refs > 0 and s.camera_runs > 0 and s.shadow_runs > 0
+
+
+def test_parity_fused_graph():
+    scene = build_scene("tiny", settings_overrides={"fragment_counts_enabled": 1})
+    _compare(scene, fused=True)
+
+
+def test_parity_unsaturated_shading():
+    # A dim light keeps the shaded colour inside (0, 1) so the Marschner terms
+    # are compared before the unorm clamp.
+    scene = build_scene("tiny", illuminance=0.02)
+    _compare(scene)
+
+
+def test_parity_no_cull_two_lights_orbit():
+    scene = build_scene("tiny", frame=37, cull=False, lights=[(1.0, 1.0, 1.0), (-1.0, 1.0, 0.5)])
+    _compare(scene)
+
+
+def test_parity_ref_overflow():
+    # A tiny reference budget overflows pages exactly like the oracle's.
+    scene = build_scene("tiny", settings_overrides={"ref_capacity_factor": 1})
+    plugin = run_gpu(scene)
+    ref = run_ref(scene)
+    s = plugin.stats(allow_overflow=True)
+    assert s.overflow_flags & 4 and ref.stats().overflow_flags & 4
+    for what in (abi.DUMP_PAGE_META, abi.DUMP_COUNTS, abi.DUMP_ACTIVE_TILES, abi.DUMP_RUNS, abi.DUMP_WORK):
+        _exact(plugin.dump(what), ref.get(what), what)
+    plugin.close()
+
+
+def test_deterministic_repeat():
+    # History off: with it on, frame 2 legitimately blends frame 1's visibility.
+    scene = build_scene("small", settings_overrides={"history_enabled": 0})
+    p = run_gpu(scene)
+    first = {w: p.dump(w).copy() for w in (abi.DUMP_REFS, abi.DUMP_WORK, abi.DUMP_COLOR, abi.DUMP_DOM_OPACITY)}
+    for _ in range(2):
+        run_gpu(scene, plugin=p)
+        for w, v in first.items():
+            assert np.array_equal(p.dump(w).view(np.uint8), v.view(np.uint8)), NAMES[w]
+    p.close()
