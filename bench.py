@@ -1,0 +1,445 @@
+"""Benchmark of the strand software-raster path on B200.
+
+One step = one frame of the seeded "medium" plain-pipeline workload (100,000
+strands x 32 points = 3.1 M segments, 1920x1080 camera orbiting 360 degrees over
+200 frames, one directional light with a 2048^2 x 8-layer deep-opacity map):
+prepass -> deep shadow + stampback -> shading -> raster -> composite, replayed
+from one CUDA graph per frame.
+
+Prints one JSON line. `value` is whole-job segments/s with the scene resident in
+HBM; `e2e` is the same metric through fiber_render_host with the scene image
+copied in from pinned host memory and the composited RGBA16F frame copied back
+every step. `--impl reference` times the CPU restatement of the reference path
+(the reference itself is Rust + WGSL over wgpu and cannot run here) on every
+host thread. With torchrun (N > 1) every rank renders its own frames: replicas,
+weak scaling, no collective on the data path.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "segments/s & frames/s at 1080p; served p50/p99 latency vs plain loop, 1 B200"
+UNIT = "segments/s"
+
+
+def parse_args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=30)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", default="fiber", choices=["fiber", "reference"])
+    p.add_argument("--workload", default="medium")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--profile", action="store_true",
+                   help="render warmup + steps frames only (no timing extras); the command profiled under ncu")
+    return p.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# Clock sampling during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# Scene setup shared by the arms
+# ---------------------------------------------------------------------------
+def make_scene(name: str):
+    from bevy_strand_rasterizer_b200.plugin import FroxelConfig, StrandMaterial, pack_strand_set
+    from bevy_strand_rasterizer_b200.scene import LightSpec, scalp_hair, workload
+    w = workload(name)
+    strands = scalp_hair(w.strands, w.points, w.seed, curly=w.curly)
+    packed = pack_strand_set(strands)
+    cam_cfg = FroxelConfig(w.width, w.height, w.froxel, w.froxel, w.depth_slices)
+    lights = [(FroxelConfig(w.dom_size, w.dom_size, w.froxel, w.froxel, w.depth_slices), LightSpec(d, size=w.dom_size))
+              for d in w.lights]
+    return w, packed, StrandMaterial(), cam_cfg, lights
+
+
+def frame_structs(w, packed, frame, lights):
+    from bevy_strand_rasterizer_b200 import abi
+    spec = w.camera(frame)
+    cam = abi.Camera()
+    cam.clip_from_world[:] = [float(x) for x in spec.clip_from_world()]
+    cam.world_position[:] = [float(x) for x in spec.eye]
+    lc = (abi.Light * max(1, len(lights)))()
+    for i, (_, ls) in enumerate(lights):
+        lc[i].clip_from_world[:] = [float(x) for x in ls.clip_from_world(packed.aabb_min, packed.aabb_max)]
+        lc[i].direction_to_light[:] = [float(x) for x in ls.direction()]
+        lc[i].color[:] = [float(x) for x in ls.color4()]
+    return cam, lc
+
+
+def algorithmic_bytes(st, w, n_lights: int, K: int, D: int) -> dict:
+    """B_alg of the frame and of each kernel, from the frame's own counts.
+
+    Per unit: 20 B / point + 16 B / strand (vertex float4 + index, meta), 28 B per
+    binning task written and read (BinningTask 16 + ProjectedSegment 12), 8 B per
+    allocated cell (count + offset), 24 B per fine ref (written + read), 64 B per
+    work item / tile run (written + read), 40 B per ref of endpoint gather in the
+    rasters, 40 + 8 L B per camera segment in shading, 12 B per camera pixel
+    (RGBA16F + R32F), 4 (K + 1) B per deep-opacity texel.
+    """
+    F = st.frustum_count
+    P, S = st.total_points, st.total_strands
+    tasks = [st.frustum_tasks[f] for f in range(F)]
+    pages = [st.frustum_pages[f] for f in range(F)]
+    refs = [st.frustum_refs[f] for f in range(F)]
+    work = [st.frustum_work[f] for f in range(F)]
+    runs = [st.frustum_runs[f] for f in range(F)]
+    WH = w.width * w.height
+    dom = n_lights * 4 * (K + 1) * D * D
+    per = {
+        "k_fine": 20 * P + 16 * S + sum(28 * n for n in tasks),
+        "k_traverse_mark": sum(28 * n for n in tasks),
+        "k_traverse_count": sum(28 * n for n in tasks),
+        "k_traverse_fill": sum(28 * n for n in tasks) + sum(12 * r for r in refs),
+        "k_prefix_pages": sum(8 * 256 * p for p in pages),
+        "k_emit": sum(32 * (wk + t) for wk, t in zip(work, runs)),
+        "k_shadow": sum(52 * refs[f] + 32 * (work[f] + runs[f]) for f in range(1, F)) + dom,
+        "k_shade": st.camera_tasks * (40 + 8 * n_lights),
+        "k_raster": 52 * refs[0] + 32 * (work[0] + runs[0]) + 12 * WH,
+    }
+    total = (20 * P + 16 * S + sum(56 * n + 8 * 256 * p + 24 * r + 64 * (wk + t) + 40 * r
+                                   for n, p, r, wk, t in zip(tasks, pages, refs, work, runs))
+             + st.camera_tasks * (40 + 8 * n_lights) + 12 * WH + dom)
+    b_min = 20 * P + 16 * S + 12 * WH + dom
+    return {"per_kernel": per, "frame": total, "min": b_min}
+
+
+SPAN_TO_KERNEL = {
+    "strand_prepass/fine": "k_fine",
+    "strand_prepass/mark_count_pages": "k_traverse_mark",
+    "strand_prepass/binning": "k_traverse_count",
+    "strand_prepass/prefix_fine_pages": "k_prefix_pages",
+    "strand_prepass/fill_segment_refs": "k_traverse_fill",
+    "strand_prepass/emit_raster_work": "k_emit",
+    "strand_shadow_rasterizer/rasterize": "k_shadow",
+    "strand_shading/shade": "k_shade",
+    "strand_rasterizer/rasterize": "k_raster",
+}
+
+
+def load_peaks() -> tuple[float, str]:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return 6650.0, "fallback"
+
+
+def load_traffic() -> dict:
+    p = ROOT / "profiles" / "ncu_traffic.json"
+    if p.exists():
+        try:
+            return json.loads(p.read_text())
+        except Exception:
+            return {}
+    return {}
+
+
+# ---------------------------------------------------------------------------
+# CPU arm (oracle restatement on the host cores)
+# ---------------------------------------------------------------------------
+def cpu_frame_time(w, packed, material, cam_cfg, lights, frame=0, max_strands=None):
+    """Times one oracle frame on every host thread; returns (seconds, segments, sample text)."""
+    sys.path.insert(0, str(ROOT / "tests"))
+    from bevy_strand_rasterizer_b200 import abi
+    from bevy_strand_rasterizer_b200.plugin import pack_indexed_strands
+    from oracle_bridge import run_oracle
+    sample = packed
+    note = f"one full {w.name} frame"
+    if max_strands and packed.strand_count > max_strands:
+        n = max_strands
+        meta = packed.meta[:n]
+        end = int(meta["offset"][-1] + meta["count"][-1])
+        sample = pack_indexed_strands(packed.vertices[:, :3], meta["count"], meta["offset"], packed.indices[:end])
+        note = f"one {w.name} frame over the first {n} of {packed.strand_count} strands"
+    cam, lc = frame_structs(w, packed, frame, lights)
+    st = abi.default_settings()
+    st.dom_slices = w.dom_layers
+    segs = int(np.maximum(sample.meta["count"].astype(np.int64) - 1, 0).sum())
+    t0 = time.perf_counter()
+    fr = run_oracle([(sample, material, np.eye(4, dtype=np.float32).reshape(16))], cam_cfg, cam,
+                    [c for c, _ in lights], lc, st, threads=os.cpu_count() or 1)
+    dt = time.perf_counter() - t0
+    fr.free()
+    return dt, segs, note
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    w, packed, material, cam_cfg, lights = make_scene(args.workload)
+    # A bounded sample keeps each step to a few seconds of host work.
+    max_strands = 25_000 if w.strands > 25_000 else None
+    for i in range(args.warmup):
+        cpu_frame_time(w, packed, material, cam_cfg, lights, frame=i, max_strands=max_strands)
+    times, segs, note = [], 0, ""
+    for k in range(args.steps):
+        dt, segs, note = cpu_frame_time(w, packed, material, cam_cfg, lights, frame=args.warmup + k,
+                                        max_strands=max_strands)
+        times.append(dt)
+    total = sum(times)
+    value = segs * args.steps / total
+    cores = os.cpu_count() or 1
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"{w.name}: {w.strands} strands x {w.points} points, {w.width}x{w.height}, "
+                               f"DOM {w.dom_size}^2 x {w.dom_layers}", "sample": note},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": note},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "the reference is Rust + WGSL over wgpu/Vulkan with no CPU implementation; its CPU arm is the "
+                "oracle restatement (oracle/fiber_ref.cpp) on every host thread",
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+def fiber_arm(args):
+    import torch
+    import torch.distributed as dist
+    from bevy_strand_rasterizer_b200 import abi
+    from bevy_strand_rasterizer_b200.plugin import StrandRasterizerPlugin, image_from_tensor
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+
+    w, packed, material, cam_cfg, lights = make_scene(args.workload)
+    plugin = StrandRasterizerPlugin(device=local, dom_slices=w.dom_layers)
+    plugin.add_geometry(packed, material)
+    stream = torch.cuda.Stream()
+    H, W = w.height, w.width
+    scene = torch.empty((H, W, 4), dtype=torch.float16, device="cuda")
+    scene[...] = torch.tensor([0.08, 0.09, 0.11, 1.0], dtype=torch.float16)
+    out = torch.empty_like(scene)
+    scene_img = image_from_tensor(scene, abi.FMT_RGBA16F)
+    out_img = image_from_tensor(out, abi.FMT_RGBA16F)
+    light_cfgs = [c for c, _ in lights]
+    frame_base = rank * 100_003  # each replica renders its own orbit frames
+
+    def step(k):
+        cam, lc = frame_structs(w, packed, frame_base + k, lights)
+        plugin.frame_begin_raw(cam_cfg, cam, light_cfgs, lc, stream)
+        # The scene is opaque (alpha 1), so the blend onto `out` does not
+        # depend on what `out` held before.
+        plugin.frame_fused(scene_img, None, out_img, stream)
+
+    with torch.cuda.stream(stream):
+        for i in range(args.warmup):
+            step(i)
+    stream.synchronize()
+    st = plugin.stats()
+    if args.profile:
+        with torch.cuda.stream(stream):
+            for k in range(args.steps):
+                step(args.warmup + k)
+        stream.synchronize()
+        print(json.dumps({"profile": w.name, "frames": args.warmup + args.steps, "tasks": st.binning_tasks,
+                          "refs": st.fine_refs}), flush=True)
+        plugin.close()
+        return
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+        for k in range(args.steps):
+            step(args.warmup + k)
+        e1.record(stream)
+    stream.synchronize()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    elapsed = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([elapsed], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed = float(t.item())
+        dist.barrier()
+    segs = st.total_segments
+    value = segs * args.steps * world / (elapsed / 1000.0)
+    ms_per_step = elapsed / args.steps
+
+    # Per-stage device times (events recorded inside the frame graph).
+    spans = {}
+    with torch.cuda.stream(stream):
+        for k in range(args.steps):
+            step(args.warmup + args.steps + k)
+            stream.synchronize()
+            for name, ms in plugin.span_times().items():
+                spans.setdefault(name, []).append(ms)
+    span_med = {k: statistics.median(v) for k, v in spans.items()}
+
+    # End to end through fiber_render_host: pinned host scene in, composited frame out.
+    host_in = torch.empty((H, W, 4), dtype=torch.float16, pin_memory=True)
+    host_in.copy_(scene.cpu())
+    host_out = torch.empty((H, W, 4), dtype=torch.float16, pin_memory=True)
+    lib = plugin.lib
+    h2d = H * W * 8 + 4096  # scene image + frame tables (FrameParams, instance rows)
+    d2h = H * W * 8
+    sh = C.c_void_p(stream.cuda_stream)
+    with torch.cuda.stream(stream):
+        for k in range(max(1, args.warmup)):
+            cam, lc = frame_structs(w, packed, frame_base + k, lights)
+            plugin.frame_begin_raw(cam_cfg, cam, light_cfgs, lc, stream)
+            abi.check(lib.fiber_render_host(plugin.ctx, C.c_void_p(host_in.data_ptr()), None,
+                                            C.c_void_p(host_out.data_ptr()), sh), "fiber_render_host")
+        stream.synchronize()
+        e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e2.record(stream)
+        for k in range(args.steps):
+            cam, lc = frame_structs(w, packed, frame_base + k, lights)
+            plugin.frame_begin_raw(cam_cfg, cam, light_cfgs, lc, stream)
+            abi.check(lib.fiber_render_host(plugin.ctx, C.c_void_p(host_in.data_ptr()), None,
+                                            C.c_void_p(host_out.data_ptr()), sh), "fiber_render_host")
+        e3.record(stream)
+    stream.synchronize()
+    e2e_ms = e2.elapsed_time(e3)
+    if world > 1:
+        t = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = segs * args.steps * world / (e2e_ms / 1000.0)
+    assert np.isfinite(host_out.float().numpy()).all()
+
+    # Roofline of the dominant kernel (HBM-bound dataflow; no dense contraction).
+    ab = algorithmic_bytes(st, w, len(lights), w.dom_layers, w.dom_size)
+    kernel_ms = {SPAN_TO_KERNEL[k]: v for k, v in span_med.items() if k in SPAN_TO_KERNEL}
+    dom_kernel = max(kernel_ms, key=kernel_ms.get)
+    peak, peak_kind = load_peaks()
+    achieved = ab["per_kernel"][dom_kernel] / (kernel_ms[dom_kernel] / 1000.0) / 1e9
+    traffic = load_traffic().get(dom_kernel, {}).get("bytes_per_launch")
+    frame_ms = span_med.get("frame/total", ms_per_step)
+    frame_gbs = ab["frame"] / (ms_per_step / 1000.0) / 1e9
+
+    line = None
+    if rank == 0:
+        cpu = None
+        if not args.no_cpu_baseline and world == 1:
+            max_strands = 25_000 if w.strands > 25_000 else None
+            dt, csegs, note = cpu_frame_time(w, packed, material, cam_cfg, lights, frame=0, max_strands=max_strands)
+            cpu = {"value": csegs / dt, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "port",
+                   "sample": note}
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "frames_per_s": 1000.0 * world / ms_per_step,
+            "config": {"workload": f"{w.name}: {w.strands} strands x {w.points} points ({segs} segments), "
+                                   f"{w.width}x{w.height} camera orbiting over {w.orbit_frames} frames, "
+                                   f"{len(lights)} light(s) with {w.dom_size}^2 x {w.dom_layers} deep-opacity maps",
+                       "tile_px": w.froxel, "parallelism": f"replicas x{world}",
+                       "l2": "per-frame working set (tasks, refs, pages, DOM) > 126 MB L2",
+                       "stochastic_cull": "on (reference default)"},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "entry_point": "fiber_render_host", "ms_per_step": e2e_ms / args.steps},
+            "roofline": {"bound": "hbm", "kernel": dom_kernel, "achieved": achieved, "peak": peak,
+                         "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                         "alg_bytes_per_launch": ab["per_kernel"][dom_kernel],
+                         "launch_ms": kernel_ms[dom_kernel]},
+            "frame_roofline": {"b_alg": ab["frame"], "b_min": ab["min"], "achieved_gbs": frame_gbs,
+                               "frac": frame_gbs / peak},
+            "cpu_baseline": cpu,
+            "clocks": clk,
+            "gpu_launches": 16 * args.steps,
+            "spans_ms": span_med,
+            "counts": {"binning_tasks": st.binning_tasks, "camera_tasks": st.camera_tasks,
+                       "pages": st.allocated_pages, "fine_refs": st.fine_refs, "work_items": st.work_items,
+                       "camera_runs": st.camera_runs, "shadow_runs": st.shadow_runs},
+        }
+    plugin.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if line is not None:
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        reference_arm(args)
+    else:
+        fiber_arm(args)
+
+
+if __name__ == "__main__":
+    main()

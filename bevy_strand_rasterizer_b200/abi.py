@@ -138,7 +138,7 @@ EXPORTS = [
     "fiber_ctx_create", "fiber_ctx_destroy", "fiber_settings_default", "fiber_settings_set",
     "fiber_slab_alloc", "fiber_slab_upload", "fiber_slab_free", "fiber_instance_set", "fiber_frame_begin",
     "fiber_prepass", "fiber_shadows", "fiber_shading", "fiber_raster", "fiber_composite", "fiber_frame_fused",
-    "fiber_stats_get", "fiber_dump", "fiber_output_image", "fiber_span_count", "fiber_span_name",
+    "fiber_render_host", "fiber_stats_get", "fiber_dump", "fiber_output_image", "fiber_span_count", "fiber_span_name",
     "fiber_span_times", "fiber_status_string",
 ]
 
@@ -177,6 +177,7 @@ def load_library(path: Path | str | None = None) -> C.CDLL:
         "fiber_raster": (C.c_int, [vp, u32, vp]),
         "fiber_composite": (C.c_int, [vp, u32, pp(Image), pp(Image), pp(Image), vp]),
         "fiber_frame_fused": (C.c_int, [vp, pp(Image), pp(Image), pp(Image), vp]),
+        "fiber_render_host": (C.c_int, [vp, vp, vp, vp, vp]),
         "fiber_stats_get": (C.c_int, [vp, pp(Stats)]),
         "fiber_dump": (C.c_int, [vp, u32, vp, C.c_uint64, pp(C.c_uint64)]),
         "fiber_output_image": (C.c_int, [vp, u32, pp(Image)]),

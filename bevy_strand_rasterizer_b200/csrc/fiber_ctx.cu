@@ -62,8 +62,8 @@ int kind_slot(uint32_t kind) {
 
 // Checks one instance's slabs on the device: every index < vertex count, every
 // strand range inside the index slab, every material index inside the material
-// slab (validate_cache, src/strand_cache.rs:174-209). out: [errors, segments
-// lo, segments hi, max count].
+// slab (validate_cache, src/strand_cache.rs:174-209). out: u32 errors at byte
+// 0, u32 max count at byte 4, u64 segment total at byte 8 (8-byte aligned).
 __global__ void k_validate(InstanceView v, uint32_t* out) {
     const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
     for (uint32_t j = tid; j < v.n_indices; j += stride)
@@ -78,8 +78,8 @@ __global__ void k_validate(InstanceView v, uint32_t* out) {
         segs += m.count - 1u;
         maxc = max(maxc, m.count);
     }
-    atomicAdd(reinterpret_cast<unsigned long long*>(out + 1), segs);
-    atomicMax(out + 3, maxc);
+    atomicMax(out + 1, maxc);
+    atomicAdd(reinterpret_cast<unsigned long long*>(out + 2), segs);
 }
 
 }  // namespace
@@ -107,7 +107,7 @@ struct fiber_ctx {
     DevBuf d_lut, d_tasks, d_projected, d_page_table, d_page_meta, d_counts, d_offsets, d_cursors;
     DevBuf d_refs, d_ref_keys, d_active_flags, d_active_list, d_work, d_runs, d_big_cells;
     DevBuf d_dom_depth, d_dom_opacity, d_shadow_map, d_atlas, d_history[2];
-    DevBuf d_color, d_depth, d_fragments, d_validate;
+    DevBuf d_color, d_depth, d_fragments, d_validate, d_host_scene, d_host_depth;
     int hist_cur = 0;
     // timing
     cudaEvent_t ev[kSpanCount + 1] = {};
@@ -228,8 +228,21 @@ RenderArgs render_args(fiber_ctx* c) {
     return R;
 }
 
+// Span events: while a stream is being captured they are recorded as external
+// event nodes, so they keep timing the frame when it is replayed from the CUDA
+// graph; otherwise they are plain records. A failed record only disables the
+// spans; it never leaves an error behind for the node that called it.
 void record(fiber_ctx* c, int span, cudaStream_t s) {
-    if (c->events_ok) cudaEventRecord(c->ev[span], s);
+    if (!c->events_ok) return;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (s && cudaStreamIsCapturing(s, &cs) != cudaSuccess) cs = cudaStreamCaptureStatusNone;
+    cudaError_t e = cs == cudaStreamCaptureStatusActive
+                        ? cudaEventRecordWithFlags(c->ev[span], s, cudaEventRecordExternal)
+                        : cudaEventRecord(c->ev[span], s);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        c->events_ok = false;
+    }
 }
 
 fiber_status check_launch() {
@@ -271,7 +284,7 @@ fiber_status run_prepass(fiber_ctx* c, cudaStream_t s) {
 
 fiber_status run_shadows(fiber_ctx* c, cudaStream_t s) {
     record(c, 9, s);
-    if (c->P.L) launch_shadow(launch_ctx(c, s), render_args(c));
+    if (c->P.L) launch_shadow(launch_ctx(c, s), render_args(c), c->P.K);
     return check_launch();
 }
 
@@ -302,6 +315,14 @@ fiber_status run_composite(fiber_ctx* c, const fiber_image* scene_color, const f
     if (scene_color->format == FIBER_FMT_R32F || out->format == FIBER_FMT_R32F) return FIBER_EINVAL;
     if (scene_depth && (scene_depth->format != FIBER_FMT_R32F || scene_depth->width != c->P.width ||
                         scene_depth->height != c->P.height))
+        return FIBER_EINVAL;
+    // Vector loads need 8 B (RGBA16F) / 16 B (RGBA32F) / 4 B (R32F) aligned rows.
+    auto aligned = [](const fiber_image* im, uint32_t px_bytes) {
+        uint32_t pitch = im->pitch ? im->pitch : im->width * px_bytes;
+        return ((uintptr_t)im->ptr % px_bytes) == 0 && pitch % px_bytes == 0 && pitch >= im->width * px_bytes;
+    };
+    if (!aligned(scene_color, fmt_bytes(scene_color->format)) || !aligned(out, fmt_bytes(out->format)) ||
+        (scene_depth && !aligned(scene_depth, 4u)))
         return FIBER_EINVAL;
     CompositeArgs C{};
     C.strand_color = dp<__half>(c->d_color);
@@ -401,7 +422,7 @@ fiber_status fiber_ctx_destroy(fiber_ctx* c) {
                       &c->d_ref_keys, &c->d_active_flags, &c->d_active_list, &c->d_work, &c->d_runs,
                       &c->d_big_cells, &c->d_dom_depth, &c->d_dom_opacity, &c->d_shadow_map, &c->d_atlas,
                       &c->d_history[0], &c->d_history[1], &c->d_color, &c->d_depth, &c->d_fragments,
-                      &c->d_validate};
+                      &c->d_validate, &c->d_host_scene, &c->d_host_depth};
     for (DevBuf* b : bufs) release(c, *b);
     for (int i = 0; i <= kSpanCount; ++i)
         if (c->ev[i]) cudaEventDestroy(c->ev[i]);
@@ -512,7 +533,7 @@ fiber_status fiber_instance_set(fiber_ctx* c, const fiber_strand_instance* rows,
         uint32_t res[4];
         FIBER_CUDA(cudaMemcpy(res, c->d_validate.p, 16, cudaMemcpyDeviceToHost));
         if (res[0] != 0u) return FIBER_EINVAL;
-        segs[i] = (uint64_t)res[1] | ((uint64_t)res[2] << 32);
+        segs[i] = (uint64_t)res[2] | ((uint64_t)res[3] << 32);
         tot_seg += segs[i];
         tot_pts += v.n_indices;
         tot_str += v.strand_count;
@@ -821,6 +842,29 @@ fiber_status fiber_frame_fused(fiber_ctx* c, const fiber_image* scene_color, con
     }
     FIBER_CUDA(cudaGraphLaunch(c->graph, s));
     c->hist_cur = 1 - c->hist_cur;
+    return FIBER_OK;
+}
+
+fiber_status fiber_render_host(fiber_ctx* c, const void* scene_host, const float* depth_host, void* out_host,
+                               void* stream_) {
+    if (!c || !scene_host || !out_host) return FIBER_EINVAL;
+    if (!c->frame_ready) return FIBER_ENOTREADY;
+    cudaSetDevice(c->device);
+    cudaStream_t s = (cudaStream_t)stream_;
+    const uint64_t W = c->P.width, H = c->P.height;
+    fiber_status e = ensure(c, c->d_host_scene, W * H * 8, false);
+    if (e == FIBER_OK && depth_host) e = ensure(c, c->d_host_depth, W * H * 4, false);
+    if (e != FIBER_OK) return e;
+    FIBER_CUDA(cudaMemcpyAsync(c->d_host_scene.p, scene_host, W * H * 8, cudaMemcpyHostToDevice, s));
+    if (depth_host) FIBER_CUDA(cudaMemcpyAsync(c->d_host_depth.p, depth_host, W * H * 4, cudaMemcpyHostToDevice, s));
+    // The composite blends onto the loaded destination; compositing in place
+    // over the scene image gives dst = scene colour (each pixel is read and
+    // written by one thread).
+    fiber_image scene{c->d_host_scene.p, (uint32_t)W, (uint32_t)H, (uint32_t)(W * 8), FIBER_FMT_RGBA16F};
+    fiber_image depth{c->d_host_depth.p, (uint32_t)W, (uint32_t)H, (uint32_t)(W * 4), FIBER_FMT_R32F};
+    fiber_status st = fiber_frame_fused(c, &scene, depth_host ? &depth : nullptr, &scene, stream_);
+    if (st != FIBER_OK) return st;
+    FIBER_CUDA(cudaMemcpyAsync(out_host, c->d_host_scene.p, W * H * 8, cudaMemcpyDeviceToHost, s));
     return FIBER_OK;
 }
 

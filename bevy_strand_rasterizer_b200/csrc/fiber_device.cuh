@@ -205,7 +205,7 @@ __device__ __forceinline__ uint32_t light_layer(const FrameParams& P, uint32_t f
 // bounded: after kSpinLimit polls the block records kErrTimeout and proceeds
 // with what it has, so a broken chain cannot hang the GPU.
 // ---------------------------------------------------------------------------
-constexpr uint32_t kSpinLimit = 1u << 22;
+constexpr uint32_t kSpinLimit = 1u << 21;
 
 __device__ __forceinline__ void lb_publish(unsigned long long* status, uint32_t tile, uint32_t epoch, uint32_t flag,
                                            uint32_t value) {
@@ -230,7 +230,9 @@ __device__ __forceinline__ uint32_t lb_exclusive(unsigned long long* status, uin
         uint32_t hi = (uint32_t)(v >> 32);
         uint32_t flag = (hi >> 2) == (epoch & 0x3FFFFFFFu) ? (hi & 3u) : 0u;
         if (flag == 0u) {
-            if (++spins > kSpinLimit) {
+            // Give up after kSpinLimit polls, or at once when another block of
+            // this frame already gave up, so a broken chain costs one limit.
+            if (++spins > kSpinLimit || ((spins & 255u) == 0u && *((volatile uint32_t*)error) != 0u)) {
                 atomicOr(error, kErrTimeout);
                 break;
             }

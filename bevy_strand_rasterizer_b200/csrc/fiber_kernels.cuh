@@ -10,6 +10,43 @@ namespace fiber {
 
 inline unsigned ceil_div_host(uint64_t x, uint64_t y) { return (unsigned)((x + y - 1) / y); }
 
+// Segment fetch (get_segment_vertices_from_index_unchecked,
+// strand_rasterizer.wgsl:289-303): 128-bit vertex loads through the read-only
+// path, world transform in the reference's evaluation order.
+__device__ __forceinline__ void segment_world(const InstanceView& in, uint32_t seg, float4& w0, float4& w1) {
+    uint32_t i0 = __ldg(in.indices + seg), i1 = __ldg(in.indices + seg + 1u);
+    float4 a = __ldg(in.vertices + i0), b = __ldg(in.vertices + i1);
+    w0 = matvec(in.world_from_local, a.x, a.y, a.z, 1.0f);
+    w1 = matvec(in.world_from_local, b.x, b.y, b.z, 1.0f);
+}
+
+// fragment_position_line_relative (strand_rasterizer.wgsl:138-147)
+__device__ __forceinline__ float line_t(float px, float py, float ax, float ay, float bx, float by) {
+    float abx = bx - ax, aby = by - ay;
+    float l2 = abx * abx + aby * aby;
+    if (l2 == 0.0f) return 0.0f;
+    return ((px - ax) * abx + (py - ay) * aby) / l2;
+}
+
+// blend_over_premult (strand_rasterizer.wgsl:156-162)
+__device__ __forceinline__ float4 over(float4 fg, float4 bg) {
+    float oma = 1.0f - fg.w;
+    return make_float4(fg.x + bg.x * oma, fg.y + bg.y * oma, fg.z + bg.z * oma, fg.w + bg.w * oma);
+}
+
+__device__ __forceinline__ float4 load_half4(const __half* p) {
+    uint2 v = *reinterpret_cast<const uint2*>(p);
+    __half2 a = *reinterpret_cast<__half2*>(&v.x), b = *reinterpret_cast<__half2*>(&v.y);
+    float2 fa = __half22float2(a), fb = __half22float2(b);
+    return make_float4(fa.x, fa.y, fb.x, fb.y);
+}
+
+__device__ __forceinline__ uint2 pack_half4(float x, float y, float z, float w) {
+    __half2 lo = __halves2half2(__float2half_rn(x), __float2half_rn(y));
+    __half2 hi = __halves2half2(__float2half_rn(z), __float2half_rn(w));
+    return make_uint2(*reinterpret_cast<uint32_t*>(&lo), *reinterpret_cast<uint32_t*>(&hi));
+}
+
 // Device buffers of the work-preparation stages.
 struct PrepassArgs {
     uint32_t* tile_counter;          // virtual block ids of the current look-back stage
@@ -87,7 +124,7 @@ void launch_compact_active(const LaunchCtx& L, const PrepassArgs& A);
 void launch_emit(const LaunchCtx& L, const PrepassArgs& A);
 void launch_sort_big(const LaunchCtx& L, const PrepassArgs& A);
 
-void launch_shadow(const LaunchCtx& L, const RenderArgs& R);
+void launch_shadow(const LaunchCtx& L, const RenderArgs& R, uint32_t K);
 void launch_shade(const LaunchCtx& L, const RenderArgs& R);
 void launch_raster(const LaunchCtx& L, const RenderArgs& R);
 void launch_composite(cudaStream_t s, const CompositeArgs& C);

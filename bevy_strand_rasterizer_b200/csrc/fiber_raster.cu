@@ -1,0 +1,472 @@
+// fiber_raster.cu — the deep-opacity shadow raster (with the shadow-map
+// stampback fused into its epilogue) and the camera colour raster:
+// strand_rasterizer.wgsl:391-711 (SHADOWS) and :855-1044 (LINEAR),
+// shadow_dom_stampback.wgsl:74-123.
+//
+// One block per tile run: 64 pixel slots x 4 workers, a pixel's 4 workers in
+// adjacent lanes of one warp. The run's references are staged into shared
+// memory a round at a time by all 256 threads (per-reference projection,
+// radii, shading texels); a round holds whole work items, or one CAP-sized
+// chunk of an item longer than CAP (CAP is a multiple of 16, so the
+// reference's groups of 4 never straddle a round). Within a round the pixels
+// walk the work items warp-synchronously (shuffles only); block barriers
+// happen only between rounds. The blend order is the reference's: work items
+// near to far, references in groups of 4 from each item's start, (w0 over w1)
+// over (w2 over w3), early out after each item once alpha > 0.98.
+#include "fiber_kernels.cuh"
+
+namespace fiber {
+
+constexpr uint32_t kMaxRunItems = 256;  // 16 coarse z x 16 fine z cells per fine tile
+
+struct RoundPlan {
+    uint32_t lo, hi;     // work items [lo, hi) of the run in this round
+    uint32_t off;        // first reference of item lo covered by the round
+    uint32_t n;          // staged references
+    uint32_t completes;  // the round ends item hi - 1
+};
+
+// Thread 0: plans the next round from (cur_item, cur_off); writes the staged
+// prefix of each item of the round into s_prefix.
+__device__ __forceinline__ RoundPlan plan_round(const uint32_t* s_wcount, uint32_t n_items, uint32_t cap,
+                                                uint32_t& cur_item, uint32_t& cur_off, uint32_t* s_prefix) {
+    RoundPlan rp;
+    rp.lo = cur_item;
+    rp.off = cur_off;
+    const uint32_t c = s_wcount[cur_item];
+    if (cur_off > 0u || c > cap) {
+        const uint32_t n = min(cap, c - cur_off);
+        s_prefix[0] = 0u;
+        s_prefix[1] = n;
+        rp.hi = cur_item + 1u;
+        rp.n = n;
+        cur_off += n;
+        rp.completes = cur_off == c ? 1u : 0u;
+        if (cur_off == c) { ++cur_item; cur_off = 0u; }
+    } else {
+        uint32_t total = 0u, k = 0u;
+        while (cur_item < n_items && total + s_wcount[cur_item] <= cap) {
+            s_prefix[k++] = total;
+            total += s_wcount[cur_item];
+            ++cur_item;
+        }
+        s_prefix[k] = total;
+        rp.hi = cur_item;
+        rp.n = total;
+        rp.completes = 1u;
+    }
+    return rp;
+}
+
+// Staged slot s -> (item, reference offset inside the item).
+__device__ __forceinline__ void slot_source(const uint32_t* s_prefix, const RoundPlan& rp, uint32_t s, uint32_t& item,
+                                            uint32_t& j) {
+    uint32_t lo = 0u, hi = rp.hi - rp.lo;  // last k with s_prefix[k] <= s
+    while (hi - lo > 1u) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (s_prefix[mid] <= s) lo = mid; else hi = mid;
+    }
+    item = rp.lo + lo;
+    j = (lo == 0u ? rp.off : 0u) + (s - s_prefix[lo]);
+}
+
+// ===========================================================================
+// K16 deep-opacity shadow raster + K17 stampback.
+// ===========================================================================
+constexpr uint32_t kShadowCap = 1024;
+constexpr int kMaxDomSlices = 16;
+
+size_t shadow_smem_bytes(uint32_t K) {
+    return (size_t)kShadowCap * (9 * sizeof(float) + sizeof(uint32_t)) + (size_t)256 * K * sizeof(float);
+}
+
+__global__ void __launch_bounds__(256) k_shadow(const FrameParams* __restrict__ Pp,
+                                                const InstanceView* __restrict__ inst, RenderArgs R) {
+    const FrameParams& P = *Pp;
+    extern __shared__ float s_dyn[];
+    float* sp0x = s_dyn;
+    float* sp0y = sp0x + kShadowCap;
+    float* sp0z = sp0y + kShadowCap;
+    float* sp1x = sp0z + kShadowCap;
+    float* sp1y = sp1x + kShadowCap;
+    float* sp1z = sp1y + kShadowCap;
+    float* srmin = sp1z + kShadowCap;
+    float* srmax = srmin + kShadowCap;
+    float* sabs = srmax + kShadowCap;
+    uint32_t* svalid = reinterpret_cast<uint32_t*>(sabs + kShadowCap);
+    float* s_partial = reinterpret_cast<float*>(svalid + kShadowCap);
+    __shared__ uint32_t s_wbase[kMaxRunItems], s_wcount[kMaxRunItems], s_prefix[kMaxRunItems + 1];
+    __shared__ RoundPlan s_plan;
+    __shared__ uint32_t s_more;
+
+    const uint32_t first = *((volatile uint32_t*)&R.counters->camera_active);
+    const uint32_t last = *((volatile uint32_t*)&R.counters->active_tiles);
+    const uint32_t K = P.K, D = P.dom_size, S = P.shadow_map_size;
+    const uint32_t slot = threadIdx.x >> 2, worker = threadIdx.x & 3u;
+    float* partial = s_partial + threadIdx.x * K;
+
+    for (uint32_t r = first + blockIdx.x; r < last; r += gridDim.x) {
+        const fiber_raster_tile_run run = R.runs[r];
+        const uint32_t f = run.frustum_id;
+        const uint32_t layer = light_layer(P, f);
+        if (run.work_count == 0u || layer == kInvalid) continue;
+        const uint32_t n_items = min(run.work_count, kMaxRunItems);
+        const fiber_frustum_desc& d = P.frusta[f];
+        const float* clip = P.clip[f];
+        const float vw = u2f(d.screen_width), vh = u2f(d.screen_height);
+        const uint32_t ftx = ceil_div(d.screen_width, d.froxel_size_x);
+        const uint32_t tx = run.screen_tile_id % ftx, ty = run.screen_tile_id / ftx;
+        const uint32_t px = tx * d.froxel_size_x + slot % d.froxel_size_x;
+        const uint32_t py = ty * d.froxel_size_y + slot / d.froxel_size_x;
+        const bool active = slot < d.froxel_size_x * d.froxel_size_y && px < d.screen_width && py < d.screen_height;
+        const float pfx = u2f(px) + 0.5f, pfy = u2f(py) + 0.5f;
+        for (uint32_t i = threadIdx.x; i < n_items; i += blockDim.x) {
+            const fiber_raster_work_item wi = R.work[run.work_base + i];
+            const bool valid_item = wi.frustum_id == f && wi.screen_tile_id == run.screen_tile_id;
+            s_wbase[i] = wi.seg_ref_base;
+            s_wcount[i] = valid_item ? wi.seg_ref_count : 0u;
+        }
+        __syncthreads();
+
+        auto stage = [&](const RoundPlan& rp) {
+            for (uint32_t s = threadIdx.x; s < rp.n; s += blockDim.x) {
+                uint32_t item, j;
+                slot_source(s_prefix, rp, s, item, j);
+                const fiber_fine_seg_ref ref = R.refs[s_wbase[item] + j];
+                const InstanceView& in = inst[ref.inst_id];
+                float4 w0, w1;
+                segment_world(in, ref.seg_id, w0, w1);
+                float4 a = world_to_screen_raw(w0, clip, vw, vh), b = world_to_screen_raw(w1, clip, vw, vh);
+                const fiber_strand_material& m = in.materials[ref.material_idx];
+                sp0x[s] = a.x; sp0y[s] = a.y; sp0z[s] = normalize_depth01(a.z);
+                sp1x[s] = b.x; sp1y[s] = b.y; sp1z[s] = normalize_depth01(b.z);
+                float rmin = wmax(m.min_radius_pixels, 1e-4f);
+                srmin[s] = rmin;
+                srmax[s] = wmax(m.max_radius_pixels, rmin);
+                sabs[s] = m.absorption_color[3];
+                svalid[s] = 1u;
+            }
+        };
+
+        // ---- Pass 1: nearest covered depth, item by item until the first item with a hit.
+        float z0 = -1.0f, zi = -1.0f;
+        bool found = false, hit = false;
+        uint32_t cur_item = 0u, cur_off = 0u;
+        bool single_round = false, staged_all = false;
+        for (bool first_round = true;; first_round = false) {
+            if (threadIdx.x == 0) {
+                s_more = cur_item < n_items ? 1u : 0u;
+                if (s_more) s_plan = plan_round(s_wcount, n_items, kShadowCap, cur_item, cur_off, s_prefix);
+                if (first_round) s_more |= (cur_item >= n_items ? 2u : 0u);
+            }
+            __syncthreads();
+            const uint32_t more = s_more;
+            if (!(more & 1u)) break;
+            if (first_round) single_round = (more & 2u) != 0u;
+            const RoundPlan rp = s_plan;
+            stage(rp);
+            __syncthreads();
+            staged_all = single_round;
+            for (uint32_t k = rp.lo; k < rp.hi; ++k) {
+                const uint32_t a = s_prefix[k - rp.lo], b = s_prefix[k - rp.lo + 1u];
+                if (!__all_sync(0xFFFFFFFFu, found || !active) && active && !found) {
+                    for (uint32_t bi = a + worker; bi < b; bi += 4u) {
+                        float t = line_t(pfx, pfy, sp0x[bi], sp0y[bi], sp1x[bi], sp1y[bi]);
+                        if (t < 0.0f || t > 1.0f) continue;
+                        float qx = wmix(sp0x[bi], sp1x[bi], t), qy = wmix(sp0y[bi], sp1y[bi], t);
+                        float qz = wmix(sp0z[bi], sp1z[bi], t);
+                        float rr = wmix(srmin[bi], srmax[bi], wclamp(qz, 0.0f, 1.0f));
+                        float dx = pfx - qx, dy = pfy - qy;
+                        float cov = wclamp(1.0f - sqrtf(dx * dx + dy * dy) / rr, 0.0f, 1.0f);
+                        if (cov > 0.0f) { zi = wmax(zi, qz); hit = true; }
+                    }
+                }
+                if (k + 1u < rp.hi || rp.completes) {
+                    float zm = wmax(zi, __shfl_xor_sync(0xFFFFFFFFu, zi, 1));
+                    zm = wmax(zm, __shfl_xor_sync(0xFFFFFFFFu, zm, 2));
+                    unsigned hm = __ballot_sync(0xFFFFFFFFu, hit);
+                    bool any_hit = ((hm >> (threadIdx.x & 28u)) & 0xFu) != 0u;
+                    if (active && !found && any_hit) { z0 = zm; found = true; }
+                    zi = -1.0f;
+                    hit = false;
+                }
+            }
+            if (__syncthreads_and(found || !active)) break;
+        }
+
+        // ---- Pass 2: opacity partials; worker w takes entries w, w+4, ... of each item.
+        for (uint32_t i = 0; i < K; ++i) partial[i] = 0.0f;
+        const bool alpha_active = active && found;
+        const float alpha_z0 = alpha_active ? z0 : 1.0f;
+        const float inv_span = 1.0f / wmax(1e-6f, alpha_z0);
+        if (__syncthreads_or(alpha_active)) {
+            cur_item = 0u;
+            cur_off = 0u;
+            for (;;) {
+                if (!staged_all) {
+                    if (threadIdx.x == 0) {
+                        s_more = cur_item < n_items ? 1u : 0u;
+                        if (s_more) s_plan = plan_round(s_wcount, n_items, kShadowCap, cur_item, cur_off, s_prefix);
+                    }
+                    __syncthreads();
+                    if (!s_more) break;
+                    stage(s_plan);
+                    __syncthreads();
+                }
+                const RoundPlan rp = s_plan;
+                for (uint32_t k = rp.lo; k < rp.hi && alpha_active; ++k) {
+                    const uint32_t a = s_prefix[k - rp.lo], b = s_prefix[k - rp.lo + 1u];
+                    for (uint32_t bi = a + worker; bi < b; bi += 4u) {
+                        float t = line_t(pfx, pfy, sp0x[bi], sp0y[bi], sp1x[bi], sp1y[bi]);
+                        if (t < 0.0f || t > 1.0f) continue;
+                        float qx = wmix(sp0x[bi], sp1x[bi], t), qy = wmix(sp0y[bi], sp1y[bi], t);
+                        float qz = wmix(sp0z[bi], sp1z[bi], t);
+                        float rr = wmix(srmin[bi], srmax[bi], wclamp(qz, 0.0f, 1.0f));
+                        float dx = pfx - qx, dy = pfy - qy;
+                        float cov = wclamp(1.0f - sqrtf(dx * dx + dy * dy) / rr, 0.0f, 1.0f);
+                        if (cov <= 0.0f) continue;
+                        float dzp = wmax(0.0f, alpha_z0 - qz) * inv_span;
+                        float u = wclamp(dzp, 0.0f, 1.0f);  // pow(u, DOM_GAMMA = 1)
+                        float tl = u * u2f(K);
+                        uint32_t si = min(f2u(floorf(tl)), K - 1u);
+                        float wf = tl - floorf(tl);
+                        float al = cov * sabs[bi] * 0.5f;
+                        float a0 = partial[si];
+                        partial[si] = wclamp(a0 + (1.0f - a0) * (1.0f - wf) * al, 0.0f, 1.0f);
+                        if (si + 1u < K) {
+                            float a1 = partial[si + 1u];
+                            partial[si + 1u] = wclamp(a1 + (1.0f - a1) * wf * al, 0.0f, 1.0f);
+                        }
+                    }
+                }
+                if (staged_all) break;
+                __syncthreads();
+            }
+        }
+        __syncwarp();
+        // ---- Combine the 4 workers per slice, write the DOM, stamp the shadow map.
+        if (worker == 0u && active) {
+            const size_t dom_px = (size_t)py * D + px;
+            if (!found) {
+                R.dom_depth[(size_t)layer * D * D + dom_px] = 0.0f;
+                for (uint32_t i = 0; i < K; ++i) R.dom_opacity[((size_t)layer * K + i) * D * D + dom_px] = 0.0f;
+            } else {
+                R.dom_depth[(size_t)layer * D * D + dom_px] = z0;
+                float acc = 0.0f;
+                for (uint32_t i = 0; i < K; ++i) {
+                    float a = 0.0f;
+                    for (uint32_t wk = 0; wk < 4u; ++wk) a = a + (1.0f - a) * s_partial[(threadIdx.x + wk) * K + i];
+                    acc = acc + (1.0f - acc) * a;  // opaque_terminal_slice = K without an opaque depth
+                    R.dom_opacity[((size_t)layer * K + i) * D * D + dom_px] = acc;
+                }
+                // Fused stampback: every target texel whose DOM footprint holds
+                // this texel takes the max depth (the target starts cleared).
+                if (z0 > 0.0f) {
+                    uint32_t x_lo = (uint32_t)(((uint64_t)px * S) / D), y_lo = (uint32_t)(((uint64_t)py * S) / D);
+                    x_lo = x_lo > 0u ? x_lo - 1u : 0u;
+                    y_lo = y_lo > 0u ? y_lo - 1u : 0u;
+                    for (uint32_t ty2 = y_lo; ty2 < S && ty2 <= y_lo + 2u + S / D; ++ty2) {
+                        uint32_t mny = min((ty2 * D) / S, D - 1u), mxy = min(((ty2 + 1u) * D + S - 1u) / S, D);
+                        if (py < mny || py >= mxy) continue;
+                        for (uint32_t tx2 = x_lo; tx2 < S && tx2 <= x_lo + 2u + S / D; ++tx2) {
+                            uint32_t mnx = min((tx2 * D) / S, D - 1u), mxx = min(((tx2 + 1u) * D + S - 1u) / S, D);
+                            if (px < mnx || px >= mxx) continue;
+                            atomicMax(reinterpret_cast<int*>(R.shadow_map + (size_t)layer * S * S + (size_t)ty2 * S + tx2),
+                                      __float_as_int(z0));
+                        }
+                    }
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// ===========================================================================
+// K19 camera colour raster.
+// ===========================================================================
+constexpr uint32_t kCamCap = 512;
+
+__global__ void __launch_bounds__(256) k_raster(const FrameParams* __restrict__ Pp,
+                                                const InstanceView* __restrict__ inst, RenderArgs R) {
+    const FrameParams& P = *Pp;
+    // Per staged reference (80 B). An invalid slot (segment behind the camera)
+    // gets an empty bounding box (mnx = +inf), which rejects every pixel
+    // exactly like the reference's valid flag.
+    __shared__ float sp0x[kCamCap], sp0y[kCamCap], sabx[kCamCap], saby[kCamCap], sinv[kCamCap];
+    __shared__ float sz0[kCamCap], sz1[kCamCap], sw0[kCamCap], sw1[kCamCap], srmin[kCamCap], srmax[kCamCap];
+    __shared__ float smnx[kCamCap], smny[kCamCap], smxx[kCamCap], smxy[kCamCap], svis[kCamCap];
+    __shared__ uint2 ss0[kCamCap], ss1[kCamCap];
+    __shared__ uint32_t s_wbase[kMaxRunItems], s_wcount[kMaxRunItems], s_prefix[kMaxRunItems + 1];
+    __shared__ RoundPlan s_plan;
+    __shared__ uint32_t s_more;
+
+    const uint32_t n_runs = *((volatile uint32_t*)&R.counters->camera_active);
+    const uint32_t slot = threadIdx.x >> 2, worker = threadIdx.x & 3u;
+    const uint32_t lane = threadIdx.x & 31u, wbase = lane & ~3u;
+    const uint32_t cap = P.atlas_cap;
+    const __half* hist = R.history[(P.hist_in & 1u) ^ 1u];
+    for (uint32_t r = blockIdx.x; r < n_runs; r += gridDim.x) {
+        const fiber_raster_tile_run run = R.runs[r];
+        const uint32_t f = run.frustum_id;
+        if (run.work_count == 0u || f >= P.camera_frustum_end) continue;
+        const uint32_t n_items = min(run.work_count, kMaxRunItems);
+        const fiber_frustum_desc& d = P.frusta[f];
+        const float* clip = P.clip[f];
+        const float vw = u2f(d.screen_width), vh = u2f(d.screen_height);
+        const uint32_t ftx = ceil_div(d.screen_width, d.froxel_size_x);
+        const uint32_t tx = run.screen_tile_id % ftx, ty = run.screen_tile_id / ftx;
+        const uint32_t px = tx * d.froxel_size_x + slot % d.froxel_size_x;
+        const uint32_t py = ty * d.froxel_size_y + slot / d.froxel_size_x;
+        const bool active = slot < d.froxel_size_x * d.froxel_size_y && px < d.screen_width && py < d.screen_height;
+        const float pcx = u2f(px) + 0.5f, pcy = u2f(py) + 0.5f;
+        for (uint32_t i = threadIdx.x; i < n_items; i += blockDim.x) {
+            const fiber_raster_work_item wi = R.work[run.work_base + i];
+            s_wbase[i] = wi.seg_ref_base;
+            s_wcount[i] = wi.seg_ref_count;
+        }
+        __syncthreads();
+        float4 fin = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        float gdepth = 0.0f;
+        bool done = !active;
+        uint32_t frags = 0;
+        uint32_t cur_item = 0u, cur_off = 0u;
+        for (;;) {
+            if (threadIdx.x == 0) {
+                s_more = cur_item < n_items ? 1u : 0u;
+                if (s_more) s_plan = plan_round(s_wcount, n_items, kCamCap, cur_item, cur_off, s_prefix);
+            }
+            __syncthreads();
+            if (!s_more) break;
+            const RoundPlan rp = s_plan;
+            for (uint32_t s = threadIdx.x; s < rp.n; s += blockDim.x) {
+                uint32_t item, j;
+                slot_source(s_prefix, rp, s, item, j);
+                const fiber_fine_seg_ref ref = R.refs[s_wbase[item] + j];
+                const InstanceView& in = inst[ref.inst_id];
+                float4 w0, w1;
+                segment_world(in, ref.seg_id, w0, w1);
+                float4 a = world_to_screen_raw(w0, clip, vw, vh), b = world_to_screen_raw(w1, clip, vw, vh);
+                if (!(a.x < 0.0f && b.x < 0.0f)) {
+                    const fiber_strand_material& m = in.materials[ref.material_idx];
+                    float rmin = wmax(m.min_radius_pixels, 1e-4f);
+                    float rmax = wmax(m.max_radius_pixels, rmin);
+                    uint32_t i0 = ref.seg_id, i1 = min(i0 + 1u, cap - 1u);
+                    size_t t0 = (size_t)ref.inst_id * cap + i0, t1 = (size_t)ref.inst_id * cap + i1;
+                    float abx = b.x - a.x, aby = b.y - a.y;
+                    sp0x[s] = a.x; sp0y[s] = a.y; sabx[s] = abx; saby[s] = aby;
+                    sinv[s] = 1.0f / (abx * abx + aby * aby);
+                    sz0[s] = a.z; sz1[s] = b.z; sw0[s] = a.w; sw1[s] = b.w;
+                    // min_radius = max(rmin, 1e-4) and max(rmax, min_radius) are
+                    // idempotent on these values, so they are applied once here.
+                    srmin[s] = rmin; srmax[s] = rmax;
+                    smnx[s] = wmin(a.x, b.x) - rmax; smny[s] = wmin(a.y, b.y) - rmax;
+                    smxx[s] = wmax(a.x, b.x) + rmax; smxy[s] = wmax(a.y, b.y) + rmax;
+                    ss0[s] = *reinterpret_cast<const uint2*>(R.atlas + t0 * 4);
+                    ss1[s] = *reinterpret_cast<const uint2*>(R.atlas + t1 * 4);
+                    svis[s] = __half2float(hist[t0 * 2]);
+                } else {
+                    smnx[s] = __int_as_float(0x7f800000);  // +inf: empty box
+                    smny[s] = 0.0f; smxx[s] = 0.0f; smxy[s] = 0.0f;
+                }
+            }
+            __syncthreads();
+            for (uint32_t k = rp.lo; k < rp.hi; ++k) {
+                const uint32_t a = s_prefix[k - rp.lo], b = s_prefix[k - rp.lo + 1u];
+                if (!__all_sync(0xFFFFFFFFu, done)) {
+                    for (uint32_t g = a; g < b; g += 4u) {
+                        float4 part = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                        float pd = 0.0f;
+                        const uint32_t bi = g + worker;
+                        if (!done && bi < b && !(pcx < smnx[bi] || pcy < smny[bi]) && !(pcx > smxx[bi] || pcy > smxy[bi])) {
+                            float t = ((pcx - sp0x[bi]) * sabx[bi] + (pcy - sp0y[bi]) * saby[bi]) * sinv[bi];
+                            if (t >= 0.0f && t <= 1.0f) {
+                                float fx = sp0x[bi] + sabx[bi] * t, fy = sp0y[bi] + saby[bi] * t;
+                                float pz = wmix(sz0[bi], sz1[bi], t);
+                                float rr = wmix(srmin[bi], srmax[bi], wclamp(normalize_depth01(pz), 0.0f, 1.0f));
+                                float dx = pcx - fx, dy = pcy - fy;
+                                float d2 = dx * dx + dy * dy;
+                                if (d2 < rr * rr) {
+                                    float cov = wclamp(1.0f - sqrtf(d2) / rr, 0.0f, 1.0f);
+                                    // perspective_correct_line_t (:149-154)
+                                    float aw0 = wmax(fabsf(sw0[bi]), 1e-6f), aw1 = wmax(fabsf(sw1[bi]), 1e-6f);
+                                    float tw = (t * aw0) / ((1.0f - t) * aw1 + t * aw0);
+                                    float4 c0 = load_half4(reinterpret_cast<const __half*>(&ss0[bi]));
+                                    float4 c1 = load_half4(reinterpret_cast<const __half*>(&ss1[bi]));
+                                    float sr = wmix(c0.x, c1.x, tw), sg = wmix(c0.y, c1.y, tw);
+                                    float sbl = wmix(c0.z, c1.z, tw), sa = wmix(c0.w, c1.w, tw);
+                                    float alpha = sa * cov;
+                                    float vsb = svis[bi];
+                                    part = make_float4(sr * vsb * alpha, sg * vsb * alpha, sbl * vsb * alpha, alpha);
+                                    pd = pz;
+                                    ++frags;
+                                }
+                            }
+                        }
+                        // (w0 over w1) over (w2 over w3), depth max.
+                        const uint32_t src = wbase + (worker | 1u);
+                        float4 rhs;
+                        rhs.x = __shfl_sync(0xFFFFFFFFu, part.x, src);
+                        rhs.y = __shfl_sync(0xFFFFFFFFu, part.y, src);
+                        rhs.z = __shfl_sync(0xFFFFFFFFu, part.z, src);
+                        rhs.w = __shfl_sync(0xFFFFFFFFu, part.w, src);
+                        float rd = __shfl_sync(0xFFFFFFFFu, pd, src);
+                        float4 pair = part;
+                        float pdd = pd;
+                        if ((worker & 1u) == 0u) {
+                            pair = over(part, rhs);
+                            pdd = wmax(pd, rd);
+                        }
+                        float4 second;
+                        second.x = __shfl_sync(0xFFFFFFFFu, pair.x, wbase + 2u);
+                        second.y = __shfl_sync(0xFFFFFFFFu, pair.y, wbase + 2u);
+                        second.z = __shfl_sync(0xFFFFFFFFu, pair.z, wbase + 2u);
+                        second.w = __shfl_sync(0xFFFFFFFFu, pair.w, wbase + 2u);
+                        float sdp = __shfl_sync(0xFFFFFFFFu, pdd, wbase + 2u);
+                        if (worker == 0u && !done) {
+                            fin = over(fin, over(pair, second));
+                            gdepth = wmax(gdepth, wmax(pdd, sdp));
+                        }
+                    }
+                }
+                if (k + 1u < rp.hi || rp.completes) {
+                    if (worker == 0u && !done && fin.w > 0.98f) {
+                        fin = make_float4(fin.x / fin.w, fin.y / fin.w, fin.z / fin.w, 1.0f);
+                        done = true;
+                    }
+                    done = __shfl_sync(0xFFFFFFFFu, done, wbase);
+                }
+            }
+            if (__syncthreads_and(done)) break;
+        }
+        frags += __shfl_xor_sync(0xFFFFFFFFu, frags, 1);
+        frags += __shfl_xor_sync(0xFFFFFFFFu, frags, 2);
+        if (worker == 0u && active) {
+            float4 o = fin;
+            if (o.w > 1e-6f && o.w < 1.0f) o = make_float4(o.x / o.w, o.y / o.w, o.z / o.w, o.w);
+            size_t pi = (size_t)py * P.width + px;
+            reinterpret_cast<uint2*>(R.color)[pi] = pack_half4(o.x, o.y, o.z, o.w);
+            R.depth[pi] = gdepth;
+            if (P.fragment_counts) R.fragments[pi] = frags;
+        }
+        __syncthreads();
+    }
+}
+
+void launch_shadow(const LaunchCtx& L, const RenderArgs& R, uint32_t K) {
+    static bool configured[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const size_t max_bytes = shadow_smem_bytes(kMaxDomSlices);
+    if (dev < 0 || dev >= 64 || !configured[dev]) {
+        cudaFuncSetAttribute(k_shadow, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_bytes);
+        if (dev >= 0 && dev < 64) configured[dev] = true;
+    }
+    k_shadow<<<L.sm_count * 3, 256, shadow_smem_bytes(K), L.stream>>>(L.P, L.inst, R);
+}
+
+void launch_raster(const LaunchCtx& L, const RenderArgs& R) {
+    k_raster<<<L.sm_count * 3, 256, 0, L.stream>>>(L.P, L.inst, R);
+}
+
+}  // namespace fiber

@@ -1,226 +1,9 @@
-// fiber_render.cu — deep shadow + stampback, shading, camera raster and
-// composite: the reference's strand_shadow_rasterizer_pass
-// (src/nodes/shadows.rs:29-221), strand_shading_pass (src/nodes/shading.rs:25-155),
-// strand_rasterizer_pass (src/nodes/raster.rs:26-179) and composition_pass
-// (src/nodes/composite.rs:19-131).
+// fiber_render.cu — shading and composite: the reference's strand_shading_pass
+// (src/nodes/shading.rs:25-155) and composition_pass
+// (src/nodes/composite.rs:19-131). The rasters live in fiber_raster.cu.
 #include "fiber_kernels.cuh"
 
 namespace fiber {
-
-// ---------------------------------------------------------------------------
-// Segment fetch (get_segment_vertices_from_index_unchecked,
-// strand_rasterizer.wgsl:289-303): 128-bit vertex loads through the read-only
-// path, world transform in the reference's evaluation order.
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ void segment_world(const InstanceView& in, uint32_t seg, float4& w0, float4& w1) {
-    uint32_t i0 = __ldg(in.indices + seg), i1 = __ldg(in.indices + seg + 1u);
-    float4 a = __ldg(in.vertices + i0), b = __ldg(in.vertices + i1);
-    w0 = matvec(in.world_from_local, a.x, a.y, a.z, 1.0f);
-    w1 = matvec(in.world_from_local, b.x, b.y, b.z, 1.0f);
-}
-
-// fragment_position_line_relative (strand_rasterizer.wgsl:138-147)
-__device__ __forceinline__ float line_t(float px, float py, float ax, float ay, float bx, float by) {
-    float abx = bx - ax, aby = by - ay;
-    float l2 = abx * abx + aby * aby;
-    if (l2 == 0.0f) return 0.0f;
-    return ((px - ax) * abx + (py - ay) * aby) / l2;
-}
-
-// ===========================================================================
-// K16 deep-opacity shadow raster (strand_rasterizer.wgsl:391-711) with the
-// stampback (shadow_dom_stampback.wgsl:74-123) fused into its epilogue.
-// One block per shadow tile run: 64 pixel slots x 4 depth workers.
-// ===========================================================================
-constexpr int kShadowBatch = 256;
-constexpr int kMaxDomSlices = 16;
-
-__global__ void __launch_bounds__(256) k_shadow(const FrameParams* __restrict__ Pp,
-                                                const InstanceView* __restrict__ inst, RenderArgs R) {
-    const FrameParams& P = *Pp;
-    __shared__ float s_p0x[kShadowBatch], s_p0y[kShadowBatch], s_p0z[kShadowBatch];
-    __shared__ float s_p1x[kShadowBatch], s_p1y[kShadowBatch], s_p1z[kShadowBatch];
-    __shared__ float s_rmin[kShadowBatch], s_rmax[kShadowBatch], s_abs[kShadowBatch];
-    __shared__ uint32_t s_valid[kShadowBatch];
-    __shared__ float s_partial[256 * kMaxDomSlices];
-    const uint32_t first = *((volatile uint32_t*)&R.counters->camera_active);
-    const uint32_t last = *((volatile uint32_t*)&R.counters->active_tiles);
-    const uint32_t K = P.K, D = P.dom_size, S = P.shadow_map_size;
-    const uint32_t slot = threadIdx.x >> 2, worker = threadIdx.x & 3u;
-    for (uint32_t r = first + blockIdx.x; r < last; r += gridDim.x) {
-        const fiber_raster_tile_run run = R.runs[r];
-        if (run.work_count == 0u) continue;
-        const uint32_t f = run.frustum_id;
-        const uint32_t layer = light_layer(P, f);
-        if (layer == kInvalid) continue;
-        const fiber_frustum_desc& d = P.frusta[f];
-        const float* clip = P.clip[f];
-        const float vw = u2f(d.screen_width), vh = u2f(d.screen_height);
-        const uint32_t ftx = ceil_div(d.screen_width, d.froxel_size_x);
-        const uint32_t tx = run.screen_tile_id % ftx, ty = run.screen_tile_id / ftx;
-        const uint32_t px = tx * d.froxel_size_x + slot % d.froxel_size_x;
-        const uint32_t py = ty * d.froxel_size_y + slot / d.froxel_size_x;
-        const bool active = slot < d.froxel_size_x * d.froxel_size_y && px < d.screen_width && py < d.screen_height;
-        const float pfx = u2f(px) + 0.5f, pfy = u2f(py) + 0.5f;
-        // Pass 1: nearest covered depth, searched work item by work item until
-        // the first item with a hit; the 4 workers split each batch and take
-        // the max (exact, order independent).
-        float z0 = -1.0f;
-        bool found = false;
-        for (uint32_t w = 0; w < run.work_count; ++w) {
-            const fiber_raster_work_item wi = R.work[run.work_base + w];
-            const bool valid_item = wi.frustum_id == f && wi.screen_tile_id == run.screen_tile_id;
-            bool hit = false;
-            float zi = -1.0f;
-            for (uint32_t bb = 0; bb < wi.seg_ref_count; bb += kShadowBatch) {
-                const uint32_t bc = min((uint32_t)kShadowBatch, wi.seg_ref_count - bb);
-                __syncthreads();
-                if (threadIdx.x < bc) {
-                    uint32_t v = 0u;
-                    if (valid_item) {
-                        fiber_fine_seg_ref ref = R.refs[wi.seg_ref_base + bb + threadIdx.x];
-                        const InstanceView& in = inst[ref.inst_id];
-                        float4 w0, w1;
-                        segment_world(in, ref.seg_id, w0, w1);
-                        float4 a = world_to_screen_raw(w0, clip, vw, vh), b = world_to_screen_raw(w1, clip, vw, vh);
-                        fiber_strand_material m = in.materials[ref.material_idx];
-                        s_p0x[threadIdx.x] = a.x; s_p0y[threadIdx.x] = a.y; s_p0z[threadIdx.x] = normalize_depth01(a.z);
-                        s_p1x[threadIdx.x] = b.x; s_p1y[threadIdx.x] = b.y; s_p1z[threadIdx.x] = normalize_depth01(b.z);
-                        float rmin = wmax(m.min_radius_pixels, 1e-4f);
-                        s_rmin[threadIdx.x] = rmin;
-                        s_rmax[threadIdx.x] = wmax(m.max_radius_pixels, rmin);
-                        s_abs[threadIdx.x] = m.absorption_color[3];
-                        v = 1u;
-                    }
-                    s_valid[threadIdx.x] = v;
-                }
-                __syncthreads();
-                if (active && !found) {
-                    for (uint32_t bi = worker; bi < bc; bi += 4u) {
-                        if (!s_valid[bi]) continue;
-                        float t = line_t(pfx, pfy, s_p0x[bi], s_p0y[bi], s_p1x[bi], s_p1y[bi]);
-                        if (t < 0.0f || t > 1.0f) continue;
-                        float qx = wmix(s_p0x[bi], s_p1x[bi], t), qy = wmix(s_p0y[bi], s_p1y[bi], t);
-                        float qz = wmix(s_p0z[bi], s_p1z[bi], t);
-                        float rr = wmix(s_rmin[bi], s_rmax[bi], wclamp(qz, 0.0f, 1.0f));
-                        float dx = pfx - qx, dy = pfy - qy;
-                        float cov = wclamp(1.0f - sqrtf(dx * dx + dy * dy) / rr, 0.0f, 1.0f);
-                        if (cov > 0.0f) { zi = wmax(zi, qz); hit = true; }
-                    }
-                }
-            }
-            // Combine the 4 workers of each pixel (adjacent lanes).
-            float zm = zi;
-            zm = wmax(zm, __shfl_xor_sync(0xFFFFFFFFu, zm, 1));
-            zm = wmax(zm, __shfl_xor_sync(0xFFFFFFFFu, zm, 2));
-            unsigned hm = __ballot_sync(0xFFFFFFFFu, hit);
-            bool any_hit = ((hm >> (threadIdx.x & 28u)) & 0xFu) != 0u;
-            if (active && !found && any_hit) {
-                z0 = wmax(z0, zm);
-                found = true;
-            }
-            if (__syncthreads_and(found || !active)) break;
-        }
-        const size_t dom_px = (size_t)py * D + px;
-        float* partial = s_partial + threadIdx.x * kMaxDomSlices;
-        for (uint32_t i = 0; i < K; ++i) partial[i] = 0.0f;
-        // No opaque directional shadow map is bound on this path (opaque depth 0).
-        const bool alpha_active = active && found;
-        const float alpha_z0 = alpha_active ? z0 : 1.0f;
-        const float inv_span = 1.0f / wmax(1e-6f, alpha_z0);
-        const bool any_alpha = __syncthreads_or(alpha_active);
-        // Pass 2: opacity partials; worker w takes entries w, w+4, ... of each item.
-        for (uint32_t w = 0; any_alpha && w < run.work_count; ++w) {
-            const fiber_raster_work_item wi = R.work[run.work_base + w];
-            const bool valid_item = wi.frustum_id == f && wi.screen_tile_id == run.screen_tile_id;
-            for (uint32_t bb = 0; bb < wi.seg_ref_count; bb += kShadowBatch) {
-                const uint32_t bc = min((uint32_t)kShadowBatch, wi.seg_ref_count - bb);
-                __syncthreads();
-                if (threadIdx.x < bc) {
-                    uint32_t v = 0u;
-                    if (valid_item) {
-                        fiber_fine_seg_ref ref = R.refs[wi.seg_ref_base + bb + threadIdx.x];
-                        const InstanceView& in = inst[ref.inst_id];
-                        float4 w0, w1;
-                        segment_world(in, ref.seg_id, w0, w1);
-                        float4 a = world_to_screen_raw(w0, clip, vw, vh), b = world_to_screen_raw(w1, clip, vw, vh);
-                        fiber_strand_material m = in.materials[ref.material_idx];
-                        s_p0x[threadIdx.x] = a.x; s_p0y[threadIdx.x] = a.y; s_p0z[threadIdx.x] = normalize_depth01(a.z);
-                        s_p1x[threadIdx.x] = b.x; s_p1y[threadIdx.x] = b.y; s_p1z[threadIdx.x] = normalize_depth01(b.z);
-                        float rmin = wmax(m.min_radius_pixels, 1e-4f);
-                        s_rmin[threadIdx.x] = rmin;
-                        s_rmax[threadIdx.x] = wmax(m.max_radius_pixels, rmin);
-                        s_abs[threadIdx.x] = m.absorption_color[3];
-                        v = 1u;
-                    }
-                    s_valid[threadIdx.x] = v;
-                }
-                __syncthreads();
-                if (!alpha_active) continue;
-                for (uint32_t bi = worker; bi < bc; bi += 4u) {
-                    if (!s_valid[bi]) continue;
-                    float t = line_t(pfx, pfy, s_p0x[bi], s_p0y[bi], s_p1x[bi], s_p1y[bi]);
-                    if (t < 0.0f || t > 1.0f) continue;
-                    float qx = wmix(s_p0x[bi], s_p1x[bi], t), qy = wmix(s_p0y[bi], s_p1y[bi], t);
-                    float qz = wmix(s_p0z[bi], s_p1z[bi], t);
-                    float rr = wmix(s_rmin[bi], s_rmax[bi], wclamp(qz, 0.0f, 1.0f));
-                    float dx = pfx - qx, dy = pfy - qy;
-                    float cov = wclamp(1.0f - sqrtf(dx * dx + dy * dy) / rr, 0.0f, 1.0f);
-                    if (cov <= 0.0f) continue;
-                    float dzp = wmax(0.0f, alpha_z0 - qz) * inv_span;
-                    float u = wclamp(dzp, 0.0f, 1.0f);  // pow(u, DOM_GAMMA = 1)
-                    float tl = u * u2f(K);
-                    uint32_t si = min(f2u(floorf(tl)), K - 1u);
-                    float wf = tl - floorf(tl);
-                    float a = cov * s_abs[bi] * 0.5f;
-                    float a0 = partial[si];
-                    partial[si] = wclamp(a0 + (1.0f - a0) * (1.0f - wf) * a, 0.0f, 1.0f);
-                    if (si + 1u < K) {
-                        float a1 = partial[si + 1u];
-                        partial[si + 1u] = wclamp(a1 + (1.0f - a1) * wf * a, 0.0f, 1.0f);
-                    }
-                }
-            }
-        }
-        __syncthreads();
-        if (worker == 0u && active) {
-            if (!found) {
-                R.dom_depth[(size_t)layer * D * D + dom_px] = 0.0f;
-                for (uint32_t i = 0; i < K; ++i) R.dom_opacity[((size_t)layer * K + i) * D * D + dom_px] = 0.0f;
-            } else {
-                R.dom_depth[(size_t)layer * D * D + dom_px] = z0;
-                float acc = 0.0f;
-                for (uint32_t i = 0; i < K; ++i) {
-                    float a = 0.0f;
-                    for (uint32_t wk = 0; wk < 4u; ++wk) {
-                        float pv = s_partial[(threadIdx.x + wk) * kMaxDomSlices + i];
-                        a = a + (1.0f - a) * pv;
-                    }
-                    acc = acc + (1.0f - acc) * a;  // opaque_terminal_slice = K without opaque depth
-                    R.dom_opacity[((size_t)layer * K + i) * D * D + dom_px] = acc;
-                }
-                // Fused stampback: every target texel whose DOM footprint holds
-                // this texel takes the max depth (the target starts cleared).
-                if (z0 > 0.0f) {
-                    uint32_t x_lo = (uint32_t)(((uint64_t)px * S) / D), y_lo = (uint32_t)(((uint64_t)py * S) / D);
-                    x_lo = x_lo > 0u ? x_lo - 1u : 0u;
-                    y_lo = y_lo > 0u ? y_lo - 1u : 0u;
-                    for (uint32_t ty2 = y_lo; ty2 < S && ty2 <= y_lo + 2u + S / D; ++ty2) {
-                        uint32_t mny = min((ty2 * D) / S, D - 1u), mxy = min(((ty2 + 1u) * D + S - 1u) / S, D);
-                        if (py < mny || py >= mxy) continue;
-                        for (uint32_t tx2 = x_lo; tx2 < S && tx2 <= x_lo + 2u + S / D; ++tx2) {
-                            uint32_t mnx = min((tx2 * D) / S, D - 1u), mxx = min(((tx2 + 1u) * D + S - 1u) / S, D);
-                            if (px < mnx || px >= mxx) continue;
-                            atomicMax(reinterpret_cast<int*>(R.shadow_map + (size_t)layer * S * S + (size_t)ty2 * S + tx2),
-                                      __float_as_int(z0));
-                        }
-                    }
-                }
-            }
-        }
-        __syncthreads();
-    }
-}
 
 // ===========================================================================
 // K18 shading: per camera segment, DOM visibility at the midpoint, temporal
@@ -281,7 +64,9 @@ __device__ __forceinline__ float fresnel_reflectance(float eta_i, float eta_t, f
 }
 
 // Sum of the 21 wrapped Gaussians (k = -10..10). Terms whose exponent is below
-// -110 are exactly zero in binary32 and are skipped without changing the sum.
+// -110 are exactly zero in binary32 and are skipped without changing the sum;
+// the test is written so that a NaN exponent is not skipped and still poisons
+// the sum, as exp(NaN) does in the reference.
 __device__ __forceinline__ float gaussian_detector(float beta, float phi_delta) {
     float var = beta * beta;
     if (var < 1e-6f) {
@@ -295,7 +80,7 @@ __device__ __forceinline__ float gaussian_detector(float beta, float phi_delta) 
     for (int k = -10; k <= 10; ++k) {
         float angle = phi_delta - 2.0f * kPi * (float)k;
         float e = -angle * angle / two_var;
-        if (e > -110.0f) total = total + expf(e);
+        if (!(e <= -110.0f)) total = total + expf(e);
     }
     return norm * total;
 }
@@ -438,173 +223,6 @@ __global__ void __launch_bounds__(128) k_shade(const FrameParams* __restrict__ P
 }
 
 // ===========================================================================
-// K19 camera colour raster (strand_rasterizer.wgsl:855-1044). One block per
-// camera tile run: 64 pixel slots x 4 segment workers, batches of 16
-// references, premultiplied "over" reduced as (w0 over w1) over (w2 over w3),
-// early out after each work item once alpha > 0.98.
-// ===========================================================================
-constexpr int kColorBatch = 16;
-
-struct ColorBatch {
-    float p0x[kColorBatch], p0y[kColorBatch], abx[kColorBatch], aby[kColorBatch], inv_len[kColorBatch];
-    float z0[kColorBatch], z1[kColorBatch], w0[kColorBatch], w1[kColorBatch];
-    float rmin[kColorBatch], rmax[kColorBatch];
-    float mnx[kColorBatch], mny[kColorBatch], mxx[kColorBatch], mxy[kColorBatch];
-    float4 s0[kColorBatch], s1[kColorBatch];
-    float vis[kColorBatch];
-    uint32_t valid[kColorBatch];
-};
-
-__device__ __forceinline__ float4 over(float4 fg, float4 bg) {
-    float oma = 1.0f - fg.w;
-    return make_float4(fg.x + bg.x * oma, fg.y + bg.y * oma, fg.z + bg.z * oma, fg.w + bg.w * oma);
-}
-__device__ __forceinline__ float4 load_half4(const __half* p) {
-    uint2 v = *reinterpret_cast<const uint2*>(p);
-    __half2 a = *reinterpret_cast<__half2*>(&v.x), b = *reinterpret_cast<__half2*>(&v.y);
-    float2 fa = __half22float2(a), fb = __half22float2(b);
-    return make_float4(fa.x, fa.y, fb.x, fb.y);
-}
-
-__global__ void __launch_bounds__(256) k_raster(const FrameParams* __restrict__ Pp,
-                                                const InstanceView* __restrict__ inst, RenderArgs R) {
-    const FrameParams& P = *Pp;
-    __shared__ ColorBatch sb;
-    const uint32_t n_runs = *((volatile uint32_t*)&R.counters->camera_active);
-    const uint32_t slot = threadIdx.x >> 2, worker = threadIdx.x & 3u;
-    const uint32_t lane = threadIdx.x & 31u, wbase = lane & ~3u;
-    const uint32_t cap = P.atlas_cap;
-    for (uint32_t r = blockIdx.x; r < n_runs; r += gridDim.x) {
-        const fiber_raster_tile_run run = R.runs[r];
-        const uint32_t f = run.frustum_id;
-        if (run.work_count == 0u || f >= P.camera_frustum_end) continue;
-        const fiber_frustum_desc& d = P.frusta[f];
-        const float* clip = P.clip[f];
-        const float vw = u2f(d.screen_width), vh = u2f(d.screen_height);
-        const uint32_t ftx = ceil_div(d.screen_width, d.froxel_size_x);
-        const uint32_t tx = run.screen_tile_id % ftx, ty = run.screen_tile_id / ftx;
-        const uint32_t px = tx * d.froxel_size_x + slot % d.froxel_size_x;
-        const uint32_t py = ty * d.froxel_size_y + slot / d.froxel_size_x;
-        const bool active = slot < d.froxel_size_x * d.froxel_size_y && px < d.screen_width && py < d.screen_height;
-        const float pcx = u2f(px) + 0.5f, pcy = u2f(py) + 0.5f;
-        float4 fin = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        float gdepth = 0.0f;
-        bool done = !active;
-        uint32_t frags = 0;
-        for (uint32_t w = 0; w < run.work_count; ++w) {
-            const fiber_raster_work_item wi = R.work[run.work_base + w];
-            for (uint32_t bb = 0; bb < wi.seg_ref_count; bb += kColorBatch) {
-                __syncthreads();
-                if (threadIdx.x < kColorBatch) {
-                    const uint32_t j = threadIdx.x;
-                    uint32_t v = 0u;
-                    if (bb + j < wi.seg_ref_count) {
-                        fiber_fine_seg_ref ref = R.refs[wi.seg_ref_base + bb + j];
-                        const InstanceView& in = inst[ref.inst_id];
-                        float4 w0, w1;
-                        segment_world(in, ref.seg_id, w0, w1);
-                        float4 a = world_to_screen_raw(w0, clip, vw, vh), b = world_to_screen_raw(w1, clip, vw, vh);
-                        if (!(a.x < 0.0f && b.x < 0.0f)) {
-                            fiber_strand_material m = in.materials[ref.material_idx];
-                            float rmin = wmax(m.min_radius_pixels, 1e-4f);
-                            float rmax = wmax(m.max_radius_pixels, rmin);
-                            uint32_t i0 = ref.seg_id, i1 = min(i0 + 1u, cap - 1u);
-                            size_t t0 = (size_t)ref.inst_id * cap + i0, t1 = (size_t)ref.inst_id * cap + i1;
-                            float abx = b.x - a.x, aby = b.y - a.y;
-                            sb.p0x[j] = a.x; sb.p0y[j] = a.y; sb.abx[j] = abx; sb.aby[j] = aby;
-                            sb.inv_len[j] = 1.0f / (abx * abx + aby * aby);
-                            sb.z0[j] = a.z; sb.z1[j] = b.z; sb.w0[j] = a.w; sb.w1[j] = b.w;
-                            sb.rmin[j] = rmin; sb.rmax[j] = rmax;
-                            sb.mnx[j] = wmin(a.x, b.x) - rmax; sb.mny[j] = wmin(a.y, b.y) - rmax;
-                            sb.mxx[j] = wmax(a.x, b.x) + rmax; sb.mxy[j] = wmax(a.y, b.y) + rmax;
-                            sb.s0[j] = load_half4(R.atlas + t0 * 4);
-                            sb.s1[j] = load_half4(R.atlas + t1 * 4);
-                            sb.vis[j] = __half2float(R.history[(P.hist_in & 1u) ^ 1u][t0 * 2]);
-                            v = 1u;
-                        }
-                    }
-                    sb.valid[j] = v;
-                }
-                __syncthreads();
-                for (uint32_t g = 0; g < kColorBatch; g += 4u) {
-                    float4 part = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-                    float pd = 0.0f;
-                    const uint32_t bi = g + worker;
-                    if (!done && sb.valid[bi] && !(pcx < sb.mnx[bi] || pcy < sb.mny[bi]) &&
-                        !(pcx > sb.mxx[bi] || pcy > sb.mxy[bi])) {
-                        float t = ((pcx - sb.p0x[bi]) * sb.abx[bi] + (pcy - sb.p0y[bi]) * sb.aby[bi]) * sb.inv_len[bi];
-                        if (t >= 0.0f && t <= 1.0f) {
-                            float fx = sb.p0x[bi] + sb.abx[bi] * t, fy = sb.p0y[bi] + sb.aby[bi] * t;
-                            float pz = wmix(sb.z0[bi], sb.z1[bi], t);
-                            float rmin = wmax(sb.rmin[bi], 1e-4f);
-                            float rr = wmix(rmin, wmax(sb.rmax[bi], rmin), wclamp(normalize_depth01(pz), 0.0f, 1.0f));
-                            float dx = pcx - fx, dy = pcy - fy;
-                            float d2 = dx * dx + dy * dy;
-                            if (d2 < rr * rr) {
-                                float cov = wclamp(1.0f - sqrtf(d2) / rr, 0.0f, 1.0f);
-                                // perspective_correct_line_t (:149-154)
-                                float aw0 = wmax(fabsf(sb.w0[bi]), 1e-6f), aw1 = wmax(fabsf(sb.w1[bi]), 1e-6f);
-                                float tw = (t * aw0) / ((1.0f - t) * aw1 + t * aw0);
-                                float4 s0 = sb.s0[bi], s1 = sb.s1[bi];
-                                float sr = wmix(s0.x, s1.x, tw), sg = wmix(s0.y, s1.y, tw);
-                                float sbl = wmix(s0.z, s1.z, tw), sa = wmix(s0.w, s1.w, tw);
-                                float alpha = sa * cov;
-                                float vsb = sb.vis[bi];
-                                part = make_float4(sr * vsb * alpha, sg * vsb * alpha, sbl * vsb * alpha, alpha);
-                                pd = pz;
-                                ++frags;
-                            }
-                        }
-                    }
-                    // (w0 over w1) over (w2 over w3), depth max.
-                    float4 rhs;
-                    rhs.x = __shfl_sync(0xFFFFFFFFu, part.x, wbase + (worker | 1u));
-                    rhs.y = __shfl_sync(0xFFFFFFFFu, part.y, wbase + (worker | 1u));
-                    rhs.z = __shfl_sync(0xFFFFFFFFu, part.z, wbase + (worker | 1u));
-                    rhs.w = __shfl_sync(0xFFFFFFFFu, part.w, wbase + (worker | 1u));
-                    float rd = __shfl_sync(0xFFFFFFFFu, pd, wbase + (worker | 1u));
-                    float4 pair = part;
-                    float pdd = pd;
-                    if ((worker & 1u) == 0u) {
-                        pair = over(part, rhs);
-                        pdd = wmax(pd, rd);
-                    }
-                    float4 second;
-                    second.x = __shfl_sync(0xFFFFFFFFu, pair.x, wbase + 2u);
-                    second.y = __shfl_sync(0xFFFFFFFFu, pair.y, wbase + 2u);
-                    second.z = __shfl_sync(0xFFFFFFFFu, pair.z, wbase + 2u);
-                    second.w = __shfl_sync(0xFFFFFFFFu, pair.w, wbase + 2u);
-                    float sdp = __shfl_sync(0xFFFFFFFFu, pdd, wbase + 2u);
-                    if (worker == 0u && !done) {
-                        fin = over(fin, over(pair, second));
-                        gdepth = wmax(gdepth, wmax(pdd, sdp));
-                    }
-                }
-            }
-            if (worker == 0u && !done && fin.w > 0.98f) {
-                fin = make_float4(fin.x / fin.w, fin.y / fin.w, fin.z / fin.w, 1.0f);
-                done = true;
-            }
-            done = __shfl_sync(0xFFFFFFFFu, done, wbase);
-            if (__syncthreads_and(done)) break;
-        }
-        // Sum the fragment counts of the 4 workers.
-        frags += __shfl_xor_sync(0xFFFFFFFFu, frags, 1);
-        frags += __shfl_xor_sync(0xFFFFFFFFu, frags, 2);
-        if (worker == 0u && active) {
-            float4 o = fin;
-            if (o.w > 1e-6f && o.w < 1.0f) o = make_float4(o.x / o.w, o.y / o.w, o.z / o.w, o.w);
-            size_t pi = (size_t)py * P.width + px;
-            __half2 lo = __halves2half2(__float2half_rn(o.x), __float2half_rn(o.y));
-            __half2 hi = __halves2half2(__float2half_rn(o.z), __float2half_rn(o.w));
-            reinterpret_cast<uint2*>(R.color)[pi] = make_uint2(*reinterpret_cast<uint32_t*>(&lo), *reinterpret_cast<uint32_t*>(&hi));
-            R.depth[pi] = gdepth;
-            if (P.fragment_counts) R.fragments[pi] = frags;
-        }
-    }
-}
-
-// ===========================================================================
 // K20 composite (strand_composite.wgsl:12-33) with BlendState::ALPHA_BLENDING
 // onto the loaded destination (pipelines/composite.rs:115-124).
 // ===========================================================================
@@ -643,14 +261,8 @@ __global__ void k_composite(CompositeArgs C) {
     }
 }
 
-void launch_shadow(const LaunchCtx& L, const RenderArgs& R) {
-    k_shadow<<<L.sm_count * 4, 256, 0, L.stream>>>(L.P, L.inst, R);
-}
 void launch_shade(const LaunchCtx& L, const RenderArgs& R) {
     k_shade<<<L.sm_count * 16, 128, 0, L.stream>>>(L.P, L.inst, R);
-}
-void launch_raster(const LaunchCtx& L, const RenderArgs& R) {
-    k_raster<<<L.sm_count * 6, 256, 0, L.stream>>>(L.P, L.inst, R);
 }
 void launch_composite(cudaStream_t s, const CompositeArgs& C) {
     unsigned blocks = ceil_div_host((uint64_t)C.width * C.height, 256);

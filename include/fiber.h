@@ -352,6 +352,18 @@ fiber_status fiber_composite(fiber_ctx* ctx, uint32_t view, const fiber_image* s
 fiber_status fiber_frame_fused(fiber_ctx* ctx, const fiber_image* scene_color,
                                const fiber_image* scene_depth, fiber_image* out, void* stream);
 
+/* One whole frame from host memory to host memory: copies the scene colour
+ * (RGBA16F, width x height of the camera) and optional scene depth (R32F)
+ * from host buffers (pinned for asynchronous copies), runs every node as
+ * fiber_frame_fused does, and copies the composited RGBA16F image back into
+ * out_rgba16f_host. Call after fiber_frame_begin; returns when the copies are
+ * queued on `stream` (synchronise the stream before reading the output).
+ * This is the whole render-graph slice of src/plugin.rs:240-260 seen from a
+ * host that owns its images, e.g. a Rust caller over the FFI. */
+fiber_status fiber_render_host(fiber_ctx* ctx, const void* scene_rgba16f_host,
+                               const float* scene_depth_host, void* out_rgba16f_host,
+                               void* stream);
+
 /* ------------------------------------------------------------------------ */
 /* Readback                                                                  */
 /* ------------------------------------------------------------------------ */
