@@ -139,7 +139,7 @@ EXPORTS = [
     "fiber_slab_alloc", "fiber_slab_upload", "fiber_slab_free", "fiber_instance_set", "fiber_frame_begin",
     "fiber_prepass", "fiber_shadows", "fiber_shading", "fiber_raster", "fiber_composite", "fiber_frame_fused",
     "fiber_render_host", "fiber_stats_get", "fiber_dump", "fiber_output_image", "fiber_span_count", "fiber_span_name",
-    "fiber_span_times", "fiber_status_string",
+    "fiber_span_times", "fiber_status_string", "fiber_prefix_pages_noalloc",
 ]
 
 _LIB = None
@@ -185,6 +185,7 @@ def load_library(path: Path | str | None = None) -> C.CDLL:
         "fiber_span_name": (C.c_char_p, [u32]),
         "fiber_span_times": (C.c_int, [vp, pp(f32), u32]),
         "fiber_status_string": (C.c_char_p, [C.c_int]),
+        "fiber_prefix_pages_noalloc": (C.c_int, [vp, u32, vp, vp, vp, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

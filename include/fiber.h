@@ -384,6 +384,27 @@ const char* fiber_span_name(uint32_t i);
 fiber_status fiber_span_times(fiber_ctx* ctx, float* ms, uint32_t n);
 const char* fiber_status_string(fiber_status s);
 
+/* ------------------------------------------------------------------------ */
+/* Page prefix without device allocation (no counterpart in the reference)   */
+/* ------------------------------------------------------------------------ */
+/* The froxel-page prefix of fiber_prepass as a standalone call for callers
+ * that cannot allocate device memory where they run it: an engine that hands
+ * out all GPU memory from its own pool, or code inside CUDA stream capture,
+ * where cudaMalloc is not allowed. All buffers are the caller's device
+ * memory: counts[pages * 256] (froxel counts, cell = (z * 4 + y) * 4 + x),
+ * offsets[pages * 256] (exclusive prefix within each page), page_base[pages]
+ * (first reference of each page, pages in order; 0 for an empty page) and
+ * totals[2] (total references; non-zero if a bounded device wait gave up).
+ * The only scratch is a fixed file-scope device array (8 B per page, for at
+ * most 65536 pages = 512 KiB) that every GPU loading the library keeps until
+ * exit; more pages return FIBER_EINVAL. Nothing is allocated or freed. The
+ * first call on a device looks up the array's address with that device
+ * current, so make it before any stream capture. Every call shares the array
+ * and clears the part it uses: calls that overlap on the GPU (two streams, or
+ * two host threads on one device) race. Work is queued on `stream`. */
+fiber_status fiber_prefix_pages_noalloc(const uint32_t* counts, uint32_t pages, uint32_t* offsets,
+                                        uint32_t* page_base, uint32_t* totals, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
