@@ -170,6 +170,11 @@ def algorithmic_bytes(st, w, n_lights: int, K: int, D: int) -> dict:
     return {"per_kernel": per, "frame": total, "min": b_min}
 
 
+# Kernels one fused frame launches: broad, lut, fine, traverse<mark>, alloc,
+# zero_pages, traverse<count>, prefix_pages, traverse<fill>, compact_active,
+# emit, sort_cells, sort_big_cells, shadow, shade, raster, composite.
+KERNELS_PER_FRAME = 17
+
 SPAN_TO_KERNEL = {
     "strand_prepass/fine": "k_fine",
     "strand_prepass/mark_count_pages": "k_traverse_mark",
@@ -419,7 +424,7 @@ def fiber_arm(args):
                                "frac": frame_gbs / peak},
             "cpu_baseline": cpu,
             "clocks": clk,
-            "gpu_launches": 16 * args.steps,
+            "gpu_launches": KERNELS_PER_FRAME * args.steps,
             "spans_ms": span_med,
             "counts": {"binning_tasks": st.binning_tasks, "camera_tasks": st.camera_tasks,
                        "pages": st.allocated_pages, "fine_refs": st.fine_refs, "work_items": st.work_items,

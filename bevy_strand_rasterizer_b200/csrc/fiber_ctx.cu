@@ -278,6 +278,7 @@ fiber_status run_prepass(fiber_ctx* c, cudaStream_t s) {
     record(c, 8, s);
     set_stage(c, A, kStageEmit);
     launch_emit(L, A);
+    launch_sort_cells(L, A);
     launch_sort_big(L, A);
     return check_launch();
 }

@@ -122,6 +122,7 @@ void launch_prefix(const LaunchCtx& L, const PrepassArgs& A);
 void launch_fill(const LaunchCtx& L, const PrepassArgs& A);
 void launch_compact_active(const LaunchCtx& L, const PrepassArgs& A);
 void launch_emit(const LaunchCtx& L, const PrepassArgs& A);
+void launch_sort_cells(const LaunchCtx& L, const PrepassArgs& A);
 void launch_sort_big(const LaunchCtx& L, const PrepassArgs& A);
 
 void launch_shadow(const LaunchCtx& L, const RenderArgs& R, uint32_t K);

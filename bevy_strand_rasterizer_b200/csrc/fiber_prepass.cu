@@ -679,42 +679,82 @@ __global__ void __launch_bounds__(kScanThreads) k_compact_active(const FramePara
 
 // ===========================================================================
 // K14: emit raster work per active fine tile (256 lanes = 16 coarse z x 16
-// fine z, near to far), and put every cell's references into canonical order
-// (projected depth key descending, then instance, then segment). Cells of up
-// to 32 references are sorted by one warp in registers; larger cells are
-// queued for k_sort_big_cells.
+// fine z, near to far); work bases from a look-back over active tiles. The
+// canonical order inside each cell (projected depth key descending, then
+// instance, then segment) is made by k_sort_cells after the fill.
 // ===========================================================================
 __device__ __forceinline__ unsigned long long ref_sort_key(uint32_t key17, uint32_t inst, uint32_t seg) {
     return ((unsigned long long)(0x1FFFFu - (key17 & 0x1FFFFu)) << 47) |
            ((unsigned long long)(inst & 0x7FFFu) << 32) | (unsigned long long)seg;
 }
 
+// One warp sorts a cell of up to 32 * R references in registers: element
+// e = lane * R + r, bitonic network over 32 R keys (padding sorts last).
+// Strides below R compare registers of one lane; larger strides exchange the
+// same register with lane ^ (stride / R).
+template <int R>
 __device__ __forceinline__ void warp_sort_cell(const PrepassArgs& A, uint32_t base, uint32_t n, int lane) {
-    unsigned long long k = ~0ull;
-    uint32_t mat = 0u;
-    if ((uint32_t)lane < n) {
-        fiber_fine_seg_ref r = A.refs[base + lane];
-        k = ref_sort_key(A.ref_keys[base + lane], r.inst_id, r.seg_id);
-        mat = r.material_idx;
-    }
-    // Bitonic sort over 32 lanes, ascending by k.
+    unsigned long long k[R];
+    uint32_t mat[R];
 #pragma unroll
-    for (int size = 2; size <= 32; size <<= 1) {
-#pragma unroll
-        for (int stride = size >> 1; stride > 0; stride >>= 1) {
-            unsigned long long ok = __shfl_xor_sync(0xFFFFFFFFu, k, stride);
-            uint32_t om = __shfl_xor_sync(0xFFFFFFFFu, mat, stride);
-            bool up = ((lane & size) == 0);
-            bool lower = (lane & stride) == 0;
-            bool take_other = lower == up ? (ok < k) : (ok > k);
-            if (take_other) { k = ok; mat = om; }
+    for (int r = 0; r < R; ++r) {
+        const uint32_t e = (uint32_t)lane * R + r;
+        k[r] = ~0ull;
+        mat[r] = 0u;
+        if (e < n) {
+            fiber_fine_seg_ref ref = A.refs[base + e];
+            k[r] = ref_sort_key(A.ref_keys[base + e], ref.inst_id, ref.seg_id);
+            mat[r] = ref.material_idx;
         }
     }
-    if ((uint32_t)lane < n) {
-        uint32_t key17 = 0x1FFFFu - (uint32_t)(k >> 47);
-        A.refs[base + lane] = fiber_fine_seg_ref{(uint32_t)(k >> 32) & 0x7FFFu, (uint32_t)k, mat};
-        A.ref_keys[base + lane] = key17;
+#pragma unroll
+    for (int size = 2; size <= 32 * R; size <<= 1) {
+#pragma unroll
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            if (stride >= R) {
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    const int e = lane * R + r;
+                    unsigned long long ok = __shfl_xor_sync(0xFFFFFFFFu, k[r], stride / R);
+                    uint32_t om = __shfl_xor_sync(0xFFFFFFFFu, mat[r], stride / R);
+                    const bool up = (e & size) == 0;
+                    const bool lower = (e & stride) == 0;
+                    const bool take_other = lower == up ? (ok < k[r]) : (ok > k[r]);
+                    if (take_other) { k[r] = ok; mat[r] = om; }
+                }
+            } else {
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    const int r2 = r ^ stride;
+                    if (r2 > r) {
+                        const int e = lane * R + r;
+                        const bool up = (e & size) == 0;
+                        if (up ? (k[r] > k[r2]) : (k[r] < k[r2])) {
+                            unsigned long long tk = k[r]; k[r] = k[r2]; k[r2] = tk;
+                            uint32_t tm = mat[r]; mat[r] = mat[r2]; mat[r2] = tm;
+                        }
+                    }
+                }
+            }
+        }
     }
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const uint32_t e = (uint32_t)lane * R + r;
+        if (e < n) {
+            A.refs[base + e] = fiber_fine_seg_ref{(uint32_t)(k[r] >> 32) & 0x7FFFu, (uint32_t)k[r], mat[r]};
+            A.ref_keys[base + e] = 0x1FFFFu - (uint32_t)(k[r] >> 47);
+        }
+    }
+}
+
+constexpr uint32_t kWarpSortMax = 256;  // 32 lanes x 8 registers
+
+__device__ __forceinline__ void warp_sort_any(const PrepassArgs& A, uint32_t base, uint32_t n, int lane) {
+    if (n <= 32u) warp_sort_cell<1>(A, base, n, lane);
+    else if (n <= 64u) warp_sort_cell<2>(A, base, n, lane);
+    else if (n <= 128u) warp_sort_cell<4>(A, base, n, lane);
+    else warp_sort_cell<8>(A, base, n, lane);
 }
 
 __global__ void __launch_bounds__(256) k_emit(const FrameParams* __restrict__ Pp, PrepassArgs A) {
@@ -722,12 +762,10 @@ __global__ void __launch_bounds__(256) k_emit(const FrameParams* __restrict__ Pp
     __shared__ uint32_t s_tile, s_base;
     __shared__ uint32_t s_warp[33];
     __shared__ uint32_t s_load[8];
-    __shared__ uint32_t s_sort_n;
-    __shared__ uint2 s_sort[256];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t n_active = *((volatile uint32_t*)&A.counters->active_tiles);
     for (;;) {
-        if (threadIdx.x == 0) { s_tile = atomicAdd(A.tile_counter, 1u); s_sort_n = 0u; }
+        if (threadIdx.x == 0) s_tile = atomicAdd(A.tile_counter, 1u);
         __syncthreads();
         const uint32_t a = s_tile;
         if (a >= n_active) break;
@@ -756,14 +794,6 @@ __global__ void __launch_bounds__(256) k_emit(const FrameParams* __restrict__ Pp
                 }
             }
         }
-        // Canonical order inside each cell.
-        if (cnt > 32u) {
-            uint32_t slot = atomicAdd(&A.counters->big_cells, 1u);
-            A.big_cells[slot] = make_uint2(base, cnt);
-        } else if (cnt >= 2u) {
-            uint32_t slot = atomicAdd(&s_sort_n, 1u);
-            s_sort[slot] = make_uint2(base, cnt);
-        }
         const uint32_t has = cnt > 0u ? 1u : 0u;
         uint32_t load = cnt;
         for (int o = 16; o > 0; o >>= 1) load += __shfl_xor_sync(0xFFFFFFFFu, load, o);
@@ -789,9 +819,36 @@ __global__ void __launch_bounds__(256) k_emit(const FrameParams* __restrict__ Pp
             else
                 atomicOr(&A.counters->overflow, 8u);
         }
-        const uint32_t n_sort = s_sort_n;
-        for (uint32_t j = warp; j < n_sort; j += 8u) warp_sort_cell(A, s_sort[j].x, s_sort[j].y, lane);
         __syncthreads();
+    }
+}
+
+// Canonical order inside every cell (projected depth key descending, then
+// instance, then segment), after the fill: one block per page, one warp per 32
+// cells; each warp sorts its cells of 2..256 references in registers and
+// queues longer cells for k_sort_big_cells. Warps never wait on each other.
+__global__ void __launch_bounds__(256) k_sort_cells(PrepassArgs A) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t pages = *((volatile uint32_t*)&A.counters->pages);
+    for (uint32_t page = blockIdx.x; page < pages; page += gridDim.x) {
+        const fiber_fine_page_meta pm = A.page_meta[page];
+        if (pm.seg_ref_count == 0u || pm.flags != 0u) continue;
+        const uint32_t cell = (uint32_t)warp * 32u + (uint32_t)lane;
+        const size_t g = (size_t)page * kPageSize + cell;
+        const uint32_t cnt = A.counts[g];
+        const uint32_t base = pm.seg_ref_base + A.offsets[g];
+        if (cnt > kWarpSortMax) {
+            uint32_t slot = atomicAdd(&A.counters->big_cells, 1u);
+            A.big_cells[slot] = make_uint2(base, cnt);
+        }
+        unsigned todo = __ballot_sync(0xFFFFFFFFu, cnt >= 2u && cnt <= kWarpSortMax);
+        while (todo) {
+            const int src = __ffs(todo) - 1;
+            todo &= todo - 1u;
+            const uint32_t b = __shfl_sync(0xFFFFFFFFu, base, src);
+            const uint32_t n = __shfl_sync(0xFFFFFFFFu, cnt, src);
+            warp_sort_any(A, b, n, lane);
+        }
     }
 }
 
@@ -915,6 +972,9 @@ void launch_compact_active(const LaunchCtx& L, const PrepassArgs& A) {
 }
 void launch_emit(const LaunchCtx& L, const PrepassArgs& A) {
     k_emit<<<L.sm_count * 6, 256, 0, L.stream>>>(L.P, A);
+}
+void launch_sort_cells(const LaunchCtx& L, const PrepassArgs& A) {
+    k_sort_cells<<<L.sm_count * 8, 256, 0, L.stream>>>(A);
 }
 void launch_sort_big(const LaunchCtx& L, const PrepassArgs& A) {
     static bool configured[64] = {};

@@ -130,32 +130,38 @@ __device__ F3 marschner(F3 L, F3 V, F3 U, const fiber_strand_material& m, float 
     float eta_prime = sqrtf(wmax(0.0f, m.eta * m.eta - sti * sti)) / ctd;
     float mup[3] = {sig[0] / ctd, sig[1] / ctd, sig[2] / ctd};
     float cos_td = cosf(theta_d);
-    for (uint32_t p = 0; p < 3u; ++p) {
-        float acc[3] = {0.0f, 0.0f, 0.0f};
-        for (uint32_t i = 0; i < 10u; ++i) {
-            float h = wclamp(-1.0f + 1e-6f, 1.0f - 1e-6f, c_leg_roots[i]);
-            // A (:383-413)
-            float gamma_t = asinf(h / eta_prime);
-            float gamma_i = asinf(h);
-            float fr = fresnel_reflectance(1.0f, m.eta, acosf(cos_td * cosf(gamma_i)));
-            float c2 = 1.0f + cosf(2.0f * gamma_t);
-            float T[3] = {expf(-2.0f * mup[0] * c2), expf(-2.0f * mup[1] * c2), expf(-2.0f * mup[2] * c2)};
+    // The quadrature point's Fresnel, absorption and azimuth terms depend on
+    // the segment only, not on the path p, so they are evaluated once per point
+    // and reused by the three paths; each path's sum keeps its order (i = 0..9).
+    float acc[3][3] = {{0.0f, 0.0f, 0.0f}, {0.0f, 0.0f, 0.0f}, {0.0f, 0.0f, 0.0f}};
+    for (uint32_t i = 0; i < 10u; ++i) {
+        float h = wclamp(-1.0f + 1e-6f, 1.0f - 1e-6f, c_leg_roots[i]);
+        // A (:383-413)
+        float gamma_t = asinf(h / eta_prime);
+        float gamma_i = asinf(h);
+        float fr = fresnel_reflectance(1.0f, m.eta, acosf(cos_td * cosf(gamma_i)));
+        float c2 = 1.0f + cosf(2.0f * gamma_t);
+        float T[3] = {expf(-2.0f * mup[0] * c2), expf(-2.0f * mup[1] * c2), expf(-2.0f * mup[2] * c2)};
+        float f_ = 1.0f - fr;
+        // Phi (:464-468)
+        float gt2 = asinf(wclamp(h / eta_prime, -1.0f, 1.0f));
+        float asin_h = asinf(h);
+        for (uint32_t p = 0; p < 3u; ++p) {
             float A[3];
             if (p == 0u) {
                 for (int q = 0; q < 3; ++q) A[q] = fr * T[q] * T[q];
             } else {
-                float f_ = 1.0f - fr;
                 float k = (f_ * f_) * powf(fr, u2f(p - 1u));
                 for (int q = 0; q < 3; ++q) A[q] = k * powf(T[q], u2f(p));
             }
-            // Phi (:464-468)
-            float gt2 = asinf(wclamp(h / eta_prime, -1.0f, 1.0f));
-            float shift = 2.0f * u2f(p) * gt2 - 2.0f * asinf(h) + u2f(p) * kPi;
+            float shift = 2.0f * u2f(p) * gt2 - 2.0f * asin_h + u2f(p) * kPi;
             float det = gaussian_detector(beta_azim, phi - shift);
-            for (int q = 0; q < 3; ++q) acc[q] = acc[q] + A[q] * det * c_leg_weights[i];
+            for (int q = 0; q < 3; ++q) acc[p][q] = acc[p][q] + A[q] * det * c_leg_weights[i];
         }
+    }
+    for (uint32_t p = 0; p < 3u; ++p) {
         float wgt = (u2f(p + 1u) * vis) / 3.0f;
-        for (int q = 0; q < 3; ++q) tot[q] = tot[q] + (acc[q] * 0.5f) * wgt;
+        for (int q = 0; q < 3; ++q) tot[q] = tot[q] + (acc[p][q] * 0.5f) * wgt;
     }
     return f3(tot[0], tot[1], tot[2]);
 }
