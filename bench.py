@@ -138,10 +138,12 @@ def algorithmic_bytes(st, w, n_lights: int, K: int, D: int) -> dict:
 
     Per unit: 20 B / point + 16 B / strand (vertex float4 + index, meta), 28 B per
     binning task written and read (BinningTask 16 + ProjectedSegment 12), 8 B per
-    allocated cell (count + offset), 24 B per fine ref (written + read), 64 B per
-    work item / tile run (written + read), 40 B per ref of endpoint gather in the
-    rasters, 40 + 8 L B per camera segment in shading, 12 B per camera pixel
-    (RGBA16F + R32F), 4 (K + 1) B per deep-opacity texel.
+    allocated cell (count + offset), 24 B per fine ref (written + read), 32 B per
+    visit record (k_visit writes slot/cell + task, k_count_visits reads 4 and
+    writes cell + rank, k_fill_visits reads 12), 64 B per work item / tile run
+    (written + read), 40 B per ref of endpoint gather in the rasters, 40 + 8 L B
+    per camera segment in shading, 12 B per camera pixel (RGBA16F + R32F),
+    4 (K + 1) B per deep-opacity texel. Visits are counted as fine refs.
     """
     F = st.frustum_count
     P, S = st.total_points, st.total_strands
@@ -154,33 +156,35 @@ def algorithmic_bytes(st, w, n_lights: int, K: int, D: int) -> dict:
     dom = n_lights * 4 * (K + 1) * D * D
     per = {
         "k_fine": 20 * P + 16 * S + sum(28 * n for n in tasks),
-        "k_traverse_mark": sum(28 * n for n in tasks),
-        "k_traverse_count": sum(28 * n for n in tasks),
-        "k_traverse_fill": sum(28 * n for n in tasks) + sum(12 * r for r in refs),
+        "k_visit": sum(28 * n for n in tasks) + sum(8 * r for r in refs),
+        "k_count_visits": sum(16 * r for r in refs),
+        "k_fill_visits": sum((12 + 4 + 20 + 16) * r for r in refs),
         "k_prefix_pages": sum(8 * 256 * p for p in pages),
         "k_emit": sum(32 * (wk + t) for wk, t in zip(work, runs)),
         "k_shadow": sum(52 * refs[f] + 32 * (work[f] + runs[f]) for f in range(1, F)) + dom,
         "k_shade": st.camera_tasks * (40 + 8 * n_lights),
         "k_raster": 52 * refs[0] + 32 * (work[0] + runs[0]) + 12 * WH,
     }
-    total = (20 * P + 16 * S + sum(56 * n + 8 * 256 * p + 24 * r + 64 * (wk + t) + 40 * r
+    total = (20 * P + 16 * S + sum(56 * n + 8 * 256 * p + 24 * r + 32 * r + 64 * (wk + t) + 40 * r
                                    for n, p, r, wk, t in zip(tasks, pages, refs, work, runs))
              + st.camera_tasks * (40 + 8 * n_lights) + 12 * WH + dom)
     b_min = 20 * P + 16 * S + 12 * WH + dom
     return {"per_kernel": per, "frame": total, "min": b_min}
 
 
-# Kernels one fused frame launches: broad, lut, fine, traverse<mark>, alloc,
-# zero_pages, traverse<count>, prefix_pages, traverse<fill>, compact_active,
-# emit, sort_cells, sort_big_cells, shadow, shade, raster, composite.
-KERNELS_PER_FRAME = 17
+# Kernels one fused frame launches: broad, lut, fine, visit, alloc, zero_pages,
+# count_visits, traverse<count> (returns at once unless the visit records did
+# not fit), prefix_pages, fill_visits, traverse<fill> (likewise),
+# compact_active, emit, sort_cells, sort_big_cells, shadow, shade, raster,
+# composite.
+KERNELS_PER_FRAME = 19
 
 SPAN_TO_KERNEL = {
     "strand_prepass/fine": "k_fine",
-    "strand_prepass/mark_count_pages": "k_traverse_mark",
-    "strand_prepass/binning": "k_traverse_count",
+    "strand_prepass/mark_count_pages": "k_visit",
+    "strand_prepass/binning": "k_count_visits",
     "strand_prepass/prefix_fine_pages": "k_prefix_pages",
-    "strand_prepass/fill_segment_refs": "k_traverse_fill",
+    "strand_prepass/fill_segment_refs": "k_fill_visits",
     "strand_prepass/emit_raster_work": "k_emit",
     "strand_shadow_rasterizer/rasterize": "k_shadow",
     "strand_shading/shade": "k_shade",

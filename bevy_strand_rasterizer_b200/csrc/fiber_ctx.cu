@@ -106,6 +106,7 @@ struct fiber_ctx {
     DevBuf d_params, d_inst, d_counters, d_lb, d_range_valid, d_ranges, d_keep, d_inst_visible, d_inst_keep;
     DevBuf d_lut, d_tasks, d_projected, d_page_table, d_page_meta, d_counts, d_offsets, d_cursors;
     DevBuf d_refs, d_ref_keys, d_active_flags, d_active_list, d_work, d_runs, d_big_cells;
+    DevBuf d_visit_rec, d_visit_task, d_visit_rank;
     DevBuf d_dom_depth, d_dom_opacity, d_shadow_map, d_atlas, d_history[2];
     DevBuf d_color, d_depth, d_fragments, d_validate, d_host_scene, d_host_depth;
     int hist_cur = 0;
@@ -201,6 +202,9 @@ PrepassArgs prepass_args(fiber_ctx* c) {
     A.work = dp<fiber_raster_work_item>(c->d_work);
     A.runs = dp<fiber_raster_tile_run>(c->d_runs);
     A.big_cells = dp<uint2>(c->d_big_cells);
+    A.visit_rec = dp<uint32_t>(c->d_visit_rec);
+    A.visit_task = dp<uint32_t>(c->d_visit_task);
+    A.visit_rank = dp<uint32_t>(c->d_visit_rank);
     return A;
 }
 
@@ -260,7 +264,7 @@ fiber_status run_prepass(fiber_ctx* c, cudaStream_t s) {
     set_stage(c, A, kStageFine);
     launch_fine(L, A);
     record(c, 2, s);
-    launch_mark(L, A);
+    launch_visit(L, A);
     record(c, 3, s);
     set_stage(c, A, kStageAlloc);
     launch_alloc(L, A);
@@ -423,7 +427,8 @@ fiber_status fiber_ctx_destroy(fiber_ctx* c) {
                       &c->d_ref_keys, &c->d_active_flags, &c->d_active_list, &c->d_work, &c->d_runs,
                       &c->d_big_cells, &c->d_dom_depth, &c->d_dom_opacity, &c->d_shadow_map, &c->d_atlas,
                       &c->d_history[0], &c->d_history[1], &c->d_color, &c->d_depth, &c->d_fragments,
-                      &c->d_validate, &c->d_host_scene, &c->d_host_depth};
+                      &c->d_validate, &c->d_host_scene, &c->d_host_depth, &c->d_visit_rec,
+                      &c->d_visit_task, &c->d_visit_rank};
     for (DevBuf* b : bufs) release(c, *b);
     for (int i = 0; i <= kSpanCount; ++i)
         if (c->ev[i]) cudaEventDestroy(c->ev[i]);
@@ -703,6 +708,13 @@ fiber_status fiber_frame_begin(fiber_ctx* c, const fiber_froxel_config* cam_cfg,
     ENSURE(c->d_work, work_cap * sizeof(fiber_raster_work_item), false);
     ENSURE(c->d_runs, fine_tiles * sizeof(fiber_raster_tile_run), false);
     ENSURE(c->d_big_cells, (ref_cap / 33 + 1) * sizeof(uint2), false);
+    // Visit records (page-table slot << 8 | cell) hold up to ref_capacity visits;
+    // slots must fit 24 bits, else count and fill walk the tasks.
+    P.visit_records = table < (1ull << 24) ? 1u : 0u;
+    const uint64_t visit_cap = P.visit_records ? ref_cap : 1u;
+    ENSURE(c->d_visit_rec, visit_cap * 4, false);
+    ENSURE(c->d_visit_task, visit_cap * 4, false);
+    ENSURE(c->d_visit_rank, visit_cap * 4, false);
     ENSURE(c->d_dom_depth, L * D * D * 4, false);
     ENSURE(c->d_dom_opacity, L * K * D * D * 4, true);
     ENSURE(c->d_shadow_map, L * S * S * 4, false);

@@ -69,6 +69,7 @@ struct FrameParams {
     uint32_t width, height;       // camera resolution
     uint32_t epoch;               // look-back status epoch of this frame
     uint32_t hist_in;             // shadow-history buffer read this frame (0/1)
+    uint32_t visit_records;       // page-table slots fit 24 bits: count/fill stream visit records
 };
 
 // Device counters of one frame (zeroed at frame start).
@@ -85,8 +86,11 @@ struct FrameCounters {
     uint32_t error;               // kErrTimeout when a bounded wait gave up
     uint32_t big_cells;           // cells queued for the large-cell sort
     uint32_t tile_counter[8];     // virtual block ids of the look-back stages
-    uint32_t pad[5];
+    uint32_t visit_overflow;      // visit records unused this frame (did not fit, or disabled)
+    unsigned long long visits;    // visit records appended by k_visit
+    uint32_t pad[2];
 };
+static_assert(sizeof(FrameCounters) == 160, "FrameCounters layout");
 
 // Look-back stages (index into FrameCounters::tile_counter and the status regions).
 enum LookbackStage : uint32_t { kStageFine = 0, kStageAlloc = 1, kStagePrefix = 2, kStageActive = 3, kStageEmit = 4, kStageCount = 5 };

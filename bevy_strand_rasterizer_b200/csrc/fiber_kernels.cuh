@@ -72,6 +72,9 @@ struct PrepassArgs {
     fiber_raster_work_item* work;
     fiber_raster_tile_run* runs;
     uint2* big_cells;
+    uint32_t* visit_rec;    // [ref_capacity] page-table slot << 8 | cell; the count pass rewrites it to the cell index
+    uint32_t* visit_task;   // [ref_capacity] binning task of the visit
+    uint32_t* visit_rank;   // [ref_capacity] rank of the visit inside its cell
 };
 
 // Device buffers of the shadow, shading, raster and composite stages.
@@ -114,7 +117,7 @@ struct LaunchCtx {
 void launch_broad(const LaunchCtx& L, const PrepassArgs& A);
 void launch_lut(const LaunchCtx& L, const PrepassArgs& A);
 void launch_fine(const LaunchCtx& L, const PrepassArgs& A);
-void launch_mark(const LaunchCtx& L, const PrepassArgs& A);
+void launch_visit(const LaunchCtx& L, const PrepassArgs& A);
 void launch_alloc(const LaunchCtx& L, const PrepassArgs& A);
 void launch_zero_pages(const LaunchCtx& L, const PrepassArgs& A);
 void launch_count(const LaunchCtx& L, const PrepassArgs& A);

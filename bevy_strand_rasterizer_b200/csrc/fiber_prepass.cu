@@ -5,11 +5,11 @@
 //   broad_prepass + broad_strand_prepass (strand_prepass.wgsl:684-782) -> k_broad, folded into k_fine
 //   coarse_interval_pass + build_depth_warp_lut (:835-1014)           -> k_lut
 //   fine_prepass (:1016-1140)                                           -> k_fine (single-pass compaction)
-//   mark_coarse_count_pages_pass (:1928-1932)                           -> k_traverse<kMark>
+//   mark_coarse_count_pages_pass (:1928-1932)                           -> k_visit (+ visit records)
 //   allocate_coarse_count_pages (:1934-1969)                            -> k_alloc_pages (ordered)
-//   binning_queue_pass (:1986-1990)                                     -> k_traverse<kCount>
+//   binning_queue_pass (:1986-1990)                                     -> k_count_visits | k_traverse<kCount>
 //   prefix_fine_pages (:2051-2143)                                      -> k_prefix_pages
-//   fill_fine_seg_refs (:2190-2194)                                     -> k_traverse<kFill>
+//   fill_fine_seg_refs (:2190-2194)                                     -> k_fill_visits | k_traverse<kFill>
 //   prefix_active_tile_blocks + compact_active_tiles (:2581-2676)       -> k_compact_active
 //   emit_raster_work (:2678-2834)                                       -> k_emit (+ canonical cell order)
 // The finalize_* indirect-argument kernels disappear: every consumer is a
@@ -351,8 +351,21 @@ __global__ void __launch_bounds__(kFineThreads) k_fine(const FrameParams* __rest
 // ===========================================================================
 // K7 / K9 / K11 traversal: coarse-tile 2-D DDA, LUT slices, then the fine
 // 3-D DDA inside each page (strand_prepass.wgsl:1251-1696,1894-1926).
+//
+// The walk is written once; what a pass does at a page-table slot that
+// survives the depth clip, and at each fine cell the 3-D DDA visits, is a sink:
+//   VisitSink  k_visit: marks the slot (mark_coarse_count_pages_pass) and
+//              records the visit (slot << 8 | cell) in a per-thread buffer
+//   SpillSink  k_visit: re-walks a task with more visits than the buffer and
+//              writes the visits past it
+//   CountSink, FillSink  the walking form of binning_queue_pass and
+//              fill_fine_seg_refs, used only when the visit records did not fit
+// With the records, the count and fill passes stream over visits instead of
+// walking every task again (k_count_visits, k_fill_visits).
 // ===========================================================================
-enum : int { kMark = 0, kCount = 1, kFill = 2 };
+enum : int { kCount = 1, kFill = 2 };
+constexpr uint32_t kVisitThreads = 256;
+constexpr uint32_t kVisitSlots = 32;  // buffered visits per task; p99 is about 17 on the camera
 
 __device__ __forceinline__ uint32_t lut_slice(const fiber_coarse_depth_lut_entry* e, float z) {
     uint32_t zq = quantize_depth01(z);
@@ -367,27 +380,78 @@ __device__ __forceinline__ uint32_t lut_slice(const fiber_coarse_depth_lut_entry
     return best;
 }
 
-template <int PASS>
-__device__ __forceinline__ void emit_cell(const PrepassArgs& A, uint32_t page, uint32_t cell, uint32_t ref_seg,
-                                          uint32_t ref_inst, uint32_t ref_mat, uint32_t key) {
-    size_t g = (size_t)page * kPageSize + cell;
-    if (PASS == kCount) {
-        atomicAdd(A.counts + g, 1u);
-    } else {
-        fiber_fine_page_meta pm = A.page_meta[page];
-        if (pm.seg_ref_count == 0u) return;
-        uint32_t lw = atomicAdd(A.cursors + g, 1u);
-        uint64_t dst = (uint64_t)pm.seg_ref_base + A.offsets[g] + lw;
-        if (dst >= (uint64_t)(pm.seg_ref_base) + pm.seg_ref_count) return;
-        A.refs[dst] = fiber_fine_seg_ref{ref_inst, ref_seg, ref_mat};
-        A.ref_keys[dst] = key;
+// Sinks. page_slot(pti) returns whether to walk the slot's fine cells.
+struct VisitSink {
+    uint32_t* page_table;
+    uint32_t* buf;  // this thread's column of the block buffer (stride kVisitThreads)
+    uint32_t cur, n;
+    bool records;
+    __device__ __forceinline__ bool page_slot(uint32_t pti) {
+        page_table[pti] = kMarked;
+        cur = pti << 8;
+        return records;
     }
-}
+    __device__ __forceinline__ void cell(uint32_t c) {
+        if (n < kVisitSlots) buf[n * kVisitThreads] = cur | c;
+        ++n;
+    }
+};
 
-template <int PASS>
-__device__ void trace_page(const FrameParams& P, const PrepassArgs& A, F3 p0, F3 p1, const fiber_frustum_desc& d,
-                           uint32_t tile, uint32_t local, uint32_t ref_inst, uint32_t ref_seg, uint32_t ref_mat,
-                           uint32_t key) {
+struct SpillSink {
+    uint32_t* rec;
+    uint32_t* task;
+    uint32_t at, k, lim, cur, n;  // lim: visits the first walk counted (the room reserved)
+    __device__ __forceinline__ bool page_slot(uint32_t pti) {
+        cur = pti << 8;
+        return true;
+    }
+    __device__ __forceinline__ void cell(uint32_t c) {
+        if (n >= kVisitSlots && n < lim) {
+            rec[at + n] = cur | c;
+            task[at + n] = k;
+        }
+        ++n;
+    }
+};
+
+struct CountSink {
+    const uint32_t* page_table;
+    uint32_t* counts;
+    uint32_t page;
+    __device__ __forceinline__ bool page_slot(uint32_t pti) {
+        uint32_t h = page_table[pti];
+        if (h == 0u || h == kMarked) return false;
+        page = h - 1u;
+        return true;
+    }
+    __device__ __forceinline__ void cell(uint32_t c) { atomicAdd(counts + (size_t)page * kPageSize + c, 1u); }
+};
+
+struct FillSink {
+    const PrepassArgs* A;
+    uint32_t page, base, count, inst, seg, mat, key;
+    __device__ __forceinline__ bool page_slot(uint32_t pti) {
+        uint32_t h = A->page_table[pti];
+        if (h == 0u || h == kMarked) return false;
+        page = h - 1u;
+        const fiber_fine_page_meta pm = A->page_meta[page];
+        base = pm.seg_ref_base;
+        count = pm.seg_ref_count;
+        return count != 0u;
+    }
+    __device__ __forceinline__ void cell(uint32_t c) {
+        const size_t g = (size_t)page * kPageSize + c;
+        const uint32_t lw = atomicAdd(A->cursors + g, 1u);
+        const uint64_t dst = (uint64_t)base + A->offsets[g] + lw;
+        if (dst >= (uint64_t)base + count) return;
+        A->refs[dst] = fiber_fine_seg_ref{inst, seg, mat};
+        A->ref_keys[dst] = key;
+    }
+};
+
+template <class Sink>
+__device__ __forceinline__ void walk_page(const PrepassArgs& A, F3 p0, F3 p1, const fiber_frustum_desc& d,
+                                          uint32_t tile, uint32_t local, Sink& sink) {
     uint32_t ccx = local % d.coarse_tiles_x, ccy = local / d.coarse_tiles_x;
     uint32_t cpx = max(1u, d.froxel_size_x * kCoarseExtent);
     uint32_t cpy = max(1u, d.froxel_size_y * kCoarseExtent);
@@ -406,14 +470,7 @@ __device__ void trace_page(const FrameParams& P, const PrepassArgs& A, F3 p0, F3
         float zmin = dequantize_depth01(e.z_min_q), zmax = dequantize_depth01(e.z_max_q);
         F3 d0, d1;
         if (!clip_segment(c0, c1, f3(ox, oy, zmin), f3(bmax.x, bmax.y, zmax), d0, d1)) continue;
-        uint32_t pti = tile * kDepthSlices + cz;
-        if (PASS == kMark) {
-            A.page_table[pti] = kMarked;
-            continue;
-        }
-        uint32_t handle = A.page_table[pti];
-        if (handle == 0u || handle == kMarked) continue;
-        uint32_t page = handle - 1u;
+        if (!sink.page_slot(tile * kDepthSlices + cz)) continue;
         float zspan = wmax(zmax - zmin, 1.0f / (float)kDepthQuantMax);
         float fsx = u2f(d.froxel_size_x), fsy = u2f(d.froxel_size_y);
         float l0[3] = {(d0.x - ox) / fsx, (d0.y - oy) / fsy, wclamp((d0.z - zmin) / zspan, 0.0f, 0.999999f) * 16.0f};
@@ -438,7 +495,7 @@ __device__ void trace_page(const FrameParams& P, const PrepassArgs& A, F3 p0, F3
             if (safety > kCoarseExtent + kCoarseExtent + kDepthSlices + 3u) break;
             // fine_tile_occluded_by_opaque (:551-573): no opaque depth tiles are
             // bound on this path, so the cull never fires.
-            emit_cell<PASS>(A, page, (uint32_t)((fc[2] * 4 + fc[1]) * 4 + fc[0]), ref_seg, ref_inst, ref_mat, key);
+            sink.cell((uint32_t)((fc[2] * 4 + fc[1]) * 4 + fc[0]));
             if (fc[0] == f1[0] && fc[1] == f1[1] && fc[2] == f1[2]) break;
             float m = wmin(wmin(tm[0], tm[1]), tm[2]);  // canonical_min_mask
             int a = tm[0] == m ? 0 : (tm[1] == m ? 1 : 2);
@@ -451,68 +508,200 @@ __device__ void trace_page(const FrameParams& P, const PrepassArgs& A, F3 p0, F3
     }
 }
 
+// One binning task's walk inputs (binning_queue_pass preamble, :1894-1926).
+struct TaskWalk {
+    F3 p0, p1;        // projected endpoints in pixels / depth01
+    uint32_t f;       // frustum
+    uint32_t i, strand, seg;
+    uint32_t depths;  // packed projected depths (the sort key source)
+    uint32_t min_cx, max_cx, min_cy, max_cy;
+};
+
+__device__ __forceinline__ bool task_walk(const FrameParams& P, const PrepassArgs& A, uint32_t k, TaskWalk& w) {
+    const uint4 t = reinterpret_cast<const uint4*>(A.tasks)[k];
+    const uint32_t f = t.w >> 3u;
+    if (f >= P.F) return false;
+    const uint32_t i = t.x;
+    if (i >= P.I) return false;
+    const fiber_frustum_desc& d = P.frusta[f];
+    const fiber_projected_segment pr = A.projected[k];
+    const float sw = u2f(d.screen_width), sh = u2f(d.screen_height);
+    const float2 a = unpack2x16unorm(pr.p0_xy), b = unpack2x16unorm(pr.p1_xy), z = unpack2x16unorm(pr.depths);
+    const F3 p0 = f3(a.x * sw, a.y * sh, z.x), p1 = f3(b.x * sw, b.y * sh, z.y);
+    const uint32_t slot = i * P.F + f;
+    if (!A.range_valid[slot]) return false;
+    const fiber_coarse_asset_range r = A.ranges[slot];
+    const uint32_t cpx = max(1u, d.froxel_size_x * kCoarseExtent);
+    const uint32_t cpy = max(1u, d.froxel_size_y * kCoarseExtent);
+    w.min_cx = max(r.min_x, min(f2u(wmax(wmin(p0.x, p1.x), 0.0f)) / cpx, d.coarse_tiles_x - 1u));
+    w.max_cx = min(r.max_x, min(f2u(wmax(wmax(p0.x, p1.x), 0.0f)) / cpx, d.coarse_tiles_x - 1u));
+    w.min_cy = max(r.min_y, min(f2u(wmax(wmin(p0.y, p1.y), 0.0f)) / cpy, d.coarse_tiles_y - 1u));
+    w.max_cy = min(r.max_y, min(f2u(wmax(wmax(p0.y, p1.y), 0.0f)) / cpy, d.coarse_tiles_y - 1u));
+    if (w.max_cx < w.min_cx || w.max_cy < w.min_cy) return false;
+    w.p0 = p0;
+    w.p1 = p1;
+    w.f = f;
+    w.i = i;
+    w.strand = t.y;
+    w.seg = t.z;
+    w.depths = pr.depths;
+    return true;
+}
+
+// Coarse-tile 2-D DDA over the task's clipped range; each coarse tile is
+// walked by walk_page.
+template <class Sink>
+__device__ __forceinline__ void walk_task(const FrameParams& P, const PrepassArgs& A, const TaskWalk& w, Sink& sink) {
+    const fiber_frustum_desc& d = P.frusta[w.f];
+    const float sw = u2f(d.screen_width), sh = u2f(d.screen_height);
+    const uint32_t cpx = max(1u, d.froxel_size_x * kCoarseExtent);
+    const uint32_t cpy = max(1u, d.froxel_size_y * kCoarseExtent);
+    const uint32_t min_cx = w.min_cx, max_cx = w.max_cx, min_cy = w.min_cy, max_cy = w.max_cy;
+    F3 bmin = f3(u2f(min_cx * cpx), u2f(min_cy * cpy), 0.0f);
+    F3 bmax = f3(wmin(u2f((max_cx + 1u) * cpx), sw) - 1e-3f, wmin(u2f((max_cy + 1u) * cpy), sh) - 1e-3f, 1.0f);
+    F3 c0, c1;
+    if (!clip_segment(w.p0, w.p1, bmin, bmax, c0, c1)) return;
+    float x0 = c0.x / u2f(cpx), y0 = c0.y / u2f(cpy), x1 = c1.x / u2f(cpx), y1 = c1.y / u2f(cpy);
+    int32_t fx = iclamp(f2i(floorf(x0)), (int32_t)min_cx, (int32_t)max_cx);
+    int32_t fy = iclamp(f2i(floorf(y0)), (int32_t)min_cy, (int32_t)max_cy);
+    int32_t ex = iclamp(f2i(floorf(x1)), (int32_t)min_cx, (int32_t)max_cx);
+    int32_t ey = iclamp(f2i(floorf(y1)), (int32_t)min_cy, (int32_t)max_cy);
+    float dx = x1 - x0, dy = y1 - y0;
+    int32_t sx = sgn_i32(dx), sy = sgn_i32(dy);
+    float sdx = fabsf(dx) < 1e-6f ? 1e-6f : dx, sdy = fabsf(dy) < 1e-6f ? 1e-6f : dy;
+    float ddx = fabsf(1.0f / sdx), ddy = fabsf(1.0f / sdy);
+    float flx = floorf(x0), fly = floorf(y0);
+    float tx = sx > 0 ? ((flx + 1.0f) - x0) / sdx : (flx - x0) / sdx;
+    float ty = sy > 0 ? ((fly + 1.0f) - y0) / sdy : (fly - y0) / sdy;
+    if (fabsf(dx) < 1e-6f) tx = 1e38f;
+    if (fabsf(dy) < 1e-6f) ty = 1e38f;
+    uint32_t safety = 0, max_steps = (max_cx - min_cx + 1u) + (max_cy - min_cy + 1u) + 2u;
+    for (;;) {
+        if (safety > max_steps) break;
+        if (fx < (int32_t)min_cx || fx > (int32_t)max_cx || fy < (int32_t)min_cy || fy > (int32_t)max_cy) break;
+        uint32_t local = (uint32_t)fy * d.coarse_tiles_x + (uint32_t)fx;
+        if (local < d.coarse_depth_tile_count)
+            walk_page(A, w.p0, w.p1, d, d.coarse_depth_tile_base + local, local, sink);
+        if (fx == ex && fy == ey) break;
+        if (tx <= ty) { fx += sx; tx += ddx; } else { fy += sy; ty += ddy; }
+        ++safety;
+    }
+}
+
+__device__ __forceinline__ bool visits_unused(const PrepassArgs& A) {
+    return *((volatile uint32_t*)&A.counters->visit_overflow) != 0u;
+}
+
+// K7: page marks + visit records. Blocks walk 256 tasks at a time; each task's
+// first kVisitSlots visits go to shared memory, the block reserves room for all
+// its visits with one atomic, and a task with more visits walks again to write
+// the rest. When the records do not fit (or slots exceed 24 bits) the pass
+// still marks every page and raises visit_overflow, which hands count and fill
+// to the walking kernels.
+__global__ void __launch_bounds__(kVisitThreads) k_visit(const FrameParams* __restrict__ Pp, PrepassArgs A) {
+    const FrameParams& P = *Pp;
+    __shared__ uint32_t s_buf[kVisitSlots * kVisitThreads];
+    __shared__ uint32_t s_warp[33];
+    __shared__ uint32_t s_base;
+    const uint32_t n = *((volatile uint32_t*)&A.counters->tasks);
+    const uint32_t n_cap = min(n, P.task_capacity);
+    const bool records = P.visit_records != 0u;
+    if (!records && blockIdx.x == 0 && threadIdx.x == 0) atomicOr(&A.counters->visit_overflow, 1u);
+    for (uint32_t k0 = blockIdx.x * kVisitThreads; k0 < n_cap; k0 += gridDim.x * kVisitThreads) {
+        const uint32_t k = k0 + threadIdx.x;
+        TaskWalk w;
+        const bool ok = k < n_cap && task_walk(P, A, k, w);
+        VisitSink vs{A.page_table, s_buf + threadIdx.x, 0u, 0u, records};
+        if (ok) walk_task(P, A, w, vs);
+        if (!records) continue;
+        uint32_t total;
+        const uint32_t excl = block_exclusive_scan<kVisitThreads>(vs.n, s_warp, total);
+        if (threadIdx.x == 0) {
+            uint32_t base = kInvalid;
+            if (total > 0u && !visits_unused(A)) {
+                const unsigned long long b = atomicAdd(&A.counters->visits, (unsigned long long)total);
+                if (b + total <= (unsigned long long)P.ref_capacity) base = (uint32_t)b;
+                else atomicOr(&A.counters->visit_overflow, 1u);
+            }
+            s_base = base;
+        }
+        __syncthreads();
+        const uint32_t base = s_base;
+        if (base != kInvalid && vs.n > 0u) {
+            const uint32_t at = base + excl;
+            const uint32_t nb = min(vs.n, kVisitSlots);
+            for (uint32_t j = 0; j < nb; ++j) {
+                A.visit_rec[at + j] = s_buf[j * kVisitThreads + threadIdx.x];
+                A.visit_task[at + j] = k;
+            }
+            if (vs.n > kVisitSlots) {
+                SpillSink sp{A.visit_rec, A.visit_task, at, k, vs.n, 0u, 0u};
+                walk_task(P, A, w, sp);
+            }
+        }
+        __syncthreads();  // s_buf and s_base are rewritten by the next round
+    }
+}
+
+// K9 over visit records: cell counts by atomics; each visit keeps its rank.
+__global__ void __launch_bounds__(256) k_count_visits(PrepassArgs A) {
+    if (visits_unused(A)) return;
+    const uint32_t n = (uint32_t)*((volatile unsigned long long*)&A.counters->visits);
+    for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+        const uint32_t rec = A.visit_rec[r];
+        const uint32_t h = A.page_table[rec >> 8];
+        uint32_t g = kInvalid, rank = 0u;
+        if (h != 0u && h != kMarked) {
+            g = (h - 1u) * kPageSize + (rec & 0xFFu);
+            rank = atomicAdd(A.counts + g, 1u);
+        }
+        A.visit_rec[r] = g;
+        A.visit_rank[r] = rank;
+    }
+}
+
+// K11 over visit records: make_fine_seg_ref (:1313-1327) at page base + cell
+// offset + rank.
+__global__ void __launch_bounds__(256) k_fill_visits(const InstanceView* __restrict__ inst, PrepassArgs A) {
+    if (visits_unused(A)) return;
+    const uint32_t n = (uint32_t)*((volatile unsigned long long*)&A.counters->visits);
+    for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+        const uint32_t g = A.visit_rec[r];
+        if (g == kInvalid) continue;
+        const fiber_fine_page_meta pm = A.page_meta[g / kPageSize];
+        if (pm.seg_ref_count == 0u) continue;
+        const uint64_t dst = (uint64_t)pm.seg_ref_base + A.offsets[g] + A.visit_rank[r];
+        if (dst >= (uint64_t)pm.seg_ref_base + pm.seg_ref_count) continue;
+        const uint32_t k = A.visit_task[r];
+        const uint4 t = reinterpret_cast<const uint4*>(A.tasks)[k];
+        const uint32_t depths = A.projected[k].depths;
+        const InstanceView& in = inst[t.x];
+        const uint32_t mat = t.y < in.n_meta ? in.meta[t.y].material_idx : 0u;
+        A.refs[dst] = fiber_fine_seg_ref{t.x, t.z, mat};
+        A.ref_keys[dst] = (depths & 0xFFFFu) + (depths >> 16u);
+    }
+}
+
+// K9 / K11 walking form, for frames whose visit records did not fit.
 template <int PASS>
 __global__ void __launch_bounds__(256) k_traverse(const FrameParams* __restrict__ Pp,
                                                   const InstanceView* __restrict__ inst, PrepassArgs A) {
+    if (!visits_unused(A)) return;
     const FrameParams& P = *Pp;
     const uint32_t n = *((volatile uint32_t*)&A.counters->tasks);
     const uint32_t n_cap = min(n, P.task_capacity);
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n_cap; k += gridDim.x * blockDim.x) {
-        uint4 t = reinterpret_cast<const uint4*>(A.tasks)[k];
-        uint32_t f = t.w >> 3u;
-        if (f >= P.F) continue;
-        uint32_t i = t.x;
-        if (i >= P.I) continue;
-        const fiber_frustum_desc& d = P.frusta[f];
-        fiber_projected_segment pr = A.projected[k];
-        float sw = u2f(d.screen_width), sh = u2f(d.screen_height);
-        float2 a = unpack2x16unorm(pr.p0_xy), b = unpack2x16unorm(pr.p1_xy), z = unpack2x16unorm(pr.depths);
-        F3 p0 = f3(a.x * sw, a.y * sh, z.x), p1 = f3(b.x * sw, b.y * sh, z.y);
-        uint32_t slot = i * P.F + f;
-        if (!A.range_valid[slot]) continue;
-        fiber_coarse_asset_range r = A.ranges[slot];
-        uint32_t ref_mat = 0, key = 0;
-        if (PASS == kFill) {
+        TaskWalk w;
+        if (!task_walk(P, A, k, w)) continue;
+        if (PASS == kCount) {
+            CountSink cs{A.page_table, A.counts, 0u};
+            walk_task(P, A, w, cs);
+        } else {
             // make_fine_seg_ref (:1313-1327)
-            const InstanceView& in = inst[i];
-            if (t.y < in.n_meta) ref_mat = in.meta[t.y].material_idx;
-            key = (pr.depths & 0xFFFFu) + (pr.depths >> 16u);
-        }
-        uint32_t cpx = max(1u, d.froxel_size_x * kCoarseExtent);
-        uint32_t cpy = max(1u, d.froxel_size_y * kCoarseExtent);
-        uint32_t min_cx = max(r.min_x, min(f2u(wmax(wmin(p0.x, p1.x), 0.0f)) / cpx, d.coarse_tiles_x - 1u));
-        uint32_t max_cx = min(r.max_x, min(f2u(wmax(wmax(p0.x, p1.x), 0.0f)) / cpx, d.coarse_tiles_x - 1u));
-        uint32_t min_cy = max(r.min_y, min(f2u(wmax(wmin(p0.y, p1.y), 0.0f)) / cpy, d.coarse_tiles_y - 1u));
-        uint32_t max_cy = min(r.max_y, min(f2u(wmax(wmax(p0.y, p1.y), 0.0f)) / cpy, d.coarse_tiles_y - 1u));
-        if (max_cx < min_cx || max_cy < min_cy) continue;
-        F3 bmin = f3(u2f(min_cx * cpx), u2f(min_cy * cpy), 0.0f);
-        F3 bmax = f3(wmin(u2f((max_cx + 1u) * cpx), sw) - 1e-3f, wmin(u2f((max_cy + 1u) * cpy), sh) - 1e-3f, 1.0f);
-        F3 c0, c1;
-        if (!clip_segment(p0, p1, bmin, bmax, c0, c1)) continue;
-        float x0 = c0.x / u2f(cpx), y0 = c0.y / u2f(cpy), x1 = c1.x / u2f(cpx), y1 = c1.y / u2f(cpy);
-        int32_t fx = iclamp(f2i(floorf(x0)), (int32_t)min_cx, (int32_t)max_cx);
-        int32_t fy = iclamp(f2i(floorf(y0)), (int32_t)min_cy, (int32_t)max_cy);
-        int32_t ex = iclamp(f2i(floorf(x1)), (int32_t)min_cx, (int32_t)max_cx);
-        int32_t ey = iclamp(f2i(floorf(y1)), (int32_t)min_cy, (int32_t)max_cy);
-        float dx = x1 - x0, dy = y1 - y0;
-        int32_t sx = sgn_i32(dx), sy = sgn_i32(dy);
-        float sdx = fabsf(dx) < 1e-6f ? 1e-6f : dx, sdy = fabsf(dy) < 1e-6f ? 1e-6f : dy;
-        float ddx = fabsf(1.0f / sdx), ddy = fabsf(1.0f / sdy);
-        float flx = floorf(x0), fly = floorf(y0);
-        float tx = sx > 0 ? ((flx + 1.0f) - x0) / sdx : (flx - x0) / sdx;
-        float ty = sy > 0 ? ((fly + 1.0f) - y0) / sdy : (fly - y0) / sdy;
-        if (fabsf(dx) < 1e-6f) tx = 1e38f;
-        if (fabsf(dy) < 1e-6f) ty = 1e38f;
-        uint32_t safety = 0, max_steps = (max_cx - min_cx + 1u) + (max_cy - min_cy + 1u) + 2u;
-        for (;;) {
-            if (safety > max_steps) break;
-            if (fx < (int32_t)min_cx || fx > (int32_t)max_cx || fy < (int32_t)min_cy || fy > (int32_t)max_cy) break;
-            uint32_t local = (uint32_t)fy * d.coarse_tiles_x + (uint32_t)fx;
-            if (local < d.coarse_depth_tile_count)
-                trace_page<PASS>(P, A, p0, p1, d, d.coarse_depth_tile_base + local, local, i, t.z, ref_mat, key);
-            if (fx == ex && fy == ey) break;
-            if (tx <= ty) { fx += sx; tx += ddx; } else { fy += sy; ty += ddy; }
-            ++safety;
+            const InstanceView& in = inst[w.i];
+            const uint32_t mat = w.strand < in.n_meta ? in.meta[w.strand].material_idx : 0u;
+            FillSink fs{&A, 0u, 0u, 0u, w.i, w.seg, mat, (w.depths & 0xFFFFu) + (w.depths >> 16u)};
+            walk_task(P, A, w, fs);
         }
     }
 }
@@ -949,8 +1138,8 @@ void launch_lut(const LaunchCtx& L, const PrepassArgs& A) {
 void launch_fine(const LaunchCtx& L, const PrepassArgs& A) {
     k_fine<<<L.sm_count * 6, kFineThreads, 0, L.stream>>>(L.P, L.inst, A);
 }
-void launch_mark(const LaunchCtx& L, const PrepassArgs& A) {
-    k_traverse<kMark><<<L.sm_count * 8, 256, 0, L.stream>>>(L.P, L.inst, A);
+void launch_visit(const LaunchCtx& L, const PrepassArgs& A) {
+    k_visit<<<L.sm_count * 8, kVisitThreads, 0, L.stream>>>(L.P, A);
 }
 void launch_alloc(const LaunchCtx& L, const PrepassArgs& A) {
     k_alloc_pages<<<L.sm_count * 4, kScanThreads, 0, L.stream>>>(L.P, A);
@@ -959,12 +1148,14 @@ void launch_zero_pages(const LaunchCtx& L, const PrepassArgs& A) {
     k_zero_pages<<<L.sm_count * 4, 256, 0, L.stream>>>(A);
 }
 void launch_count(const LaunchCtx& L, const PrepassArgs& A) {
+    k_count_visits<<<L.sm_count * 8, 256, 0, L.stream>>>(A);
     k_traverse<kCount><<<L.sm_count * 8, 256, 0, L.stream>>>(L.P, L.inst, A);
 }
 void launch_prefix(const LaunchCtx& L, const PrepassArgs& A) {
     k_prefix_pages<<<L.sm_count * 6, 256, 0, L.stream>>>(L.P, A);
 }
 void launch_fill(const LaunchCtx& L, const PrepassArgs& A) {
+    k_fill_visits<<<L.sm_count * 8, 256, 0, L.stream>>>(L.inst, A);
     k_traverse<kFill><<<L.sm_count * 8, 256, 0, L.stream>>>(L.P, L.inst, A);
 }
 void launch_compact_active(const LaunchCtx& L, const PrepassArgs& A) {
