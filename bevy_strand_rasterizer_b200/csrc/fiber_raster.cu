@@ -74,10 +74,61 @@ __device__ __forceinline__ void slot_source(const uint32_t* s_prefix, const Roun
 // K16 deep-opacity shadow raster + K17 stampback.
 // ===========================================================================
 constexpr uint32_t kShadowCap = 1024;
+constexpr uint32_t kShadowWords = kShadowCap / 32;
 constexpr int kMaxDomSlices = 16;
 
 size_t shadow_smem_bytes(uint32_t K) {
-    return (size_t)kShadowCap * (9 * sizeof(float) + sizeof(uint32_t)) + (size_t)256 * K * sizeof(float);
+    return (size_t)kShadowCap * 9 * sizeof(float) + (size_t)256 * K * sizeof(float);
+}
+
+// Coverage candidates. The exact test below covers pixel p (cov > 0) only if
+// p lies within the radius bound rb = rmin + (rmax - rmin) clamp(max z) of the
+// segment's line and between the normals through its end points (t in [0, 1]).
+// The band is widened by 1e-4 rb + 1e-6 rmax + 0.01 px + 1e-5 of the largest
+// coordinate magnitude, hundreds of float ulps beyond the rounding of the
+// exact test and of this one, so every pixel the band rejects is one the exact
+// test leaves uncovered. Comparisons are written so that NaN never rejects;
+// segments shorter than 1e-6 px are tested as a disc around the first point.
+struct Band {
+    float nx, ny, c;    // d = n . p - c
+    float ux, uy, cu;   // s = u . p - cu
+    float thr, slo, shi;
+    float ax, ay;
+    bool disc;
+};
+
+__device__ __forceinline__ Band make_band(float ax, float ay, float bx, float by, float z0, float z1, float rmin,
+                                          float rmax, float tile_max) {
+    Band B;
+    const float X = fmaxf(fmaxf(fmaxf(fabsf(ax), fabsf(ay)), fmaxf(fabsf(bx), fabsf(by))), tile_max);
+    const float rb = rmin + (rmax - rmin) * wclamp(fmaxf(z0, z1), 0.0f, 1.0f);
+    const float slack = 0.01f + 1e-5f * X;
+    B.thr = rb * 1.0001f + 1e-6f * rmax + slack;
+    const float abx = bx - ax, aby = by - ay;
+    const float l2 = abx * abx + aby * aby;
+    B.disc = !(l2 > 1e-12f);
+    const float len = sqrtf(l2);
+    B.ux = abx / len;
+    B.uy = aby / len;
+    B.nx = -B.uy;
+    B.ny = B.ux;
+    B.c = __fmaf_rn(B.nx, ax, B.ny * ay);
+    B.cu = __fmaf_rn(B.ux, ax, B.uy * ay);
+    B.slo = -slack;
+    B.shi = len + slack;
+    B.ax = ax;
+    B.ay = ay;
+    return B;
+}
+
+__device__ __forceinline__ bool band_candidate(const Band& B, float px, float py) {
+    if (B.disc) {
+        const float dx = px - B.ax, dy = py - B.ay;
+        return !(dx * dx + dy * dy > B.thr * B.thr);
+    }
+    const float d = __fmaf_rn(B.nx, px, __fmaf_rn(B.ny, py, -B.c));
+    const float s = __fmaf_rn(B.ux, px, __fmaf_rn(B.uy, py, -B.cu));
+    return !(fabsf(d) > B.thr) && !(s < B.slo) && !(s > B.shi);
 }
 
 __global__ void __launch_bounds__(256) k_shadow(const FrameParams* __restrict__ Pp,
@@ -93,9 +144,12 @@ __global__ void __launch_bounds__(256) k_shadow(const FrameParams* __restrict__ 
     float* srmin = sp1z + kShadowCap;
     float* srmax = srmin + kShadowCap;
     float* sabs = srmax + kShadowCap;
-    uint32_t* svalid = reinterpret_cast<uint32_t*>(sabs + kShadowCap);
-    float* s_partial = reinterpret_cast<float*>(svalid + kShadowCap);
+    float* s_partial = sabs + kShadowCap;
     __shared__ uint32_t s_wbase[kMaxRunItems], s_wcount[kMaxRunItems], s_prefix[kMaxRunItems + 1];
+    __shared__ uint32_t s_pmask[kShadowWords * kPixelSlots];  // [word][pixel] candidate bits
+    __shared__ uint32_t s_wmask[4 * kShadowWords];            // [worker][word] entries of worker w
+    __shared__ uint16_t s_item[kShadowCap];                   // run item of each staged entry
+    __shared__ float2 s_pix[kPixelSlots];
     __shared__ RoundPlan s_plan;
     __shared__ uint32_t s_more;
 
@@ -103,6 +157,7 @@ __global__ void __launch_bounds__(256) k_shadow(const FrameParams* __restrict__ 
     const uint32_t last = *((volatile uint32_t*)&R.counters->active_tiles);
     const uint32_t K = P.K, D = P.dom_size, S = P.shadow_map_size;
     const uint32_t slot = threadIdx.x >> 2, worker = threadIdx.x & 3u;
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     float* partial = s_partial + threadIdx.x * K;
 
     for (uint32_t r = first + blockIdx.x; r < last; r += gridDim.x) {
@@ -120,14 +175,19 @@ __global__ void __launch_bounds__(256) k_shadow(const FrameParams* __restrict__ 
         const uint32_t py = ty * d.froxel_size_y + slot / d.froxel_size_x;
         const bool active = slot < d.froxel_size_x * d.froxel_size_y && px < d.screen_width && py < d.screen_height;
         const float pfx = u2f(px) + 0.5f, pfy = u2f(py) + 0.5f;
+        const float tile_max = fmaxf(u2f((tx + 1u) * d.froxel_size_x), u2f((ty + 1u) * d.froxel_size_y)) + 1.0f;
         for (uint32_t i = threadIdx.x; i < n_items; i += blockDim.x) {
             const fiber_raster_work_item wi = R.work[run.work_base + i];
             const bool valid_item = wi.frustum_id == f && wi.screen_tile_id == run.screen_tile_id;
             s_wbase[i] = wi.seg_ref_base;
             s_wcount[i] = valid_item ? wi.seg_ref_count : 0u;
         }
+        if (worker == 0u) s_pix[slot] = make_float2(pfx, pfy);
         __syncthreads();
 
+        // Stage a round (projection, radii, run item, worker of each entry:
+        // worker w takes entries w, w+4, ... from each item's start), then build
+        // the candidate bits: warp per 32-entry word, one ballot per pixel.
         auto stage = [&](const RoundPlan& rp) {
             for (uint32_t s = threadIdx.x; s < rp.n; s += blockDim.x) {
                 uint32_t item, j;
@@ -144,13 +204,55 @@ __global__ void __launch_bounds__(256) k_shadow(const FrameParams* __restrict__ 
                 srmin[s] = rmin;
                 srmax[s] = wmax(m.max_radius_pixels, rmin);
                 sabs[s] = m.absorption_color[3];
-                svalid[s] = 1u;
+                s_item[s] = (uint16_t)((item << 2) | (j & 3u));
+            }
+            __syncthreads();
+            const uint32_t nq = (rp.n + 31u) >> 5;
+            for (uint32_t q = warp; q < nq; q += blockDim.x >> 5) {
+                const uint32_t s = q * 32u + lane;
+                const bool v = s < rp.n;
+                const uint32_t e = v ? s : 0u;
+                const Band B = make_band(sp0x[e], sp0y[e], sp1x[e], sp1y[e], sp0z[e], sp1z[e], srmin[e], srmax[e],
+                                         tile_max);
+                uint32_t lo = 0u, hi = 0u;
+#pragma unroll 8
+                for (uint32_t p = 0; p < kPixelSlots; ++p) {
+                    const float2 pp = s_pix[p];
+                    const unsigned bal = __ballot_sync(0xFFFFFFFFu, v && band_candidate(B, pp.x, pp.y));
+                    if (p == lane) lo = bal;
+                    if (p == lane + 32u) hi = bal;
+                }
+                s_pmask[q * kPixelSlots + lane] = lo;
+                s_pmask[q * kPixelSlots + lane + 32u] = hi;
+                const uint32_t wk = v ? (s_item[s] & 3u) : 4u;
+#pragma unroll
+                for (uint32_t w = 0; w < 4u; ++w) {
+                    const unsigned bal = __ballot_sync(0xFFFFFFFFu, wk == w);
+                    if (lane == w) s_wmask[w * kShadowWords + q] = bal;
+                }
             }
         };
 
-        // ---- Pass 1: nearest covered depth, item by item until the first item with a hit.
-        float z0 = -1.0f, zi = -1.0f;
-        bool found = false, hit = false;
+        // This lane's candidates (pixel slot, worker) in entry order.
+        auto next_candidate = [&](uint32_t nq, uint32_t& q, uint32_t& m) -> uint32_t {
+            while (m == 0u && q < nq) {
+                m = s_pmask[q * kPixelSlots + slot] & s_wmask[worker * kShadowWords + q];
+                ++q;
+            }
+            if (m == 0u) return kInvalid;
+            const uint32_t bit = (uint32_t)(__ffs(m) - 1);
+            m &= m - 1u;
+            return (q - 1u) * 32u + bit;
+        };
+
+        // ---- Pass 1: nearest covered depth = max depth of the covered entries
+        // of the first run item holding one. The max does not depend on order,
+        // so the pixel's 4 lanes split its candidates by worker; a lane stops
+        // once its next candidate lies past the pixel's best item so far.
+        uint32_t best = kInvalid;      // this lane's first item with a covered entry
+        float zb = -1.0f;              // its max covered depth in that item
+        uint32_t pix_best = kInvalid;  // min of best over the pixel's 4 lanes
+        bool complete = !active;       // the pixel's best item is fully processed
         uint32_t cur_item = 0u, cur_off = 0u;
         bool single_round = false, staged_all = false;
         for (bool first_round = true;; first_round = false) {
@@ -167,32 +269,41 @@ __global__ void __launch_bounds__(256) k_shadow(const FrameParams* __restrict__ 
             stage(rp);
             __syncthreads();
             staged_all = single_round;
-            for (uint32_t k = rp.lo; k < rp.hi; ++k) {
-                const uint32_t a = s_prefix[k - rp.lo], b = s_prefix[k - rp.lo + 1u];
-                if (!__all_sync(0xFFFFFFFFu, found || !active) && active && !found) {
-                    for (uint32_t bi = a + worker; bi < b; bi += 4u) {
+            const uint32_t nq = (rp.n + 31u) >> 5;
+            uint32_t q = 0u, m = 0u;
+            bool done = complete;
+            while (!__all_sync(0xFFFFFFFFu, done)) {
+                if (!done) {
+                    const uint32_t bi = next_candidate(nq, q, m);
+                    const uint32_t item = bi != kInvalid ? (uint32_t)(s_item[bi] >> 2) : kInvalid;
+                    if (bi == kInvalid || item > pix_best) {
+                        done = true;
+                    } else {
                         float t = line_t(pfx, pfy, sp0x[bi], sp0y[bi], sp1x[bi], sp1y[bi]);
-                        if (t < 0.0f || t > 1.0f) continue;
-                        float qx = wmix(sp0x[bi], sp1x[bi], t), qy = wmix(sp0y[bi], sp1y[bi], t);
-                        float qz = wmix(sp0z[bi], sp1z[bi], t);
-                        float rr = wmix(srmin[bi], srmax[bi], wclamp(qz, 0.0f, 1.0f));
-                        float dx = pfx - qx, dy = pfy - qy;
-                        float cov = wclamp(1.0f - sqrtf(dx * dx + dy * dy) / rr, 0.0f, 1.0f);
-                        if (cov > 0.0f) { zi = wmax(zi, qz); hit = true; }
+                        if (!(t < 0.0f || t > 1.0f)) {
+                            float qx = wmix(sp0x[bi], sp1x[bi], t), qy = wmix(sp0y[bi], sp1y[bi], t);
+                            float qz = wmix(sp0z[bi], sp1z[bi], t);
+                            float rr = wmix(srmin[bi], srmax[bi], wclamp(qz, 0.0f, 1.0f));
+                            float dx = pfx - qx, dy = pfy - qy;
+                            float cov = wclamp(1.0f - sqrtf(dx * dx + dy * dy) / rr, 0.0f, 1.0f);
+                            if (cov > 0.0f) {
+                                if (best == kInvalid) { best = item; zb = wmax(-1.0f, qz); }
+                                else if (item == best) zb = wmax(zb, qz);
+                            }
+                        }
                     }
                 }
-                if (k + 1u < rp.hi || rp.completes) {
-                    float zm = wmax(zi, __shfl_xor_sync(0xFFFFFFFFu, zi, 1));
-                    zm = wmax(zm, __shfl_xor_sync(0xFFFFFFFFu, zm, 2));
-                    unsigned hm = __ballot_sync(0xFFFFFFFFu, hit);
-                    bool any_hit = ((hm >> (threadIdx.x & 28u)) & 0xFu) != 0u;
-                    if (active && !found && any_hit) { z0 = zm; found = true; }
-                    zi = -1.0f;
-                    hit = false;
-                }
+                uint32_t pb = min(best, __shfl_xor_sync(0xFFFFFFFFu, best, 1));
+                pix_best = min(pb, __shfl_xor_sync(0xFFFFFFFFu, pb, 2));
             }
-            if (__syncthreads_and(found || !active)) break;
+            complete = !active || (pix_best != kInvalid && (pix_best + 1u < rp.hi || rp.completes));
+            if (__syncthreads_and(complete)) break;
         }
+        float zc = best == pix_best ? zb : -1.0f;
+        zc = wmax(zc, __shfl_xor_sync(0xFFFFFFFFu, zc, 1));
+        zc = wmax(zc, __shfl_xor_sync(0xFFFFFFFFu, zc, 2));
+        const bool found = active && pix_best != kInvalid;
+        const float z0 = zc;
 
         // ---- Pass 2: opacity partials; worker w takes entries w, w+4, ... of each item.
         for (uint32_t i = 0; i < K; ++i) partial[i] = 0.0f;
@@ -214,9 +325,10 @@ __global__ void __launch_bounds__(256) k_shadow(const FrameParams* __restrict__ 
                     __syncthreads();
                 }
                 const RoundPlan rp = s_plan;
-                for (uint32_t k = rp.lo; k < rp.hi && alpha_active; ++k) {
-                    const uint32_t a = s_prefix[k - rp.lo], b = s_prefix[k - rp.lo + 1u];
-                    for (uint32_t bi = a + worker; bi < b; bi += 4u) {
+                if (alpha_active) {
+                    const uint32_t nq = (rp.n + 31u) >> 5;
+                    uint32_t q = 0u, m = 0u;
+                    for (uint32_t bi; (bi = next_candidate(nq, q, m)) != kInvalid;) {
                         float t = line_t(pfx, pfy, sp0x[bi], sp0y[bi], sp1x[bi], sp1y[bi]);
                         if (t < 0.0f || t > 1.0f) continue;
                         float qx = wmix(sp0x[bi], sp1x[bi], t), qy = wmix(sp0y[bi], sp1y[bi], t);
