@@ -398,24 +398,33 @@ __global__ void __launch_bounds__(256) k_shadow(const FrameParams* __restrict__ 
 // K19 camera colour raster.
 // ===========================================================================
 constexpr uint32_t kCamCap = 512;
+constexpr uint32_t kCamWords = kCamCap / 32;
+constexpr uint16_t kEntryInvalid = 0x8000u;
 
+// One pixel's walk over the groups of 4 (an item's entries 4g .. 4g+3 from
+// the item start) that hold a candidate: the pixel's 4 lanes run it
+// redundantly, so they stay in step for the group blend. A group without a
+// candidate contributes transparent black and depth 0 in every lane, which
+// leaves the blend unchanged, so skipping it keeps the result.
 __global__ void __launch_bounds__(256) k_raster(const FrameParams* __restrict__ Pp,
                                                 const InstanceView* __restrict__ inst, RenderArgs R) {
     const FrameParams& P = *Pp;
-    // Per staged reference (80 B). An invalid slot (segment behind the camera)
-    // gets an empty bounding box (mnx = +inf), which rejects every pixel
-    // exactly like the reference's valid flag.
-    __shared__ float sp0x[kCamCap], sp0y[kCamCap], sabx[kCamCap], saby[kCamCap], sinv[kCamCap];
+    // Per staged entry: 64 B of projection, radii and shading texels, the run
+    // item and position in it (bit 15: behind the camera, never a candidate).
+    __shared__ float sp0x[kCamCap], sp0y[kCamCap], sp1x[kCamCap], sp1y[kCamCap], sinv[kCamCap];
     __shared__ float sz0[kCamCap], sz1[kCamCap], sw0[kCamCap], sw1[kCamCap], srmin[kCamCap], srmax[kCamCap];
-    __shared__ float smnx[kCamCap], smny[kCamCap], smxx[kCamCap], smxy[kCamCap], svis[kCamCap];
+    __shared__ float svis[kCamCap];
     __shared__ uint2 ss0[kCamCap], ss1[kCamCap];
+    __shared__ uint16_t s_item[kCamCap];
+    __shared__ uint32_t s_pmask[kCamWords * kPixelSlots];  // [word][pixel] candidate bits
+    __shared__ float2 s_pix[kPixelSlots];
     __shared__ uint32_t s_wbase[kMaxRunItems], s_wcount[kMaxRunItems], s_prefix[kMaxRunItems + 1];
     __shared__ RoundPlan s_plan;
     __shared__ uint32_t s_more;
 
     const uint32_t n_runs = *((volatile uint32_t*)&R.counters->camera_active);
     const uint32_t slot = threadIdx.x >> 2, worker = threadIdx.x & 3u;
-    const uint32_t lane = threadIdx.x & 31u, wbase = lane & ~3u;
+    const uint32_t lane = threadIdx.x & 31u, wbase = lane & ~3u, warp = threadIdx.x >> 5;
     const uint32_t cap = P.atlas_cap;
     const __half* hist = R.history[(P.hist_in & 1u) ^ 1u];
     for (uint32_t r = blockIdx.x; r < n_runs; r += gridDim.x) {
@@ -432,17 +441,29 @@ __global__ void __launch_bounds__(256) k_raster(const FrameParams* __restrict__ 
         const uint32_t py = ty * d.froxel_size_y + slot / d.froxel_size_x;
         const bool active = slot < d.froxel_size_x * d.froxel_size_y && px < d.screen_width && py < d.screen_height;
         const float pcx = u2f(px) + 0.5f, pcy = u2f(py) + 0.5f;
+        const float tile_max = fmaxf(u2f((tx + 1u) * d.froxel_size_x), u2f((ty + 1u) * d.froxel_size_y)) + 1.0f;
         for (uint32_t i = threadIdx.x; i < n_items; i += blockDim.x) {
             const fiber_raster_work_item wi = R.work[run.work_base + i];
             s_wbase[i] = wi.seg_ref_base;
             s_wcount[i] = wi.seg_ref_count;
         }
+        if (worker == 0u) s_pix[slot] = make_float2(pcx, pcy);
         __syncthreads();
         float4 fin = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         float gdepth = 0.0f;
         bool done = !active;
         uint32_t frags = 0;
+        uint32_t pending = kInvalid;  // last item blended into, whose end test is still due
         uint32_t cur_item = 0u, cur_off = 0u;
+        // Early out (alpha > 0.98) at the end of an item; worker 0 holds the blend.
+        auto end_of_item = [&](bool due) {
+            if (due && worker == 0u && !done && fin.w > 0.98f) {
+                fin = make_float4(fin.x / fin.w, fin.y / fin.w, fin.z / fin.w, 1.0f);
+                done = true;
+            }
+            done = __shfl_sync(0xFFFFFFFFu, done, wbase);
+            if (due) pending = kInvalid;
+        };
         for (;;) {
             if (threadIdx.x == 0) {
                 s_more = cur_item < n_items ? 1u : 0u;
@@ -459,6 +480,7 @@ __global__ void __launch_bounds__(256) k_raster(const FrameParams* __restrict__ 
                 float4 w0, w1;
                 segment_world(in, ref.seg_id, w0, w1);
                 float4 a = world_to_screen_raw(w0, clip, vw, vh), b = world_to_screen_raw(w1, clip, vw, vh);
+                uint16_t tag = (uint16_t)((item << 2) | (j & 3u));
                 if (!(a.x < 0.0f && b.x < 0.0f)) {
                     const fiber_strand_material& m = in.materials[ref.material_idx];
                     float rmin = wmax(m.min_radius_pixels, 1e-4f);
@@ -466,36 +488,77 @@ __global__ void __launch_bounds__(256) k_raster(const FrameParams* __restrict__ 
                     uint32_t i0 = ref.seg_id, i1 = min(i0 + 1u, cap - 1u);
                     size_t t0 = (size_t)ref.inst_id * cap + i0, t1 = (size_t)ref.inst_id * cap + i1;
                     float abx = b.x - a.x, aby = b.y - a.y;
-                    sp0x[s] = a.x; sp0y[s] = a.y; sabx[s] = abx; saby[s] = aby;
+                    sp0x[s] = a.x; sp0y[s] = a.y; sp1x[s] = b.x; sp1y[s] = b.y;
                     sinv[s] = 1.0f / (abx * abx + aby * aby);
                     sz0[s] = a.z; sz1[s] = b.z; sw0[s] = a.w; sw1[s] = b.w;
                     // min_radius = max(rmin, 1e-4) and max(rmax, min_radius) are
                     // idempotent on these values, so they are applied once here.
                     srmin[s] = rmin; srmax[s] = rmax;
-                    smnx[s] = wmin(a.x, b.x) - rmax; smny[s] = wmin(a.y, b.y) - rmax;
-                    smxx[s] = wmax(a.x, b.x) + rmax; smxy[s] = wmax(a.y, b.y) + rmax;
                     ss0[s] = *reinterpret_cast<const uint2*>(R.atlas + t0 * 4);
                     ss1[s] = *reinterpret_cast<const uint2*>(R.atlas + t1 * 4);
                     svis[s] = __half2float(hist[t0 * 2]);
                 } else {
-                    smnx[s] = __int_as_float(0x7f800000);  // +inf: empty box
-                    smny[s] = 0.0f; smxx[s] = 0.0f; smxy[s] = 0.0f;
+                    tag |= kEntryInvalid;
                 }
+                s_item[s] = tag;
             }
             __syncthreads();
-            for (uint32_t k = rp.lo; k < rp.hi; ++k) {
-                const uint32_t a = s_prefix[k - rp.lo], b = s_prefix[k - rp.lo + 1u];
-                if (!__all_sync(0xFFFFFFFFu, done)) {
-                    for (uint32_t g = a; g < b; g += 4u) {
-                        float4 part = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-                        float pd = 0.0f;
-                        const uint32_t bi = g + worker;
-                        if (!done && bi < b && !(pcx < smnx[bi] || pcy < smny[bi]) && !(pcx > smxx[bi] || pcy > smxy[bi])) {
-                            float t = ((pcx - sp0x[bi]) * sabx[bi] + (pcy - sp0y[bi]) * saby[bi]) * sinv[bi];
+            // Candidate bits: warp per 32-entry word, one ballot per pixel. The
+            // radius bound uses the normalised depth the exact test clamps.
+            const uint32_t nq = (rp.n + 31u) >> 5;
+            for (uint32_t q = warp; q < nq; q += blockDim.x >> 5) {
+                const uint32_t s = q * 32u + lane;
+                const bool v = s < rp.n && !(s_item[s] & kEntryInvalid);
+                const uint32_t e = v ? s : 0u;
+                const Band B = make_band(sp0x[e], sp0y[e], sp1x[e], sp1y[e], normalize_depth01(sz0[e]),
+                                         normalize_depth01(sz1[e]), srmin[e], srmax[e], tile_max);
+                uint32_t lo = 0u, hi = 0u;
+#pragma unroll 8
+                for (uint32_t p = 0; p < kPixelSlots; ++p) {
+                    const float2 pp = s_pix[p];
+                    const unsigned bal = __ballot_sync(0xFFFFFFFFu, v && band_candidate(B, pp.x, pp.y));
+                    if (p == lane) lo = bal;
+                    if (p == lane + 32u) hi = bal;
+                }
+                s_pmask[q * kPixelSlots + lane] = lo;
+                s_pmask[q * kPixelSlots + lane + 32u] = hi;
+            }
+            __syncthreads();
+            uint32_t pos = 0u;         // next entry of this pixel's walk
+            bool exhausted = done;
+            while (!__all_sync(0xFFFFFFFFu, exhausted)) {
+                bool act = !exhausted;
+                uint32_t c = kInvalid;
+                if (act) {
+                    // first candidate entry >= pos
+                    uint32_t q = pos >> 5;
+                    uint32_t m = q < nq ? (s_pmask[q * kPixelSlots + slot] & (0xFFFFFFFFu << (pos & 31u))) : 0u;
+                    while (m == 0u && q + 1u < nq) m = s_pmask[(++q) * kPixelSlots + slot];
+                    if (m != 0u) c = q * 32u + (uint32_t)(__ffs(m) - 1);
+                    else { exhausted = true; act = false; }
+                }
+                const uint32_t item = act ? (uint32_t)((s_item[c] >> 2) & 0x3FFu) : 0u;
+                end_of_item(act && pending != kInvalid && item > pending);
+                if (done) { exhausted = true; act = false; }
+                float4 part = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                float pd = 0.0f;
+                if (act) {
+                    const uint32_t lead = c - (s_item[c] & 3u);
+                    const uint32_t end = min(lead + 4u, s_prefix[item - rp.lo + 1u]);
+                    const uint32_t bi = lead + worker;
+                    pos = end;
+                    pending = item;
+                    if (bi < end && ((s_pmask[(bi >> 5) * kPixelSlots + slot] >> (bi & 31u)) & 1u)) {
+                        const float ax = sp0x[bi], ay = sp0y[bi], bx = sp1x[bi], by = sp1y[bi];
+                        const float rmax = srmax[bi];
+                        if (!(pcx < wmin(ax, bx) - rmax || pcy < wmin(ay, by) - rmax) &&
+                            !(pcx > wmax(ax, bx) + rmax || pcy > wmax(ay, by) + rmax)) {
+                            const float abx = bx - ax, aby = by - ay;
+                            float t = ((pcx - ax) * abx + (pcy - ay) * aby) * sinv[bi];
                             if (t >= 0.0f && t <= 1.0f) {
-                                float fx = sp0x[bi] + sabx[bi] * t, fy = sp0y[bi] + saby[bi] * t;
+                                float fx = ax + abx * t, fy = ay + aby * t;
                                 float pz = wmix(sz0[bi], sz1[bi], t);
-                                float rr = wmix(srmin[bi], srmax[bi], wclamp(normalize_depth01(pz), 0.0f, 1.0f));
+                                float rr = wmix(srmin[bi], rmax, wclamp(normalize_depth01(pz), 0.0f, 1.0f));
                                 float dx = pcx - fx, dy = pcy - fy;
                                 float d2 = dx * dx + dy * dy;
                                 if (d2 < rr * rr) {
@@ -515,40 +578,36 @@ __global__ void __launch_bounds__(256) k_raster(const FrameParams* __restrict__ 
                                 }
                             }
                         }
-                        // (w0 over w1) over (w2 over w3), depth max.
-                        const uint32_t src = wbase + (worker | 1u);
-                        float4 rhs;
-                        rhs.x = __shfl_sync(0xFFFFFFFFu, part.x, src);
-                        rhs.y = __shfl_sync(0xFFFFFFFFu, part.y, src);
-                        rhs.z = __shfl_sync(0xFFFFFFFFu, part.z, src);
-                        rhs.w = __shfl_sync(0xFFFFFFFFu, part.w, src);
-                        float rd = __shfl_sync(0xFFFFFFFFu, pd, src);
-                        float4 pair = part;
-                        float pdd = pd;
-                        if ((worker & 1u) == 0u) {
-                            pair = over(part, rhs);
-                            pdd = wmax(pd, rd);
-                        }
-                        float4 second;
-                        second.x = __shfl_sync(0xFFFFFFFFu, pair.x, wbase + 2u);
-                        second.y = __shfl_sync(0xFFFFFFFFu, pair.y, wbase + 2u);
-                        second.z = __shfl_sync(0xFFFFFFFFu, pair.z, wbase + 2u);
-                        second.w = __shfl_sync(0xFFFFFFFFu, pair.w, wbase + 2u);
-                        float sdp = __shfl_sync(0xFFFFFFFFu, pdd, wbase + 2u);
-                        if (worker == 0u && !done) {
-                            fin = over(fin, over(pair, second));
-                            gdepth = wmax(gdepth, wmax(pdd, sdp));
-                        }
                     }
                 }
-                if (k + 1u < rp.hi || rp.completes) {
-                    if (worker == 0u && !done && fin.w > 0.98f) {
-                        fin = make_float4(fin.x / fin.w, fin.y / fin.w, fin.z / fin.w, 1.0f);
-                        done = true;
-                    }
-                    done = __shfl_sync(0xFFFFFFFFu, done, wbase);
+                // (w0 over w1) over (w2 over w3), depth max.
+                const uint32_t src = wbase + (worker | 1u);
+                float4 rhs;
+                rhs.x = __shfl_sync(0xFFFFFFFFu, part.x, src);
+                rhs.y = __shfl_sync(0xFFFFFFFFu, part.y, src);
+                rhs.z = __shfl_sync(0xFFFFFFFFu, part.z, src);
+                rhs.w = __shfl_sync(0xFFFFFFFFu, part.w, src);
+                float rd = __shfl_sync(0xFFFFFFFFu, pd, src);
+                float4 pair = part;
+                float pdd = pd;
+                if ((worker & 1u) == 0u) {
+                    pair = over(part, rhs);
+                    pdd = wmax(pd, rd);
+                }
+                float4 second;
+                second.x = __shfl_sync(0xFFFFFFFFu, pair.x, wbase + 2u);
+                second.y = __shfl_sync(0xFFFFFFFFu, pair.y, wbase + 2u);
+                second.z = __shfl_sync(0xFFFFFFFFu, pair.z, wbase + 2u);
+                second.w = __shfl_sync(0xFFFFFFFFu, pair.w, wbase + 2u);
+                float sdp = __shfl_sync(0xFFFFFFFFu, pdd, wbase + 2u);
+                if (worker == 0u && act) {
+                    fin = over(fin, over(pair, second));
+                    gdepth = wmax(gdepth, wmax(pdd, sdp));
                 }
             }
+            // The last item blended into ends in this round unless the round
+            // stops inside it.
+            end_of_item(pending != kInvalid && (pending + 1u < rp.hi || rp.completes));
             if (__syncthreads_and(done)) break;
         }
         frags += __shfl_xor_sync(0xFFFFFFFFu, frags, 1);
