@@ -66,7 +66,10 @@ __device__ __forceinline__ float fresnel_reflectance(float eta_i, float eta_t, f
 // Sum of the 21 wrapped Gaussians (k = -10..10). Terms whose exponent is below
 // -110 are exactly zero in binary32 and are skipped without changing the sum;
 // the test is written so that a NaN exponent is not skipped and still poisons
-// the sum, as exp(NaN) does in the reference.
+// the sum, as exp(NaN) does in the reference. Only k with |phi - 2 pi k| below
+// sqrt(110 * 2 var) can pass it, so the loop runs over that window (widened
+// by one k on each side and by 1e-3 relative + 1e-3 absolute), in the same
+// increasing k order; a NaN phi takes the full range.
 __device__ __forceinline__ float gaussian_detector(float beta, float phi_delta) {
     float var = beta * beta;
     if (var < 1e-6f) {
@@ -76,8 +79,17 @@ __device__ __forceinline__ float gaussian_detector(float beta, float phi_delta) 
     }
     float norm = 1.0f / (sqrtf(2.0f * kPi) * beta);
     float two_var = 2.0f * var;
+    int k0 = -10, k1 = 10;
+    if (phi_delta == phi_delta) {
+        const float reach = sqrtf(110.0f * two_var) * 1.001f + 1e-3f;
+        const float inv_two_pi = 1.0f / (2.0f * kPi);
+        const float lo = wclamp(floorf((phi_delta - reach) * inv_two_pi) - 1.0f, -11.0f, 11.0f);
+        const float hi = wclamp(ceilf((phi_delta + reach) * inv_two_pi) + 1.0f, -11.0f, 11.0f);
+        k0 = max(k0, (int)lo);
+        k1 = min(k1, (int)hi);
+    }
     float total = 0.0f;
-    for (int k = -10; k <= 10; ++k) {
+    for (int k = k0; k <= k1; ++k) {
         float angle = phi_delta - 2.0f * kPi * (float)k;
         float e = -angle * angle / two_var;
         if (!(e <= -110.0f)) total = total + expf(e);
@@ -85,7 +97,23 @@ __device__ __forceinline__ float gaussian_detector(float beta, float phi_delta) 
     return norm * total;
 }
 
-__device__ F3 marschner(F3 L, F3 V, F3 U, const fiber_strand_material& m, float occlusion) {
+// Per quadrature point i, terms that depend on the root alone: h (the clamped
+// root), asin(h) and cos(asin(h)). A block fills them once.
+struct QuadTable {
+    float h[10], gi[10], cgi[10];
+};
+
+__device__ __forceinline__ void fill_quad_table(QuadTable& t) {
+    if (threadIdx.x < 10u) {
+        const float h = wclamp(-1.0f + 1e-6f, 1.0f - 1e-6f, c_leg_roots[threadIdx.x]);
+        const float gi = asinf(h);
+        t.h[threadIdx.x] = h;
+        t.gi[threadIdx.x] = gi;
+        t.cgi[threadIdx.x] = cosf(gi);
+    }
+}
+
+__device__ F3 marschner(F3 L, F3 V, F3 U, const fiber_strand_material& m, float occlusion, const QuadTable& qt) {
     float theta_i = acosf(dot3(L, U));
     float theta_r = acosf(dot3(L, V));
     float dUL = dot3(U, L), dVL = dot3(V, L);
@@ -129,30 +157,37 @@ __device__ F3 marschner(F3 L, F3 V, F3 U, const fiber_strand_material& m, float 
     float ctd = cosf(theta_d);
     float eta_prime = sqrtf(wmax(0.0f, m.eta * m.eta - sti * sti)) / ctd;
     float mup[3] = {sig[0] / ctd, sig[1] / ctd, sig[2] / ctd};
-    float cos_td = cosf(theta_d);
+    const float cos_td = ctd;  // cos(theta_d), the same evaluation
     // The quadrature point's Fresnel, absorption and azimuth terms depend on
     // the segment only, not on the path p, so they are evaluated once per point
     // and reused by the three paths; each path's sum keeps its order (i = 0..9).
+    // asin(h) serves gamma_i and the azimuth shift alike, and asin(clamp(x))
+    // equals asin(x) whenever |x| <= 1. The path powers are exact products:
+    // pow(x, 0) = 1, pow(x, 1) = x and pow(x, 2) = x * x correctly rounded.
     float acc[3][3] = {{0.0f, 0.0f, 0.0f}, {0.0f, 0.0f, 0.0f}, {0.0f, 0.0f, 0.0f}};
     for (uint32_t i = 0; i < 10u; ++i) {
-        float h = wclamp(-1.0f + 1e-6f, 1.0f - 1e-6f, c_leg_roots[i]);
+        const float h = qt.h[i];
         // A (:383-413)
-        float gamma_t = asinf(h / eta_prime);
-        float gamma_i = asinf(h);
-        float fr = fresnel_reflectance(1.0f, m.eta, acosf(cos_td * cosf(gamma_i)));
+        const float x_t = h / eta_prime;
+        float gamma_t = asinf(x_t);
+        float gamma_i = qt.gi[i];
+        float fr = fresnel_reflectance(1.0f, m.eta, acosf(cos_td * qt.cgi[i]));
         float c2 = 1.0f + cosf(2.0f * gamma_t);
         float T[3] = {expf(-2.0f * mup[0] * c2), expf(-2.0f * mup[1] * c2), expf(-2.0f * mup[2] * c2)};
         float f_ = 1.0f - fr;
         // Phi (:464-468)
-        float gt2 = asinf(wclamp(h / eta_prime, -1.0f, 1.0f));
-        float asin_h = asinf(h);
+        float gt2 = fabsf(x_t) <= 1.0f ? gamma_t : asinf(wclamp(x_t, -1.0f, 1.0f));
+        float asin_h = gamma_i;
         for (uint32_t p = 0; p < 3u; ++p) {
             float A[3];
             if (p == 0u) {
                 for (int q = 0; q < 3; ++q) A[q] = fr * T[q] * T[q];
+            } else if (p == 1u) {
+                float k = (f_ * f_) * 1.0f;
+                for (int q = 0; q < 3; ++q) A[q] = k * T[q];
             } else {
-                float k = (f_ * f_) * powf(fr, u2f(p - 1u));
-                for (int q = 0; q < 3; ++q) A[q] = k * powf(T[q], u2f(p));
+                float k = (f_ * f_) * fr;
+                for (int q = 0; q < 3; ++q) A[q] = k * (T[q] * T[q]);
             }
             float shift = 2.0f * u2f(p) * gt2 - 2.0f * asin_h + u2f(p) * kPi;
             float det = gaussian_detector(beta_azim, phi - shift);
@@ -169,6 +204,9 @@ __device__ F3 marschner(F3 L, F3 V, F3 U, const fiber_strand_material& m, float 
 __global__ void __launch_bounds__(128) k_shade(const FrameParams* __restrict__ Pp,
                                                const InstanceView* __restrict__ inst, RenderArgs R) {
     const FrameParams& P = *Pp;
+    __shared__ QuadTable s_quad;
+    fill_quad_table(s_quad);
+    __syncthreads();
     const uint32_t n = *((volatile uint32_t*)&R.counters->frustum_task_base[P.camera_frustum_end]);
     const uint32_t cap = P.atlas_cap;
     const uint32_t nl = min(P.L, 4u);
@@ -203,7 +241,7 @@ __global__ void __launch_bounds__(128) k_shade(const FrameParams* __restrict__ P
         for (uint32_t j = 0; j < P.L; ++j) {
             const float* ld = P.light_dir[j];
             F3 L = nrm3(f3(ld[0], ld[1], ld[2]));
-            F3 b = marschner(L, V, U, mat, occ);
+            F3 b = marschner(L, V, U, mat, occ, s_quad);
             float bb[3] = {b.x, b.y, b.z};
             for (int q = 0; q < 3; ++q) {
                 float c = bb[q] * (P.light_color[j][q] / 255.0f);
