@@ -251,6 +251,61 @@ __device__ __forceinline__ uint32_t lb_exclusive(unsigned long long* status, uin
     return excl;
 }
 
+// Warp form of lb_exclusive: called by all 32 lanes of one warp with the same
+// tile and aggregate; returns the exclusive prefix in every lane. Each step
+// reads a window of 32 predecessors at once (lane i reads tile - 1 - i) and
+// adds the values up to the nearest inclusive one, so a block walks back
+// through 32 published aggregates per L2 round trip. Waiting is bounded as in
+// lb_exclusive.
+__device__ __forceinline__ uint32_t lb_exclusive_warp(unsigned long long* status, uint32_t tile, uint32_t epoch,
+                                                      uint32_t aggregate, uint32_t* error) {
+    const uint32_t lane = threadIdx.x & 31u;
+    if (tile == 0) {
+        if (lane == 0) lb_publish(status, 0, epoch, 2u, aggregate);
+        return 0u;
+    }
+    if (lane == 0) lb_publish(status, tile, epoch, 1u, aggregate);
+    uint32_t excl = 0;
+    int64_t end = (int64_t)tile;  // window: predecessors end - 1 - lane
+    uint32_t spins = 0;
+    for (;;) {
+        const int64_t pred = end - 1 - (int64_t)lane;
+        uint32_t flag = 2u, val = 0u;  // below tile 0: an inclusive zero
+        if (pred >= 0) {
+            cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> a(status[pred]);
+            const unsigned long long v = a.load(cuda::memory_order_acquire);
+            const uint32_t hi = (uint32_t)(v >> 32);
+            flag = (hi >> 2) == (epoch & 0x3FFFFFFFu) ? (hi & 3u) : 0u;
+            val = (uint32_t)v;
+        }
+        const unsigned incl = __ballot_sync(0xFFFFFFFFu, flag == 2u);
+        const unsigned waiting = __ballot_sync(0xFFFFFFFFu, flag == 0u);
+        const uint32_t first = incl ? (uint32_t)(__ffs(incl) - 1) : 32u;
+        const unsigned needed = first >= 31u ? 0xFFFFFFFFu : ((2u << first) - 1u);
+        if (waiting & needed) {
+            bool give_up = ++spins > kSpinLimit;
+            if ((spins & 255u) == 0u) {
+                const uint32_t err = lane == 0 ? *((volatile uint32_t*)error) : 0u;
+                give_up = give_up || __shfl_sync(0xFFFFFFFFu, err, 0) != 0u;
+            }
+            if (give_up) {
+                if (lane == 0) atomicOr(error, kErrTimeout);
+                break;
+            }
+            __nanosleep(32);
+            continue;
+        }
+        uint32_t part = lane <= first ? val : 0u;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xFFFFFFFFu, part, o);
+        excl += part;
+        if (first < 32u) break;
+        end -= 32;
+    }
+    if (lane == 0) lb_publish(status, tile, epoch, 2u, excl + aggregate);
+    return excl;
+}
+
 // Block-wide exclusive scan of one value per thread (blockDim multiple of 32).
 template <int kThreads>
 __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* smem_warp, uint32_t& total) {

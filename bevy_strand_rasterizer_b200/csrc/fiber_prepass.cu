@@ -312,15 +312,17 @@ __global__ void __launch_bounds__(kFineThreads) k_fine(const FrameParams* __rest
         }
         if (lane == 0) s_warp_count[warp] = count;
         __syncthreads();
-        if (threadIdx.x == 0) {
+        if (threadIdx.x < 32u) {
             uint32_t agg = 0;
             for (int w = 0; w < kFineWarps; ++w) agg += s_warp_count[w];
-            uint32_t base = lb_exclusive(A.lb_status, tile, P.epoch, agg, &A.counters->error);
-            s_base = base;
-            if (tile % tiles_per_f == 0u) A.counters->frustum_task_base[f] = base;
-            if (tile == n_tiles - 1u) {
-                A.counters->tasks = base + agg;
-                A.counters->frustum_task_base[P.F] = base + agg;
+            uint32_t base = lb_exclusive_warp(A.lb_status, tile, P.epoch, agg, &A.counters->error);
+            if (threadIdx.x == 0) {
+                s_base = base;
+                if (tile % tiles_per_f == 0u) A.counters->frustum_task_base[f] = base;
+                if (tile == n_tiles - 1u) {
+                    A.counters->tasks = base + agg;
+                    A.counters->frustum_task_base[P.F] = base + agg;
+                }
             }
         }
         __syncthreads();
@@ -429,7 +431,7 @@ struct CountSink {
 
 struct FillSink {
     const PrepassArgs* A;
-    uint32_t page, base, count, inst, seg, mat, key;
+    uint32_t page, base, count, task;
     __device__ __forceinline__ bool page_slot(uint32_t pti) {
         uint32_t h = A->page_table[pti];
         if (h == 0u || h == kMarked) return false;
@@ -444,8 +446,7 @@ struct FillSink {
         const uint32_t lw = atomicAdd(A->cursors + g, 1u);
         const uint64_t dst = (uint64_t)base + A->offsets[g] + lw;
         if (dst >= (uint64_t)base + count) return;
-        A->refs[dst] = fiber_fine_seg_ref{inst, seg, mat};
-        A->ref_keys[dst] = key;
+        A->ref_keys[dst] = task;  // k_sort_cells turns it into the reference
     }
 };
 
@@ -598,7 +599,7 @@ __device__ __forceinline__ bool visits_unused(const PrepassArgs& A) {
 // the rest. When the records do not fit (or slots exceed 24 bits) the pass
 // still marks every page and raises visit_overflow, which hands count and fill
 // to the walking kernels.
-__global__ void __launch_bounds__(kVisitThreads) k_visit(const FrameParams* __restrict__ Pp, PrepassArgs A) {
+__global__ void __launch_bounds__(kVisitThreads, 3) k_visit(const FrameParams* __restrict__ Pp, PrepassArgs A) {
     const FrameParams& P = *Pp;
     __shared__ uint32_t s_buf[kVisitSlots * kVisitThreads];
     __shared__ uint32_t s_warp[33];
@@ -660,9 +661,12 @@ __global__ void __launch_bounds__(256) k_count_visits(PrepassArgs A) {
     }
 }
 
-// K11 over visit records: make_fine_seg_ref (:1313-1327) at page base + cell
-// offset + rank.
-__global__ void __launch_bounds__(256) k_fill_visits(const InstanceView* __restrict__ inst, PrepassArgs A) {
+// K11 over visit records: the visit's slot is page base + cell offset + rank.
+// The fill scatters only the binning task index (4 B, into ref_keys, which a
+// frame's L2 holds); k_sort_cells gathers each cell's tasks, builds the
+// references (make_fine_seg_ref, :1313-1327) and writes them in canonical
+// order, contiguously.
+__global__ void __launch_bounds__(256) k_fill_visits(PrepassArgs A) {
     if (visits_unused(A)) return;
     const uint32_t n = (uint32_t)*((volatile unsigned long long*)&A.counters->visits);
     for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
@@ -672,13 +676,7 @@ __global__ void __launch_bounds__(256) k_fill_visits(const InstanceView* __restr
         if (pm.seg_ref_count == 0u) continue;
         const uint64_t dst = (uint64_t)pm.seg_ref_base + A.offsets[g] + A.visit_rank[r];
         if (dst >= (uint64_t)pm.seg_ref_base + pm.seg_ref_count) continue;
-        const uint32_t k = A.visit_task[r];
-        const uint4 t = reinterpret_cast<const uint4*>(A.tasks)[k];
-        const uint32_t depths = A.projected[k].depths;
-        const InstanceView& in = inst[t.x];
-        const uint32_t mat = t.y < in.n_meta ? in.meta[t.y].material_idx : 0u;
-        A.refs[dst] = fiber_fine_seg_ref{t.x, t.z, mat};
-        A.ref_keys[dst] = (depths & 0xFFFFu) + (depths >> 16u);
+        A.ref_keys[dst] = A.visit_task[r];
     }
 }
 
@@ -697,10 +695,7 @@ __global__ void __launch_bounds__(256) k_traverse(const FrameParams* __restrict_
             CountSink cs{A.page_table, A.counts, 0u};
             walk_task(P, A, w, cs);
         } else {
-            // make_fine_seg_ref (:1313-1327)
-            const InstanceView& in = inst[w.i];
-            const uint32_t mat = w.strand < in.n_meta ? in.meta[w.strand].material_idx : 0u;
-            FillSink fs{&A, 0u, 0u, 0u, w.i, w.seg, mat, (w.depths & 0xFFFFu) + (w.depths >> 16u)};
+            FillSink fs{&A, 0u, 0u, 0u, k};
             walk_task(P, A, w, fs);
         }
     }
@@ -733,10 +728,12 @@ __global__ void __launch_bounds__(kScanThreads) k_alloc_pages(const FrameParams*
         }
         uint32_t total;
         uint32_t excl = block_exclusive_scan<kScanThreads>(cnt, s_warp, total);
-        if (threadIdx.x == 0) {
-            uint32_t base = lb_exclusive(A.lb_status, tile, P.epoch, total, &A.counters->error);
-            s_base = base;
-            if (tile == n_tiles - 1u) A.counters->pages = min(base + total, P.page_capacity);
+        if (threadIdx.x < 32u) {
+            uint32_t base = lb_exclusive_warp(A.lb_status, tile, P.epoch, total, &A.counters->error);
+            if (threadIdx.x == 0) {
+                s_base = base;
+                if (tile == n_tiles - 1u) A.counters->pages = min(base + total, P.page_capacity);
+            }
         }
         __syncthreads();
         uint32_t idx = s_base + excl;
@@ -787,8 +784,9 @@ __global__ void __launch_bounds__(256) k_prefix_pages(const FrameParams* __restr
         uint32_t excl = block_exclusive_scan<256>(c, s_warp, total);
         A.offsets[g] = excl;
         A.cursors[g] = 0u;
+        uint32_t base = 0u;
+        if (threadIdx.x < 32u) base = lb_exclusive_warp(A.lb_status, page, P.epoch, total, &A.counters->error);
         if (threadIdx.x == 0) {
-            uint32_t base = lb_exclusive(A.lb_status, page, P.epoch, total, &A.counters->error);
             fiber_fine_page_meta pm = A.page_meta[page];
             uint32_t flags = 0u;
             if (total > 0u && (uint64_t)base + total > (uint64_t)P.ref_capacity) {
@@ -852,10 +850,12 @@ __global__ void __launch_bounds__(kScanThreads) k_compact_active(const FramePara
         uint32_t excl = block_exclusive_scan<kScanThreads>(cnt, s_warp, total);
         for (int o = 16; o > 0; o >>= 1) cam += __shfl_xor_sync(0xFFFFFFFFu, cam, o);
         if ((threadIdx.x & 31) == 0 && cam) atomicAdd(&A.counters->camera_active, cam);
-        if (threadIdx.x == 0) {
-            uint32_t base = lb_exclusive(A.lb_status, tile, P.epoch, total, &A.counters->error);
-            s_base = base;
-            if (tile == n_tiles - 1u) A.counters->active_tiles = base + total;
+        if (threadIdx.x < 32u) {
+            uint32_t base = lb_exclusive_warp(A.lb_status, tile, P.epoch, total, &A.counters->error);
+            if (threadIdx.x == 0) {
+                s_base = base;
+                if (tile == n_tiles - 1u) A.counters->active_tiles = base + total;
+            }
         }
         __syncthreads();
         uint32_t idx = s_base + excl;
@@ -881,8 +881,25 @@ __device__ __forceinline__ unsigned long long ref_sort_key(uint32_t key17, uint3
 // e = lane * R + r, bitonic network over 32 R keys (padding sorts last).
 // Strides below R compare registers of one lane; larger strides exchange the
 // same register with lane ^ (stride / R).
+// The reference of binning task k (make_fine_seg_ref, :1313-1327) as a sort
+// key (depth key, instance, segment) and its material.
+__device__ __forceinline__ void task_entry(const PrepassArgs& A, const InstanceView* __restrict__ inst, uint32_t k,
+                                           unsigned long long& key, uint32_t& mat) {
+    const uint4 t = reinterpret_cast<const uint4*>(A.tasks)[k];
+    const uint32_t depths = A.projected[k].depths;
+    const InstanceView& in = inst[t.x];
+    mat = t.y < in.n_meta ? in.meta[t.y].material_idx : 0u;
+    key = ref_sort_key((depths & 0xFFFFu) + (depths >> 16u), t.x, t.z);
+}
+
+__device__ __forceinline__ void store_entry(const PrepassArgs& A, uint32_t dst, unsigned long long key, uint32_t mat) {
+    A.refs[dst] = fiber_fine_seg_ref{(uint32_t)(key >> 32) & 0x7FFFu, (uint32_t)key, mat};
+    A.ref_keys[dst] = 0x1FFFFu - (uint32_t)(key >> 47);
+}
+
 template <int R>
-__device__ __forceinline__ void warp_sort_cell(const PrepassArgs& A, uint32_t base, uint32_t n, int lane) {
+__device__ __forceinline__ void warp_sort_cell(const PrepassArgs& A, const InstanceView* __restrict__ inst,
+                                               uint32_t base, uint32_t n, int lane) {
     unsigned long long k[R];
     uint32_t mat[R];
 #pragma unroll
@@ -890,11 +907,7 @@ __device__ __forceinline__ void warp_sort_cell(const PrepassArgs& A, uint32_t ba
         const uint32_t e = (uint32_t)lane * R + r;
         k[r] = ~0ull;
         mat[r] = 0u;
-        if (e < n) {
-            fiber_fine_seg_ref ref = A.refs[base + e];
-            k[r] = ref_sort_key(A.ref_keys[base + e], ref.inst_id, ref.seg_id);
-            mat[r] = ref.material_idx;
-        }
+        if (e < n) task_entry(A, inst, A.ref_keys[base + e], k[r], mat[r]);
     }
 #pragma unroll
     for (int size = 2; size <= 32 * R; size <<= 1) {
@@ -930,20 +943,48 @@ __device__ __forceinline__ void warp_sort_cell(const PrepassArgs& A, uint32_t ba
 #pragma unroll
     for (int r = 0; r < R; ++r) {
         const uint32_t e = (uint32_t)lane * R + r;
-        if (e < n) {
-            A.refs[base + e] = fiber_fine_seg_ref{(uint32_t)(k[r] >> 32) & 0x7FFFu, (uint32_t)k[r], mat[r]};
-            A.ref_keys[base + e] = 0x1FFFFu - (uint32_t)(k[r] >> 47);
-        }
+        if (e < n) store_entry(A, base + e, k[r], mat[r]);
     }
 }
 
 constexpr uint32_t kWarpSortMax = 256;  // 32 lanes x 8 registers
+constexpr uint32_t kThreadSortMax = 8;
 
-__device__ __forceinline__ void warp_sort_any(const PrepassArgs& A, uint32_t base, uint32_t n, int lane) {
-    if (n <= 32u) warp_sort_cell<1>(A, base, n, lane);
-    else if (n <= 64u) warp_sort_cell<2>(A, base, n, lane);
-    else if (n <= 128u) warp_sort_cell<4>(A, base, n, lane);
-    else warp_sort_cell<8>(A, base, n, lane);
+__device__ __forceinline__ void warp_sort_any(const PrepassArgs& A, const InstanceView* __restrict__ inst,
+                                              uint32_t base, uint32_t n, int lane) {
+    if (n <= 32u) warp_sort_cell<1>(A, inst, base, n, lane);
+    else if (n <= 64u) warp_sort_cell<2>(A, inst, base, n, lane);
+    else if (n <= 128u) warp_sort_cell<4>(A, inst, base, n, lane);
+    else warp_sort_cell<8>(A, inst, base, n, lane);
+}
+
+// One thread sorts a cell of at most 8 references in registers: Batcher's
+// odd-even merge network for 8 inputs (19 comparators); padding sorts last.
+__device__ __forceinline__ void thread_sort_cell(const PrepassArgs& A, const InstanceView* __restrict__ inst,
+                                                 uint32_t base, uint32_t n) {
+    unsigned long long k[8];
+    uint32_t mat[8];
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+        k[e] = ~0ull;
+        mat[e] = 0u;
+        if ((uint32_t)e < n) task_entry(A, inst, A.ref_keys[base + e], k[e], mat[e]);
+    }
+    auto cas = [&](int a, int b) {
+        if (k[a] > k[b]) {
+            const unsigned long long tk = k[a]; k[a] = k[b]; k[b] = tk;
+            const uint32_t tm = mat[a]; mat[a] = mat[b]; mat[b] = tm;
+        }
+    };
+    cas(0, 1); cas(2, 3); cas(4, 5); cas(6, 7);
+    cas(0, 2); cas(1, 3); cas(4, 6); cas(5, 7);
+    cas(1, 2); cas(5, 6);
+    cas(0, 4); cas(1, 5); cas(2, 6); cas(3, 7);
+    cas(2, 4); cas(3, 5);
+    cas(1, 2); cas(3, 4); cas(5, 6);
+#pragma unroll
+    for (int e = 0; e < 8; ++e)
+        if ((uint32_t)e < n) store_entry(A, base + e, k[e], mat[e]);
 }
 
 __global__ void __launch_bounds__(256) k_emit(const FrameParams* __restrict__ Pp, PrepassArgs A) {
@@ -989,8 +1030,9 @@ __global__ void __launch_bounds__(256) k_emit(const FrameParams* __restrict__ Pp
         if (lane == 0) s_load[warp] = load;
         uint32_t n_work;
         uint32_t excl = block_exclusive_scan<256>(has, s_warp, n_work);
+        uint32_t wb = 0u;
+        if (threadIdx.x < 32u) wb = lb_exclusive_warp(A.lb_status, a, P.epoch, n_work, &A.counters->error);
         if (threadIdx.x == 0) {
-            uint32_t wb = lb_exclusive(A.lb_status, a, P.epoch, n_work, &A.counters->error);
             s_base = wb;
             uint32_t total_load = 0;
             for (int w = 0; w < 8; ++w) total_load += s_load[w];
@@ -1016,7 +1058,7 @@ __global__ void __launch_bounds__(256) k_emit(const FrameParams* __restrict__ Pp
 // instance, then segment), after the fill: one block per page, one warp per 32
 // cells; each warp sorts its cells of 2..256 references in registers and
 // queues longer cells for k_sort_big_cells. Warps never wait on each other.
-__global__ void __launch_bounds__(256) k_sort_cells(PrepassArgs A) {
+__global__ void __launch_bounds__(256) k_sort_cells(const InstanceView* __restrict__ inst, PrepassArgs A) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t pages = *((volatile uint32_t*)&A.counters->pages);
     for (uint32_t page = blockIdx.x; page < pages; page += gridDim.x) {
@@ -1026,17 +1068,38 @@ __global__ void __launch_bounds__(256) k_sort_cells(PrepassArgs A) {
         const size_t g = (size_t)page * kPageSize + cell;
         const uint32_t cnt = A.counts[g];
         const uint32_t base = pm.seg_ref_base + A.offsets[g];
-        if (cnt > kWarpSortMax) {
-            uint32_t slot = atomicAdd(&A.counters->big_cells, 1u);
-            A.big_cells[slot] = make_uint2(base, cnt);
+        // Cells of up to 8 (nearly all of them) sort in their own thread; the
+        // warp then takes the larger ones one at a time. A cell longer than a
+        // warp sort is converted in place by the warp and queued for
+        // k_sort_big_cells.
+        if (cnt == 1u) {
+            unsigned long long key;
+            uint32_t mat;
+            task_entry(A, inst, A.ref_keys[base], key, mat);
+            store_entry(A, base, key, mat);
+        } else if (cnt >= 2u && cnt <= kThreadSortMax) {
+            thread_sort_cell(A, inst, base, cnt);
         }
-        unsigned todo = __ballot_sync(0xFFFFFFFFu, cnt >= 2u && cnt <= kWarpSortMax);
+        unsigned todo = __ballot_sync(0xFFFFFFFFu, cnt > kThreadSortMax);
         while (todo) {
             const int src = __ffs(todo) - 1;
             todo &= todo - 1u;
             const uint32_t b = __shfl_sync(0xFFFFFFFFu, base, src);
             const uint32_t n = __shfl_sync(0xFFFFFFFFu, cnt, src);
-            warp_sort_any(A, b, n, lane);
+            if (n <= kWarpSortMax) {
+                warp_sort_any(A, inst, b, n, lane);
+            } else {
+                for (uint32_t e = (uint32_t)lane; e < n; e += 32u) {
+                    unsigned long long key;
+                    uint32_t mat;
+                    task_entry(A, inst, A.ref_keys[b + e], key, mat);
+                    store_entry(A, b + e, key, mat);
+                }
+                if (lane == src) {
+                    const uint32_t slot = atomicAdd(&A.counters->big_cells, 1u);
+                    A.big_cells[slot] = make_uint2(b, n);
+                }
+            }
         }
     }
 }
@@ -1155,7 +1218,7 @@ void launch_prefix(const LaunchCtx& L, const PrepassArgs& A) {
     k_prefix_pages<<<L.sm_count * 6, 256, 0, L.stream>>>(L.P, A);
 }
 void launch_fill(const LaunchCtx& L, const PrepassArgs& A) {
-    k_fill_visits<<<L.sm_count * 8, 256, 0, L.stream>>>(L.inst, A);
+    k_fill_visits<<<L.sm_count * 8, 256, 0, L.stream>>>(A);
     k_traverse<kFill><<<L.sm_count * 8, 256, 0, L.stream>>>(L.P, L.inst, A);
 }
 void launch_compact_active(const LaunchCtx& L, const PrepassArgs& A) {
@@ -1165,7 +1228,7 @@ void launch_emit(const LaunchCtx& L, const PrepassArgs& A) {
     k_emit<<<L.sm_count * 6, 256, 0, L.stream>>>(L.P, A);
 }
 void launch_sort_cells(const LaunchCtx& L, const PrepassArgs& A) {
-    k_sort_cells<<<L.sm_count * 8, 256, 0, L.stream>>>(A);
+    k_sort_cells<<<L.sm_count * 8, 256, 0, L.stream>>>(L.inst, A);
 }
 void launch_sort_big(const LaunchCtx& L, const PrepassArgs& A) {
     static bool configured[64] = {};
