@@ -987,17 +987,18 @@ __device__ __forceinline__ void thread_sort_cell(const PrepassArgs& A, const Ins
         if ((uint32_t)e < n) store_entry(A, base + e, k[e], mat[e]);
 }
 
+// One warp per active tile: the tile's 256 depth slots (16 coarse z x 16 fine
+// z, near to far) are slots t = 8 lane .. 8 lane + 7, so each lane's slots
+// share one coarse z (one page) and the warp scan keeps the slot order. Warps
+// claim tiles and look back on their own; no block barrier is involved.
 __global__ void __launch_bounds__(256) k_emit(const FrameParams* __restrict__ Pp, PrepassArgs A) {
     const FrameParams& P = *Pp;
-    __shared__ uint32_t s_tile, s_base;
-    __shared__ uint32_t s_warp[33];
-    __shared__ uint32_t s_load[8];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t lane = threadIdx.x & 31u;
     const uint32_t n_active = *((volatile uint32_t*)&A.counters->active_tiles);
     for (;;) {
-        if (threadIdx.x == 0) s_tile = atomicAdd(A.tile_counter, 1u);
-        __syncthreads();
-        const uint32_t a = s_tile;
+        uint32_t a = 0u;
+        if (lane == 0) a = atomicAdd(A.tile_counter, 1u);
+        a = __shfl_sync(0xFFFFFFFFu, a, 0);
         if (a >= n_active) break;
         const uint32_t packed = A.active_list[a];
         const uint32_t lt = packed % 16u, tile = packed / 16u;
@@ -1008,49 +1009,63 @@ __global__ void __launch_bounds__(256) k_emit(const FrameParams* __restrict__ Pp
         const uint32_t fx = (lc % d.coarse_tiles_x) * kCoarseExtent + lx;
         const uint32_t fy = (lc / d.coarse_tiles_x) * kCoarseExtent + ly;
         const uint32_t screen_tile = fy * ceil_div(d.screen_width, d.froxel_size_x) + fx;
-        const uint32_t depth_lane = kPageSize - 1u - threadIdx.x;
-        const uint32_t cz = depth_lane / kDepthSlices, fz = depth_lane % kDepthSlices;
+        const uint32_t dl0 = kPageSize - 1u - lane * 8u;  // depth slot of j = 0; slot j is dl0 - j
+        const uint32_t cz = dl0 / kDepthSlices;
         const uint32_t pti = tile * kDepthSlices + cz;
-        uint32_t cnt = 0, base = 0, page = kInvalid, cell = 0;
+        uint32_t page = kInvalid, pbase = 0u;
+        bool ok = false;
         if (f != kInvalid) {
-            uint32_t handle = A.page_table[pti];
+            const uint32_t handle = A.page_table[pti];
             if (handle != 0u && handle != kMarked) {
                 page = handle - 1u;
-                fiber_fine_page_meta pm = A.page_meta[page];
-                cell = (fz * kCoarseExtent + ly) * kCoarseExtent + lx;
-                if (pm.seg_ref_count > 0u && pm.flags == 0u) {
-                    cnt = A.counts[(size_t)page * kPageSize + cell];
-                    if (cnt > 0u) base = pm.seg_ref_base + A.offsets[(size_t)page * kPageSize + cell];
-                }
+                const fiber_fine_page_meta pm = A.page_meta[page];
+                ok = pm.seg_ref_count > 0u && pm.flags == 0u;
+                pbase = pm.seg_ref_base;
             }
         }
-        const uint32_t has = cnt > 0u ? 1u : 0u;
-        uint32_t load = cnt;
+        uint32_t cnt[8];
+        uint32_t nh = 0u, load = 0u;
+#pragma unroll
+        for (uint32_t j = 0; j < 8u; ++j) {
+            const uint32_t fz = (dl0 - j) % kDepthSlices;
+            const uint32_t cell = (fz * kCoarseExtent + ly) * kCoarseExtent + lx;
+            cnt[j] = ok ? A.counts[(size_t)page * kPageSize + cell] : 0u;
+            nh += cnt[j] > 0u ? 1u : 0u;
+            load += cnt[j];
+        }
+        uint32_t x = nh;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+            if (lane >= (uint32_t)o) x += y;
+        }
+        const uint32_t excl = x - nh;
+        const uint32_t n_work = __shfl_sync(0xFFFFFFFFu, x, 31);
+#pragma unroll
         for (int o = 16; o > 0; o >>= 1) load += __shfl_xor_sync(0xFFFFFFFFu, load, o);
-        if (lane == 0) s_load[warp] = load;
-        uint32_t n_work;
-        uint32_t excl = block_exclusive_scan<256>(has, s_warp, n_work);
-        uint32_t wb = 0u;
-        if (threadIdx.x < 32u) wb = lb_exclusive_warp(A.lb_status, a, P.epoch, n_work, &A.counters->error);
-        if (threadIdx.x == 0) {
-            s_base = wb;
-            uint32_t total_load = 0;
-            for (int w = 0; w < 8; ++w) total_load += s_load[w];
-            A.runs[a] = fiber_raster_tile_run{wb, n_work, f, screen_tile, total_load, 0u, 0u, 0u};
+        const uint32_t wb = lb_exclusive_warp(A.lb_status, a, P.epoch, n_work, &A.counters->error);
+        if (lane == 0) {
+            A.runs[a] = fiber_raster_tile_run{wb, n_work, f, screen_tile, load, 0u, 0u, 0u};
             if (a == n_active - 1u) A.counters->work_items = wb + n_work;
         }
-        __syncthreads();
-        if (has) {
-            uint32_t lutk = pti;
-            fiber_coarse_depth_lut_entry lut = A.lut[lutk];
-            uint32_t dkey = lut.virtual_count_q == 0u ? fz : lut.virtual_start_q + (lut.virtual_count_q * fz) / kDepthSlices;
-            uint32_t dst = s_base + excl;
-            if (dst < P.work_capacity)
-                A.work[dst] = fiber_raster_work_item{base, cnt, f, screen_tile, dkey, cnt, page, cell};
-            else
-                atomicOr(&A.counters->overflow, 8u);
+        if (nh) {
+            const fiber_coarse_depth_lut_entry lut = A.lut[pti];
+            uint32_t dst = wb + excl;
+#pragma unroll
+            for (uint32_t j = 0; j < 8u; ++j) {
+                if (cnt[j] == 0u) continue;
+                const uint32_t fz = (dl0 - j) % kDepthSlices;
+                const uint32_t cell = (fz * kCoarseExtent + ly) * kCoarseExtent + lx;
+                const uint32_t dkey =
+                    lut.virtual_count_q == 0u ? fz : lut.virtual_start_q + (lut.virtual_count_q * fz) / kDepthSlices;
+                const uint32_t base = pbase + A.offsets[(size_t)page * kPageSize + cell];
+                if (dst < P.work_capacity)
+                    A.work[dst] = fiber_raster_work_item{base, cnt[j], f, screen_tile, dkey, cnt[j], page, cell};
+                else
+                    atomicOr(&A.counters->overflow, 8u);
+                ++dst;
+            }
         }
-        __syncthreads();
     }
 }
 
@@ -1058,7 +1073,7 @@ __global__ void __launch_bounds__(256) k_emit(const FrameParams* __restrict__ Pp
 // instance, then segment), after the fill: one block per page, one warp per 32
 // cells; each warp sorts its cells of 2..256 references in registers and
 // queues longer cells for k_sort_big_cells. Warps never wait on each other.
-__global__ void __launch_bounds__(256) k_sort_cells(const InstanceView* __restrict__ inst, PrepassArgs A) {
+__global__ void __launch_bounds__(256, 4) k_sort_cells(const InstanceView* __restrict__ inst, PrepassArgs A) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t pages = *((volatile uint32_t*)&A.counters->pages);
     for (uint32_t page = blockIdx.x; page < pages; page += gridDim.x) {
