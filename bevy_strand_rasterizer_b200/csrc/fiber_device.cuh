@@ -94,6 +94,8 @@ static_assert(sizeof(FrameCounters) == 160, "FrameCounters layout");
 
 // Look-back stages (index into FrameCounters::tile_counter and the status regions).
 enum LookbackStage : uint32_t { kStageFine = 0, kStageAlloc = 1, kStagePrefix = 2, kStageActive = 3, kStageEmit = 4, kStageCount = 5 };
+// Run counters of the rasters (blocks claim tile runs dynamically).
+constexpr uint32_t kShadowRunCounter = 5, kCameraRunCounter = 6;
 
 // ---------------------------------------------------------------------------
 // WGSL builtin semantics

@@ -131,7 +131,7 @@ __device__ __forceinline__ bool band_candidate(const Band& B, float px, float py
     return !(fabsf(d) > B.thr) && !(s < B.slo) && !(s > B.shi);
 }
 
-__global__ void __launch_bounds__(256) k_shadow(const FrameParams* __restrict__ Pp,
+__global__ void __launch_bounds__(256, 3) k_shadow(const FrameParams* __restrict__ Pp,
                                                 const InstanceView* __restrict__ inst, RenderArgs R) {
     const FrameParams& P = *Pp;
     extern __shared__ float s_dyn[];
@@ -159,8 +159,15 @@ __global__ void __launch_bounds__(256) k_shadow(const FrameParams* __restrict__ 
     const uint32_t slot = threadIdx.x >> 2, worker = threadIdx.x & 3u;
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     float* partial = s_partial + threadIdx.x * K;
+    __shared__ uint32_t s_run;
 
-    for (uint32_t r = first + blockIdx.x; r < last; r += gridDim.x) {
+    // Blocks claim runs from a counter, so long runs do not pile up on one block.
+    for (;;) {
+        __syncthreads();
+        if (threadIdx.x == 0) s_run = first + atomicAdd(&R.counters->tile_counter[kShadowRunCounter], 1u);
+        __syncthreads();
+        const uint32_t r = s_run;
+        if (r >= last) break;
         const fiber_raster_tile_run run = R.runs[r];
         const uint32_t f = run.frustum_id;
         const uint32_t layer = light_layer(P, f);
@@ -406,7 +413,7 @@ constexpr uint16_t kEntryInvalid = 0x8000u;
 // redundantly, so they stay in step for the group blend. A group without a
 // candidate contributes transparent black and depth 0 in every lane, which
 // leaves the blend unchanged, so skipping it keeps the result.
-__global__ void __launch_bounds__(256) k_raster(const FrameParams* __restrict__ Pp,
+__global__ void __launch_bounds__(256, 3) k_raster(const FrameParams* __restrict__ Pp,
                                                 const InstanceView* __restrict__ inst, RenderArgs R) {
     const FrameParams& P = *Pp;
     // Per staged entry: 64 B of projection, radii and shading texels, the run
@@ -427,7 +434,14 @@ __global__ void __launch_bounds__(256) k_raster(const FrameParams* __restrict__ 
     const uint32_t lane = threadIdx.x & 31u, wbase = lane & ~3u, warp = threadIdx.x >> 5;
     const uint32_t cap = P.atlas_cap;
     const __half* hist = R.history[(P.hist_in & 1u) ^ 1u];
-    for (uint32_t r = blockIdx.x; r < n_runs; r += gridDim.x) {
+    __shared__ uint32_t s_run;
+    // Blocks claim runs from a counter, so long runs do not pile up on one block.
+    for (;;) {
+        __syncthreads();
+        if (threadIdx.x == 0) s_run = atomicAdd(&R.counters->tile_counter[kCameraRunCounter], 1u);
+        __syncthreads();
+        const uint32_t r = s_run;
+        if (r >= n_runs) break;
         const fiber_raster_tile_run run = R.runs[r];
         const uint32_t f = run.frustum_id;
         if (run.work_count == 0u || f >= P.camera_frustum_end) continue;
