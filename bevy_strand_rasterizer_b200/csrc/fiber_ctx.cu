@@ -106,7 +106,7 @@ struct fiber_ctx {
     DevBuf d_params, d_inst, d_counters, d_lb, d_range_valid, d_ranges, d_keep, d_inst_visible, d_inst_keep;
     DevBuf d_lut, d_tasks, d_projected, d_page_table, d_page_meta, d_counts, d_offsets, d_cursors;
     DevBuf d_refs, d_ref_keys, d_active_flags, d_active_list, d_work, d_runs, d_big_cells;
-    DevBuf d_visit_rec, d_visit_task, d_visit_rank;
+    DevBuf d_visit_rec, d_visit_task, d_visit_rank, d_task_key, d_task_mat;
     DevBuf d_dom_depth, d_dom_opacity, d_shadow_map, d_atlas, d_history[2];
     DevBuf d_color, d_depth, d_fragments, d_validate, d_host_scene, d_host_depth;
     int hist_cur = 0;
@@ -205,6 +205,8 @@ PrepassArgs prepass_args(fiber_ctx* c) {
     A.visit_rec = dp<uint32_t>(c->d_visit_rec);
     A.visit_task = dp<uint32_t>(c->d_visit_task);
     A.visit_rank = dp<uint32_t>(c->d_visit_rank);
+    A.task_key = dp<unsigned long long>(c->d_task_key);
+    A.task_mat = dp<uint32_t>(c->d_task_mat);
     return A;
 }
 
@@ -428,7 +430,7 @@ fiber_status fiber_ctx_destroy(fiber_ctx* c) {
                       &c->d_big_cells, &c->d_dom_depth, &c->d_dom_opacity, &c->d_shadow_map, &c->d_atlas,
                       &c->d_history[0], &c->d_history[1], &c->d_color, &c->d_depth, &c->d_fragments,
                       &c->d_validate, &c->d_host_scene, &c->d_host_depth, &c->d_visit_rec,
-                      &c->d_visit_task, &c->d_visit_rank};
+                      &c->d_visit_task, &c->d_visit_rank, &c->d_task_key, &c->d_task_mat};
     for (DevBuf* b : bufs) release(c, *b);
     for (int i = 0; i <= kSpanCount; ++i)
         if (c->ev[i]) cudaEventDestroy(c->ev[i]);
@@ -715,6 +717,8 @@ fiber_status fiber_frame_begin(fiber_ctx* c, const fiber_froxel_config* cam_cfg,
     ENSURE(c->d_visit_rec, visit_cap * 4, false);
     ENSURE(c->d_visit_task, visit_cap * 4, false);
     ENSURE(c->d_visit_rank, visit_cap * 4, false);
+    ENSURE(c->d_task_key, task_cap * 8, false);
+    ENSURE(c->d_task_mat, task_cap * 4, false);
     ENSURE(c->d_dom_depth, L * D * D * 4, false);
     ENSURE(c->d_dom_opacity, L * K * D * D * 4, true);
     ENSURE(c->d_shadow_map, L * S * S * 4, false);

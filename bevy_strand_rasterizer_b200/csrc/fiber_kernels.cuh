@@ -75,6 +75,8 @@ struct PrepassArgs {
     uint32_t* visit_rec;    // [ref_capacity] page-table slot << 8 | cell; the count pass rewrites it to the cell index
     uint32_t* visit_task;   // [ref_capacity] binning task of the visit
     uint32_t* visit_rank;   // [ref_capacity] rank of the visit inside its cell
+    unsigned long long* task_key;  // [task_capacity] canonical cell-order key of the task's reference
+    uint32_t* task_mat;            // [task_capacity] material index of the task's reference
 };
 
 // Device buffers of the shadow, shading, raster and composite stages.

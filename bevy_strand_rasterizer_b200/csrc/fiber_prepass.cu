@@ -589,6 +589,13 @@ __device__ __forceinline__ void walk_task(const FrameParams& P, const PrepassArg
     }
 }
 
+// Canonical order of the references in a cell as one 64-bit key: projected
+// depth key (z0_16 + z1_16, 17 bits) descending, then instance, then segment.
+__device__ __forceinline__ unsigned long long ref_sort_key(uint32_t key17, uint32_t inst, uint32_t seg) {
+    return ((unsigned long long)(0x1FFFFu - (key17 & 0x1FFFFu)) << 47) |
+           ((unsigned long long)(inst & 0x7FFFu) << 32) | (unsigned long long)seg;
+}
+
 __device__ __forceinline__ bool visits_unused(const PrepassArgs& A) {
     return *((volatile uint32_t*)&A.counters->visit_overflow) != 0u;
 }
@@ -599,7 +606,8 @@ __device__ __forceinline__ bool visits_unused(const PrepassArgs& A) {
 // the rest. When the records do not fit (or slots exceed 24 bits) the pass
 // still marks every page and raises visit_overflow, which hands count and fill
 // to the walking kernels.
-__global__ void __launch_bounds__(kVisitThreads, 3) k_visit(const FrameParams* __restrict__ Pp, PrepassArgs A) {
+__global__ void __launch_bounds__(kVisitThreads, 3) k_visit(const FrameParams* __restrict__ Pp,
+                                                            const InstanceView* __restrict__ inst, PrepassArgs A) {
     const FrameParams& P = *Pp;
     __shared__ uint32_t s_buf[kVisitSlots * kVisitThreads];
     __shared__ uint32_t s_warp[33];
@@ -613,7 +621,15 @@ __global__ void __launch_bounds__(kVisitThreads, 3) k_visit(const FrameParams* _
         TaskWalk w;
         const bool ok = k < n_cap && task_walk(P, A, k, w);
         VisitSink vs{A.page_table, s_buf + threadIdx.x, 0u, 0u, records};
-        if (ok) walk_task(P, A, w, vs);
+        if (ok) {
+            // The task's reference (make_fine_seg_ref, :1313-1327) as its sort
+            // key and material, gathered later by k_sort_cells from these
+            // compact arrays instead of from the task records.
+            const InstanceView& in = inst[w.i];
+            A.task_key[k] = ref_sort_key((w.depths & 0xFFFFu) + (w.depths >> 16u), w.i, w.seg);
+            A.task_mat[k] = w.strand < in.n_meta ? in.meta[w.strand].material_idx : 0u;
+            walk_task(P, A, w, vs);
+        }
         if (!records) continue;
         uint32_t total;
         const uint32_t excl = block_exclusive_scan<kVisitThreads>(vs.n, s_warp, total);
@@ -872,24 +888,18 @@ __global__ void __launch_bounds__(kScanThreads) k_compact_active(const FramePara
 // canonical order inside each cell (projected depth key descending, then
 // instance, then segment) is made by k_sort_cells after the fill.
 // ===========================================================================
-__device__ __forceinline__ unsigned long long ref_sort_key(uint32_t key17, uint32_t inst, uint32_t seg) {
-    return ((unsigned long long)(0x1FFFFu - (key17 & 0x1FFFFu)) << 47) |
-           ((unsigned long long)(inst & 0x7FFFu) << 32) | (unsigned long long)seg;
-}
 
 // One warp sorts a cell of up to 32 * R references in registers: element
 // e = lane * R + r, bitonic network over 32 R keys (padding sorts last).
 // Strides below R compare registers of one lane; larger strides exchange the
 // same register with lane ^ (stride / R).
 // The reference of binning task k (make_fine_seg_ref, :1313-1327) as a sort
-// key (depth key, instance, segment) and its material.
-__device__ __forceinline__ void task_entry(const PrepassArgs& A, const InstanceView* __restrict__ inst, uint32_t k,
-                                           unsigned long long& key, uint32_t& mat) {
-    const uint4 t = reinterpret_cast<const uint4*>(A.tasks)[k];
-    const uint32_t depths = A.projected[k].depths;
-    const InstanceView& in = inst[t.x];
-    mat = t.y < in.n_meta ? in.meta[t.y].material_idx : 0u;
-    key = ref_sort_key((depths & 0xFFFFu) + (depths >> 16u), t.x, t.z);
+// key (depth key, instance, segment) and its material, as k_visit stored them
+// (12 B per task, which a frame's L2 mostly holds).
+__device__ __forceinline__ void task_entry(const PrepassArgs& A, const InstanceView* __restrict__ /*inst*/,
+                                           uint32_t k, unsigned long long& key, uint32_t& mat) {
+    key = A.task_key[k];
+    mat = A.task_mat[k];
 }
 
 __device__ __forceinline__ void store_entry(const PrepassArgs& A, uint32_t dst, unsigned long long key, uint32_t mat) {
@@ -1217,7 +1227,7 @@ void launch_fine(const LaunchCtx& L, const PrepassArgs& A) {
     k_fine<<<L.sm_count * 6, kFineThreads, 0, L.stream>>>(L.P, L.inst, A);
 }
 void launch_visit(const LaunchCtx& L, const PrepassArgs& A) {
-    k_visit<<<L.sm_count * 8, kVisitThreads, 0, L.stream>>>(L.P, A);
+    k_visit<<<L.sm_count * 8, kVisitThreads, 0, L.stream>>>(L.P, L.inst, A);
 }
 void launch_alloc(const LaunchCtx& L, const PrepassArgs& A) {
     k_alloc_pages<<<L.sm_count * 4, kScanThreads, 0, L.stream>>>(L.P, A);
