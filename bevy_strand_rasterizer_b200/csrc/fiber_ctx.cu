@@ -106,7 +106,7 @@ struct fiber_ctx {
     DevBuf d_params, d_inst, d_counters, d_lb, d_range_valid, d_ranges, d_keep, d_inst_visible, d_inst_keep;
     DevBuf d_lut, d_tasks, d_projected, d_page_table, d_page_meta, d_counts, d_offsets, d_cursors;
     DevBuf d_refs, d_ref_keys, d_active_flags, d_active_list, d_work, d_runs, d_big_cells;
-    DevBuf d_visit_rec, d_visit_task, d_visit_rank, d_task_key, d_task_mat;
+    DevBuf d_visit_rec, d_visit_task, d_visit_rank, d_task_key, d_task_mat, d_cells_small, d_cells_large;
     DevBuf d_dom_depth, d_dom_opacity, d_shadow_map, d_atlas, d_history[2];
     DevBuf d_color, d_depth, d_fragments, d_validate, d_host_scene, d_host_depth;
     int hist_cur = 0;
@@ -207,6 +207,8 @@ PrepassArgs prepass_args(fiber_ctx* c) {
     A.visit_rank = dp<uint32_t>(c->d_visit_rank);
     A.task_key = dp<unsigned long long>(c->d_task_key);
     A.task_mat = dp<uint32_t>(c->d_task_mat);
+    A.cells_small = dp<uint2>(c->d_cells_small);
+    A.cells_large = dp<uint2>(c->d_cells_large);
     return A;
 }
 
@@ -430,7 +432,8 @@ fiber_status fiber_ctx_destroy(fiber_ctx* c) {
                       &c->d_big_cells, &c->d_dom_depth, &c->d_dom_opacity, &c->d_shadow_map, &c->d_atlas,
                       &c->d_history[0], &c->d_history[1], &c->d_color, &c->d_depth, &c->d_fragments,
                       &c->d_validate, &c->d_host_scene, &c->d_host_depth, &c->d_visit_rec,
-                      &c->d_visit_task, &c->d_visit_rank, &c->d_task_key, &c->d_task_mat};
+                      &c->d_visit_task, &c->d_visit_rank, &c->d_task_key, &c->d_task_mat,
+                      &c->d_cells_small, &c->d_cells_large};
     for (DevBuf* b : bufs) release(c, *b);
     for (int i = 0; i <= kSpanCount; ++i)
         if (c->ev[i]) cudaEventDestroy(c->ev[i]);
@@ -719,6 +722,9 @@ fiber_status fiber_frame_begin(fiber_ctx* c, const fiber_froxel_config* cam_cfg,
     ENSURE(c->d_visit_rank, visit_cap * 4, false);
     ENSURE(c->d_task_key, task_cap * 8, false);
     ENSURE(c->d_task_mat, task_cap * 4, false);
+    // Non-empty cells: at most one per kept reference and one per cell.
+    ENSURE(c->d_cells_small, std::min<uint64_t>(ref_cap, page_cap * kPageSize) * sizeof(uint2), false);
+    ENSURE(c->d_cells_large, (ref_cap / 9 + 1) * sizeof(uint2), false);
     ENSURE(c->d_dom_depth, L * D * D * 4, false);
     ENSURE(c->d_dom_opacity, L * K * D * D * 4, true);
     ENSURE(c->d_shadow_map, L * S * S * 4, false);

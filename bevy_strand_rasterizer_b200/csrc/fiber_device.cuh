@@ -88,7 +88,8 @@ struct FrameCounters {
     uint32_t tile_counter[8];     // virtual block ids of the look-back stages
     uint32_t visit_overflow;      // visit records unused this frame (did not fit, or disabled)
     unsigned long long visits;    // visit records appended by k_visit
-    uint32_t pad[2];
+    uint32_t small_cells;         // cells of 1..8 references listed for the cell sort
+    uint32_t large_cells;         // cells of more than 8 references listed for the cell sort
 };
 static_assert(sizeof(FrameCounters) == 160, "FrameCounters layout");
 

@@ -77,6 +77,8 @@ struct PrepassArgs {
     uint32_t* visit_rank;   // [ref_capacity] rank of the visit inside its cell
     unsigned long long* task_key;  // [task_capacity] canonical cell-order key of the task's reference
     uint32_t* task_mat;            // [task_capacity] material index of the task's reference
+    uint2* cells_small;            // (ref base, count) of cells with 1..8 references
+    uint2* cells_large;            // (ref base, count) of cells with more than 8
 };
 
 // Device buffers of the shadow, shading, raster and composite stages.

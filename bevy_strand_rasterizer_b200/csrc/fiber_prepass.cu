@@ -368,6 +368,10 @@ __global__ void __launch_bounds__(kFineThreads) k_fine(const FrameParams* __rest
 enum : int { kCount = 1, kFill = 2 };
 constexpr uint32_t kVisitThreads = 256;
 constexpr uint32_t kVisitSlots = 32;  // buffered visits per task; p99 is about 17 on the camera
+// Cell sort sizes: a thread sorts a cell of up to 8 references, a warp one of
+// up to 256 (32 lanes x 8 registers), a block anything longer.
+constexpr uint32_t kThreadSortMax = 8;
+constexpr uint32_t kWarpSortMax = 256;
 
 __device__ __forceinline__ uint32_t lut_slice(const fiber_coarse_depth_lut_entry* e, float z) {
     uint32_t zq = quantize_depth01(z);
@@ -784,7 +788,7 @@ __global__ void k_zero_pages(PrepassArgs A) {
 // ===========================================================================
 __global__ void __launch_bounds__(256) k_prefix_pages(const FrameParams* __restrict__ Pp, PrepassArgs A) {
     const FrameParams& P = *Pp;
-    __shared__ uint32_t s_tile, s_base;
+    __shared__ uint32_t s_tile, s_base, s_pbase, s_small, s_large;
     __shared__ uint32_t s_warp[33];
     __shared__ uint32_t s_counts[kPageSize];
     const uint32_t pages = *((volatile uint32_t*)&A.counters->pages);
@@ -814,9 +818,28 @@ __global__ void __launch_bounds__(256) k_prefix_pages(const FrameParams* __restr
             pm.flags = flags;
             A.page_meta[page] = pm;
             s_base = flags;
+            s_pbase = base;
             if (page == pages - 1u) A.counters->refs = base + total;
         }
         __syncthreads();
+        // List the page's non-empty cells for k_sort_cells (a page that lost its
+        // references lists none): up to 8 references in the small list, more in
+        // the large one. One scan carries both flags (small low, large high).
+        if (s_base == 0u) {
+            const uint32_t small = (c >= 1u && c <= kThreadSortMax) ? 1u : 0u;
+            const uint32_t large = c > kThreadSortMax ? 1u : 0u;
+            uint32_t both;
+            const uint32_t x = block_exclusive_scan<256>(small | (large << 16), s_warp, both);
+            if (threadIdx.x == 0) {
+                const uint32_t ns = both & 0xFFFFu, nl = both >> 16;
+                s_small = ns ? atomicAdd(&A.counters->small_cells, ns) : 0u;
+                s_large = nl ? atomicAdd(&A.counters->large_cells, nl) : 0u;
+            }
+            __syncthreads();
+            const uint32_t cb = s_pbase + excl;
+            if (small) A.cells_small[s_small + (x & 0xFFFFu)] = make_uint2(cb, c);
+            if (large) A.cells_large[s_large + (x >> 16)] = make_uint2(cb, c);
+        }
         if (threadIdx.x < 16u && s_base == 0u) {
             const uint32_t lt = threadIdx.x;
             bool has = false;
@@ -957,8 +980,6 @@ __device__ __forceinline__ void warp_sort_cell(const PrepassArgs& A, const Insta
     }
 }
 
-constexpr uint32_t kWarpSortMax = 256;  // 32 lanes x 8 registers
-constexpr uint32_t kThreadSortMax = 8;
 
 __device__ __forceinline__ void warp_sort_any(const PrepassArgs& A, const InstanceView* __restrict__ inst,
                                               uint32_t base, uint32_t n, int lane) {
@@ -1080,50 +1101,35 @@ __global__ void __launch_bounds__(256) k_emit(const FrameParams* __restrict__ Pp
 }
 
 // Canonical order inside every cell (projected depth key descending, then
-// instance, then segment), after the fill: one block per page, one warp per 32
-// cells; each warp sorts its cells of 2..256 references in registers and
-// queues longer cells for k_sort_big_cells. Warps never wait on each other.
+// instance, then segment), after the fill, over the cell lists k_prefix_pages
+// made: a thread per cell of up to 8 references (nearly all of them), then a
+// warp per larger cell. A cell longer than a warp sort is converted in place
+// by its warp and queued for k_sort_big_cells.
 __global__ void __launch_bounds__(256, 4) k_sort_cells(const InstanceView* __restrict__ inst, PrepassArgs A) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const uint32_t pages = *((volatile uint32_t*)&A.counters->pages);
-    for (uint32_t page = blockIdx.x; page < pages; page += gridDim.x) {
-        const fiber_fine_page_meta pm = A.page_meta[page];
-        if (pm.seg_ref_count == 0u || pm.flags != 0u) continue;
-        const uint32_t cell = (uint32_t)warp * 32u + (uint32_t)lane;
-        const size_t g = (size_t)page * kPageSize + cell;
-        const uint32_t cnt = A.counts[g];
-        const uint32_t base = pm.seg_ref_base + A.offsets[g];
-        // Cells of up to 8 (nearly all of them) sort in their own thread; the
-        // warp then takes the larger ones one at a time. A cell longer than a
-        // warp sort is converted in place by the warp and queued for
-        // k_sort_big_cells.
-        if (cnt == 1u) {
-            unsigned long long key;
-            uint32_t mat;
-            task_entry(A, inst, A.ref_keys[base], key, mat);
-            store_entry(A, base, key, mat);
-        } else if (cnt >= 2u && cnt <= kThreadSortMax) {
-            thread_sort_cell(A, inst, base, cnt);
-        }
-        unsigned todo = __ballot_sync(0xFFFFFFFFu, cnt > kThreadSortMax);
-        while (todo) {
-            const int src = __ffs(todo) - 1;
-            todo &= todo - 1u;
-            const uint32_t b = __shfl_sync(0xFFFFFFFFu, base, src);
-            const uint32_t n = __shfl_sync(0xFFFFFFFFu, cnt, src);
-            if (n <= kWarpSortMax) {
-                warp_sort_any(A, inst, b, n, lane);
-            } else {
-                for (uint32_t e = (uint32_t)lane; e < n; e += 32u) {
-                    unsigned long long key;
-                    uint32_t mat;
-                    task_entry(A, inst, A.ref_keys[b + e], key, mat);
-                    store_entry(A, b + e, key, mat);
-                }
-                if (lane == src) {
-                    const uint32_t slot = atomicAdd(&A.counters->big_cells, 1u);
-                    A.big_cells[slot] = make_uint2(b, n);
-                }
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t n_small = *((volatile uint32_t*)&A.counters->small_cells);
+    const uint32_t n_large = *((volatile uint32_t*)&A.counters->large_cells);
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n_small; i += stride) {
+        const uint2 e = A.cells_small[i];
+        thread_sort_cell(A, inst, e.x, e.y);
+    }
+    const uint32_t warps = stride >> 5;
+    for (uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < n_large; w += warps) {
+        const uint2 e = A.cells_large[w];
+        const uint32_t b = e.x, n = e.y;
+        if (n <= kWarpSortMax) {
+            warp_sort_any(A, inst, b, n, (int)lane);
+        } else {
+            for (uint32_t j = lane; j < n; j += 32u) {
+                unsigned long long key;
+                uint32_t mat;
+                task_entry(A, inst, A.ref_keys[b + j], key, mat);
+                store_entry(A, b + j, key, mat);
+            }
+            if (lane == 0u) {
+                const uint32_t slot = atomicAdd(&A.counters->big_cells, 1u);
+                A.big_cells[slot] = make_uint2(b, n);
             }
         }
     }
