@@ -82,6 +82,8 @@ __global__ void k_validate(InstanceView v, uint32_t* out) {
     atomicAdd(reinterpret_cast<unsigned long long*>(out + 2), segs);
 }
 
+constexpr int kGraphKeyWords = 12;  // what a captured frame graph depends on (fiber_frame_fused)
+
 }  // namespace
 
 struct fiber_ctx {
@@ -116,7 +118,7 @@ struct fiber_ctx {
     cudaStream_t last_stream = nullptr;
     // graph replay of fiber_frame_fused
     cudaGraphExec_t graph = nullptr;
-    uint64_t graph_key[8] = {0};
+    uint64_t graph_key[kGraphKeyWords] = {0};
     uint64_t buffer_generation = 0, graph_generation = ~0ull;
     FrameCounters h_counters{};
 };
@@ -830,12 +832,25 @@ fiber_status fiber_frame_fused(fiber_ctx* c, const fiber_image* scene_color, con
     }
     // Every kernel argument is stable across frames (per-frame values live in
     // the device FrameParams), so one captured graph serves every frame of the
-    // same shape and buffers.
-    uint64_t key[8] = {c->buffer_generation, (uint64_t)(composite ? 1 : 0),
-                       (uint64_t)(uintptr_t)(scene_color ? scene_color->ptr : nullptr),
-                       (uint64_t)(uintptr_t)(scene_depth ? scene_depth->ptr : nullptr),
-                       (uint64_t)(uintptr_t)(out ? out->ptr : nullptr), (uint64_t)(uintptr_t)s,
-                       (uint64_t)(composite ? scene_color->format : 0), (uint64_t)(composite ? out->format : 0)};
+    // same shape and buffers. The shape is whatever the host bakes into the
+    // launches: grid sizes (instances, coarse tiles), the shadow's shared
+    // memory (K) and whether it runs (lights), and the composite's image
+    // extents, pitches and formats.
+    auto pitch_of = [](const fiber_image* im) -> uint64_t {
+        return im ? ((uint64_t)im->pitch << 32) | (uint64_t)im->format : 0u;
+    };
+    uint64_t key[kGraphKeyWords] = {c->buffer_generation,
+                                    (uint64_t)(composite ? 1 : 0),
+                                    (uint64_t)(uintptr_t)(scene_color ? scene_color->ptr : nullptr),
+                                    (uint64_t)(uintptr_t)(scene_depth ? scene_depth->ptr : nullptr),
+                                    (uint64_t)(uintptr_t)(out ? out->ptr : nullptr),
+                                    (uint64_t)(uintptr_t)s,
+                                    composite ? pitch_of(scene_color) : 0u,
+                                    composite ? pitch_of(out) : 0u,
+                                    scene_depth ? pitch_of(scene_depth) : 0u,
+                                    ((uint64_t)c->P.width << 32) | c->P.height,
+                                    ((uint64_t)c->P.I << 32) | c->P.total_coarse_tiles,
+                                    ((uint64_t)c->P.K << 32) | c->P.L};
     bool reuse = c->graph && std::memcmp(key, c->graph_key, sizeof(key)) == 0;
     if (!reuse) {
         if (c->graph) {

@@ -8,6 +8,8 @@ colour, shading atlas and deep-shadow opacity must agree within max-abs 2e-3
 and PSNR >= 50 dB in FP32 (the DOM stages use no transcendental functions and
 are compared exactly).
 """
+import ctypes as C
+
 import numpy as np
 import pytest
 
@@ -111,6 +113,49 @@ def test_parity_ref_overflow():
     for what in (abi.DUMP_PAGE_META, abi.DUMP_COUNTS, abi.DUMP_ACTIVE_TILES, abi.DUMP_RUNS, abi.DUMP_WORK):
         _exact(plugin.dump(what), ref.get(what), what)
     plugin.close()
+
+
+def test_fused_graph_follows_frame_shape():
+    # One context replays its captured frame graph on a stream while the frame
+    # shape changes (resolution, light count) and the composite keeps writing
+    # into the same backing buffers. Every frame must match a fresh context
+    # that renders it with the plain node sequence.
+    import torch
+    from bevy_strand_rasterizer_b200.plugin import StrandRasterizerPlugin  # noqa: F401
+
+    stream = torch.cuda.Stream()
+    scene_buf = torch.empty((240 * 320 * 4,), dtype=torch.float16, device="cuda")
+    out_buf = torch.empty_like(scene_buf)
+
+    def images(w, h):
+        scene_buf.zero_()
+        scene_buf[: w * h * 4].view(h, w, 4)[...] = torch.tensor([0.1, 0.2, 0.3, 1.0], dtype=torch.float16)
+        out_buf.zero_()
+        torch.cuda.synchronize()
+        return (abi.Image(C.c_void_p(scene_buf.data_ptr()), w, h, w * 8, abi.FMT_RGBA16F),
+                abi.Image(C.c_void_p(out_buf.data_ptr()), w, h, w * 8, abi.FMT_RGBA16F))
+
+    shapes = [dict(width=320, height=240), dict(width=160, height=120),
+              dict(width=200, height=152, lights=[(1.0, 1.0, 1.0), (-1.0, 1.0, 0.5)]), dict(width=320, height=240)]
+    p = None
+    for kw in shapes:
+        scene = build_scene("tiny", settings_overrides={"history_enabled": 0, "fragment_counts_enabled": 1}, **kw)
+        w, h = kw["width"], kw["height"]
+        sc, out = images(w, h)
+        with torch.cuda.stream(stream):
+            p = run_gpu(scene, plugin=p, fused=True, stream=stream, scene_color=sc, out=out)
+        stream.synchronize()
+        got = out_buf[: w * h * 4].cpu().numpy().copy()
+        dumps = {what: p.dump(what).copy() for what in (abi.DUMP_COLOR, abi.DUMP_FRAGMENTS, abi.DUMP_DOM_OPACITY)}
+        sc, out = images(w, h)
+        fresh = run_gpu(scene, scene_color=sc, out=out)
+        torch.cuda.synchronize()
+        want = out_buf[: w * h * 4].cpu().numpy()
+        assert np.array_equal(got.view(np.uint16), want.view(np.uint16)), f"composite differs at {w}x{h}"
+        for what, v in dumps.items():
+            assert np.array_equal(v.view(np.uint8), fresh.dump(what).view(np.uint8)), f"{NAMES[what]} at {w}x{h}"
+        fresh.close()
+    p.close()
 
 
 def test_deterministic_repeat():
