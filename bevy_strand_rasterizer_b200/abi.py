@@ -106,6 +106,32 @@ class Stats(C.Structure):
         return out
 
 
+# Request server (fiber_server_*).
+SERVER_MAX_LIGHTS = 4
+
+
+class ServerConfig(C.Structure):
+    _fields_ = [("slots", u32), ("max_width", u32), ("max_height", u32), ("max_lights", u32), ("max_dom", u32),
+                ("pad", u32), ("hbm_budget", C.c_uint64)]
+
+
+class ServerScene(C.Structure):
+    _fields_ = [("vertices", C.c_void_p), ("n_vertices", u32), ("indices", C.c_void_p), ("n_indices", u32),
+                ("meta", C.c_void_p), ("n_meta", u32), ("geo", StrandGeo), ("materials", C.c_void_p),
+                ("n_materials", u32), ("world_from_local", f32 * 16)]
+
+
+class ServerRequest(C.Structure):
+    _fields_ = [("scene", u32), ("n_lights", u32), ("camera_cfg", FroxelConfigC), ("camera", Camera),
+                ("light_cfgs", FroxelConfigC * SERVER_MAX_LIGHTS), ("lights", Light * SERVER_MAX_LIGHTS),
+                ("scene_rgba16f", C.c_void_p), ("out_rgba16f", C.c_void_p), ("arrival_ns", C.c_uint64)]
+
+
+class ServerResult(C.Structure):
+    _fields_ = [("status", C.c_int), ("slot", u32), ("arrival_ns", C.c_uint64), ("admit_ns", C.c_uint64),
+                ("done_ns", C.c_uint64)]
+
+
 # numpy views of the task-contract structs (src/pipelines/task_contract.rs:45-135)
 BINNING_TASK = np.dtype([("id_info", "<u4"), ("chunk_id", "<u4"), ("seg_idx", "<u4"), ("packed_field", "<u4")])
 PROJECTED_SEGMENT = np.dtype([("p0_xy", "<u4"), ("p1_xy", "<u4"), ("depths", "<u4")])
@@ -139,7 +165,9 @@ EXPORTS = [
     "fiber_slab_alloc", "fiber_slab_upload", "fiber_slab_free", "fiber_instance_set", "fiber_frame_begin",
     "fiber_prepass", "fiber_shadows", "fiber_shading", "fiber_raster", "fiber_composite", "fiber_frame_fused",
     "fiber_render_host", "fiber_stats_get", "fiber_dump", "fiber_output_image", "fiber_span_count", "fiber_span_name",
-    "fiber_span_times", "fiber_status_string", "fiber_prefix_pages_noalloc",
+    "fiber_span_times", "fiber_status_string", "fiber_server_create", "fiber_server_add_scene",
+    "fiber_server_start", "fiber_server_submit", "fiber_server_wait", "fiber_server_destroy", "fiber_server_now_ns",
+    "fiber_prefix_pages_noalloc",
 ]
 
 _LIB = None
@@ -185,6 +213,13 @@ def load_library(path: Path | str | None = None) -> C.CDLL:
         "fiber_span_name": (C.c_char_p, [u32]),
         "fiber_span_times": (C.c_int, [vp, pp(f32), u32]),
         "fiber_status_string": (C.c_char_p, [C.c_int]),
+        "fiber_server_create": (C.c_int, [C.c_int, pp(Settings), pp(ServerConfig), pp(vp)]),
+        "fiber_server_add_scene": (C.c_int, [vp, pp(ServerScene), pp(u32)]),
+        "fiber_server_start": (C.c_int, [vp, pp(u32)]),
+        "fiber_server_submit": (C.c_int, [vp, pp(ServerRequest), pp(C.c_uint64)]),
+        "fiber_server_wait": (C.c_int, [vp, C.c_uint64, pp(ServerResult)]),
+        "fiber_server_destroy": (C.c_int, [vp]),
+        "fiber_server_now_ns": (C.c_uint64, []),
         "fiber_prefix_pages_noalloc": (C.c_int, [vp, u32, vp, vp, vp, vp]),
     }
     for name, (res, args) in sig.items():

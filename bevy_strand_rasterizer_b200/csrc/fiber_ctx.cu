@@ -9,11 +9,13 @@
 // reads its item count from device memory, so a whole frame is one stream of
 // launches that can be replayed from a CUDA graph.
 #include <algorithm>
+#include <cstddef>
 #include <cstdio>
 #include <cstring>
 #include <string>
 #include <vector>
 
+#include "fiber_internal.h"
 #include "fiber_kernels.cuh"
 
 using namespace fiber;
@@ -905,6 +907,86 @@ fiber_status fiber_render_host(fiber_ctx* c, const void* scene_host, const float
     FIBER_CUDA(cudaMemcpyAsync(out_host, c->d_host_scene.p, W * H * 8, cudaMemcpyDeviceToHost, s));
     return FIBER_OK;
 }
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Hooks for the request server (fiber_internal.h), C++ linkage.
+// ---------------------------------------------------------------------------
+struct fiber_scene_state {
+    std::vector<fiber_strand_instance> rows;
+    std::vector<InstanceView> views;
+    std::vector<uint64_t> inst_segments;
+    uint64_t total_segments = 0, total_points = 0, total_strands = 0;
+    uint32_t max_texels = 0, total_strand_count = 0, max_strand_count = 0;
+};
+
+fiber_scene_state* fiber_ctx_save_scene(const fiber_ctx* c) {
+    fiber_scene_state* s = new fiber_scene_state();
+    s->rows = c->rows;
+    s->views = c->views;
+    s->inst_segments = c->inst_segments;
+    s->total_segments = c->total_segments;
+    s->total_points = c->total_points;
+    s->total_strands = c->total_strands;
+    s->max_texels = c->max_texels;
+    s->total_strand_count = c->total_strand_count;
+    s->max_strand_count = c->max_strand_count;
+    return s;
+}
+
+void fiber_ctx_load_scene(fiber_ctx* c, const fiber_scene_state* s) {
+    c->rows = s->rows;
+    c->views = s->views;
+    c->inst_segments = s->inst_segments;
+    c->total_segments = s->total_segments;
+    c->total_points = s->total_points;
+    c->total_strands = s->total_strands;
+    c->max_texels = s->max_texels;
+    c->total_strand_count = s->total_strand_count;
+    c->max_strand_count = s->max_strand_count;
+    c->frame_ready = false;
+}
+
+void fiber_scene_state_free(fiber_scene_state* s) { delete s; }
+
+uint64_t fiber_scene_segments(const fiber_scene_state* s) { return s ? s->total_segments : 0u; }
+
+uint64_t fiber_ctx_allocated(const fiber_ctx* c) { return c ? c->allocated : 0u; }
+
+fiber_status fiber_ctx_frame_status(fiber_ctx* c, cudaStream_t s) {
+    if (!c) return FIBER_EINVAL;
+    uint32_t w[2] = {0u, 0u};  // overflow, error (adjacent words of FrameCounters)
+    static_assert(offsetof(FrameCounters, error) == offsetof(FrameCounters, overflow) + 4, "counter layout");
+    FIBER_CUDA(cudaMemcpyAsync(w, reinterpret_cast<const char*>(c->d_counters.p) + offsetof(FrameCounters, overflow),
+                               sizeof(w), cudaMemcpyDeviceToHost, s));
+    FIBER_CUDA(cudaStreamSynchronize(s));
+    if (w[1] != 0u) return FIBER_ETIMEDOUT;
+    if (w[0] != 0u) return FIBER_EOVERFLOW;
+    return FIBER_OK;
+}
+
+fiber_status fiber_ctx_render_host_nodes(fiber_ctx* c, const void* scene_host, void* out_host, cudaStream_t s) {
+    if (!c || !scene_host || !out_host) return FIBER_EINVAL;
+    if (!c->frame_ready) return FIBER_ENOTREADY;
+    const uint64_t W = c->P.width, H = c->P.height;
+    fiber_status e = ensure(c, c->d_host_scene, W * H * 8, false);
+    if (e != FIBER_OK) return e;
+    c->last_stream = s;
+    FIBER_CUDA(cudaMemcpyAsync(c->d_host_scene.p, scene_host, W * H * 8, cudaMemcpyHostToDevice, s));
+    fiber_image scene{c->d_host_scene.p, (uint32_t)W, (uint32_t)H, (uint32_t)(W * 8), FIBER_FMT_RGBA16F};
+    fiber_status st = run_prepass(c, s);
+    if (st == FIBER_OK) st = run_shadows(c, s);
+    if (st == FIBER_OK) st = run_shading(c, s);
+    if (st == FIBER_OK) st = run_raster(c, s);
+    if (st == FIBER_OK) st = run_composite(c, &scene, nullptr, &scene, s);
+    record(c, 13, s);
+    if (st != FIBER_OK) return st;
+    FIBER_CUDA(cudaMemcpyAsync(out_host, c->d_host_scene.p, W * H * 8, cudaMemcpyDeviceToHost, s));
+    return FIBER_OK;
+}
+
+extern "C" {
 
 fiber_status fiber_stats_get(fiber_ctx* c, fiber_stats* out) {
     if (!c || !out) return FIBER_EINVAL;

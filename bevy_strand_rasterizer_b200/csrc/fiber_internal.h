@@ -1,0 +1,31 @@
+// fiber_internal.h — hooks between the context runtime (fiber_ctx.cu) and the
+// request server (fiber_server.cu). Library-internal: not part of the C ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "fiber.h"
+
+// A context's instance table with everything fiber_instance_set derives from
+// it (validated device views, segment totals). Saving one per resident scene
+// lets a context switch scenes between frames on the host alone: no
+// validation kernel, no device synchronisation.
+struct fiber_scene_state;
+
+fiber_scene_state* fiber_ctx_save_scene(const fiber_ctx* c);
+void fiber_ctx_load_scene(fiber_ctx* c, const fiber_scene_state* s);
+void fiber_scene_state_free(fiber_scene_state* s);
+uint64_t fiber_scene_segments(const fiber_scene_state* s);
+
+// fiber_render_host with the node sequence launched directly on `s` (no graph
+// capture), for callers whose frame shape changes from frame to frame.
+fiber_status fiber_ctx_render_host_nodes(fiber_ctx* c, const void* scene_host, void* out_host, cudaStream_t s);
+
+// Device bytes the context holds.
+uint64_t fiber_ctx_allocated(const fiber_ctx* c);
+
+// After the frame on `s` completed: ETIMEDOUT if a bounded device wait gave
+// up, EOVERFLOW if a queue dropped work, else OK. Reads two counter words.
+fiber_status fiber_ctx_frame_status(fiber_ctx* c, cudaStream_t s);

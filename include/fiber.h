@@ -385,6 +385,81 @@ fiber_status fiber_span_times(fiber_ctx* ctx, float* ms, uint32_t n);
 const char* fiber_status_string(fiber_status s);
 
 /* ------------------------------------------------------------------------ */
+/* Request server: continuous batching of render requests over resident      */
+/* scenes. No counterpart in the reference (a Bevy app renders one frame per */
+/* view per tick); it is the served mode of the path's specification.        */
+/* ------------------------------------------------------------------------ */
+typedef struct fiber_server fiber_server;
+
+typedef struct fiber_server_config {
+    uint32_t slots;        /* frames in flight at once (each slot is a context with
+                              its own stream and worker thread); 0 = as many as the
+                              HBM budget admits, at most 8                         */
+    uint32_t max_width;    /* largest request resolution; every slot is sized   */
+    uint32_t max_height;   /* for it at fiber_server_start                      */
+    uint32_t max_lights;   /* most lights of one request (<= 4)                 */
+    uint32_t max_dom;      /* largest deep-shadow map side of one request       */
+    uint32_t pad;
+    uint64_t hbm_budget;   /* device bytes all slots may hold (0 = no cap)      */
+} fiber_server_config;
+
+/* One resident scene: a strand instance in the reference's slab format
+ * (pack_strands / pack_indexed_strands, src/plugin.rs:1315-1393), host memory. */
+typedef struct fiber_server_scene {
+    const float* vertices;           /* float4 per point (w = 1)          */
+    uint32_t n_vertices;
+    const uint32_t* indices;         /* u32 per point                     */
+    uint32_t n_indices;
+    const fiber_strand_meta* meta;   /* per strand                        */
+    uint32_t n_meta;
+    fiber_strand_geo geo;
+    const fiber_strand_material* materials;
+    uint32_t n_materials;
+    float world_from_local[16];      /* column-major                      */
+} fiber_server_scene;
+
+#define FIBER_SERVER_MAX_LIGHTS 4
+typedef struct fiber_server_request {
+    uint32_t scene;                  /* id from fiber_server_add_scene    */
+    uint32_t n_lights;
+    fiber_froxel_config camera_cfg;
+    fiber_camera camera;
+    fiber_froxel_config light_cfgs[FIBER_SERVER_MAX_LIGHTS];
+    fiber_light lights[FIBER_SERVER_MAX_LIGHTS];
+    const void* scene_rgba16f;       /* host W x H RGBA16F under the strands, or NULL (transparent) */
+    void* out_rgba16f;               /* host W x H RGBA16F result, written before the ticket completes */
+    uint64_t arrival_ns;             /* arrival on fiber_server_now_ns's clock; 0 = at submit */
+} fiber_server_request;
+
+typedef struct fiber_server_result {
+    fiber_status status;
+    uint32_t slot;                   /* slot that rendered it             */
+    uint64_t arrival_ns, admit_ns, done_ns;  /* fiber_server_now_ns clock  */
+} fiber_server_result;
+
+/* Creates a server on `device`; `settings` apply to every slot except that the
+ * temporal shadow history is off, so a request's image does not depend on
+ * which requests ran before it on the same slot. */
+fiber_status fiber_server_create(int device, const fiber_settings* settings, const fiber_server_config* cfg,
+                                 fiber_server** out);
+/* Uploads a scene to every slot (before fiber_server_start). */
+fiber_status fiber_server_add_scene(fiber_server* srv, const fiber_server_scene* scene, uint32_t* scene_id);
+/* Sizes every slot for the largest scene at the configured maximum frame,
+ * settles the slot count under the HBM budget and starts the workers. */
+fiber_status fiber_server_start(fiber_server* srv, uint32_t* slots_started);
+/* Queues a request; a free slot admits it at once, otherwise the first slot to
+ * finish does (arrival order). Requests beyond the configured maximum shape
+ * return FIBER_EINVAL. The request and its host buffers must stay valid until
+ * its ticket completes. */
+fiber_status fiber_server_submit(fiber_server* srv, const fiber_server_request* req, uint64_t* ticket);
+/* Blocks until `ticket` completes. */
+fiber_status fiber_server_wait(fiber_server* srv, uint64_t ticket, fiber_server_result* out);
+/* Finishes queued requests, stops the workers and frees every slot. */
+fiber_status fiber_server_destroy(fiber_server* srv);
+/* The server's steady clock in nanoseconds. */
+uint64_t fiber_server_now_ns(void);
+
+/* ------------------------------------------------------------------------ */
 /* Page prefix without device allocation (no counterpart in the reference)   */
 /* ------------------------------------------------------------------------ */
 /* The froxel-page prefix of fiber_prepass as a standalone call for callers

@@ -13,7 +13,7 @@ HEADER = Path(__file__).resolve().parents[1] / "include" / "fiber.h"
 
 def header_functions():
     text = HEADER.read_text()
-    return sorted(set(re.findall(r"^\s*(?:fiber_status|uint32_t|const char\*)\s+(fiber_\w+)\(", text, re.M)))
+    return sorted(set(re.findall(r"^\s*(?:fiber_status|uint32_t|uint64_t|const char\*)\s+(fiber_\w+)\(", text, re.M)))
 
 
 def test_exports_every_declared_symbol():
@@ -28,6 +28,7 @@ def test_exports_every_declared_symbol():
 @pytest.mark.parametrize("ctype,size", [
     (abi.DevicePtr, 12), (abi.Aabb, 32), (abi.StrandGeo, 64), (abi.StrandMaterialC, 64),
     (abi.StrandInstance, 160), (abi.FroxelConfigC, 20), (abi.Camera, 80), (abi.Light, 96), (abi.Image, 24),
+    (abi.ServerConfig, 32), (abi.ServerScene, 192), (abi.ServerRequest, 600), (abi.ServerResult, 32),
 ])
 def test_struct_sizes(ctype, size):
     assert C.sizeof(ctype) == size
