@@ -47,6 +47,10 @@ def parse_args():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--profile", action="store_true",
                    help="render warmup + steps frames only (no timing extras); the command profiled under ncu")
+    p.add_argument("--no-served", action="store_true", help="skip the served-mode measurement")
+    p.add_argument("--served-rate", type=float, default=200.0, help="Poisson arrival rate, requests/s")
+    p.add_argument("--served-seconds", type=float, default=5.0, help="length of the arrival stream")
+    p.add_argument("--served-saturate", type=int, default=256, help="requests submitted at once for throughput")
     return p.parse_args()
 
 
@@ -435,11 +439,67 @@ def fiber_arm(args):
                        "camera_runs": st.camera_runs, "shadow_runs": st.shadow_runs},
         }
     plugin.close()
+    if line is not None and world == 1 and not args.no_served:
+        line["served"] = served_section(args)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
     if line is not None:
         print(json.dumps(line), flush=True)
+
+
+SERVED_BUDGET = 150 * 10**9  # bytes of HBM the served configuration may hold
+
+
+def served_section(args) -> dict:
+    """The served configuration: 8 resident scenes (5k-500k strands), a seeded
+    Poisson stream of requests of mixed scenes, resolutions (256^2 to 1080p)
+    and shadow-map sizes. The server admits requests into as many slots as the
+    HBM budget holds and overlaps them on the GPU; the plain per-request loop
+    is the same server with one slot (each request runs alone, in arrival
+    order). Latency is arrival to image in pinned host memory. A second pass
+    submits a batch at once to measure throughput when every slot is busy."""
+    import torch
+
+    from bevy_strand_rasterizer_b200 import served
+    from bevy_strand_rasterizer_b200.server import FiberServer
+
+    t = time.time()
+    scenes = served.served_scenes()
+    gen_s = time.time() - t
+    outputs = {(w, h): torch.empty((h, w, 4), dtype=torch.float16, pin_memory=True) for (w, h) in served.RESOLUTIONS}
+    n_stream = max(1, int(args.served_rate * args.served_seconds))
+    arrivals, reqs = served.request_stream(n_stream, args.served_rate, scenes, seed=7)
+    _, batch = served.request_stream(args.served_saturate, 0.0, scenes, seed=8)
+    _, warm = served.request_stream(32, 0.0, scenes, seed=9)
+    result = {"scenes": [int(s.strand_count) for s in scenes], "points_per_strand": served.SCENE_POINTS,
+              "resolutions": [f"{w}x{h}" for w, h in served.RESOLUTIONS], "dom_sizes": list(served.DOM_SIZES),
+              "offered_rps": args.served_rate, "stream_s": args.served_seconds, "hbm_budget": SERVED_BUDGET,
+              "scene_gen_s": gen_s}
+    # The plain loop runs first: its batch throughput sets the second, sustainable
+    # arrival rate (80 % of what one request at a time can serve), at which
+    # latency is service time rather than queue growth.
+    sustain = None
+    for label, slots in (("plain", 1), ("served", 0)):
+        t = time.time()
+        srv = FiberServer(slots=slots, max_width=1920, max_height=1080, max_lights=1, max_dom=2048,
+                          hbm_budget=SERVED_BUDGET)
+        ids = [srv.add_scene(p) for p in scenes]
+        n = srv.start()
+        setup_s = time.time() - t
+        served.replay(srv, ids, np.zeros(len(warm)), warm, outputs)
+        sat = served.replay(srv, ids, np.zeros(len(batch)), batch, outputs)
+        if sustain is None:
+            rate = 0.8 * sat["frames_per_s"]
+            sustain = (rate,) + served.request_stream(max(1, int(rate * args.served_seconds)), rate, scenes, seed=10)
+        stream = served.replay(srv, ids, arrivals, reqs, outputs)
+        stream_s = served.replay(srv, ids, sustain[1], sustain[2], outputs)
+        srv.close()
+        result[label] = {"slots": n, "setup_s": setup_s, "batch": sat, "stream": stream,
+                         "stream_sustainable": stream_s}
+    result["sustainable_rps"] = sustain[0]
+    result["frames_per_s_ratio"] = result["served"]["batch"]["frames_per_s"] / result["plain"]["batch"]["frames_per_s"]
+    return result
 
 
 def main():

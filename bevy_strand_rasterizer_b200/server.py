@@ -94,11 +94,14 @@ class FiberServer:
         self._keep[int(t.value)] = (r, out, scene_rgba16f)
         return int(t.value)
 
-    def wait(self, ticket: int) -> abi.ServerResult:
+    def wait(self, ticket: int, allow_overflow: bool = True) -> abi.ServerResult:
+        """Result of a request. EOVERFLOW (a capacity-sized queue dropped work,
+        flagged exactly as the reference flags it; the image was still written)
+        is returned, not raised, unless allow_overflow is False."""
         res = abi.ServerResult()
         abi.check(self.lib.fiber_server_wait(self.srv, ticket, C.byref(res)), "fiber_server_wait")
         self._keep.pop(ticket, None)
-        abi.check(res.status, f"request {ticket}")
+        abi.check(res.status, f"request {ticket}", (abi.OK, abi.EOVERFLOW) if allow_overflow else (abi.OK,))
         return res
 
     def close(self):
