@@ -142,12 +142,15 @@ def algorithmic_bytes(st, w, n_lights: int, K: int, D: int) -> dict:
 
     Per unit: 20 B / point + 16 B / strand (vertex float4 + index, meta), 28 B per
     binning task written and read (BinningTask 16 + ProjectedSegment 12), 8 B per
-    allocated cell (count + offset), 24 B per fine ref (written + read), 32 B per
-    visit record (k_visit writes slot/cell + task, k_count_visits reads 4 and
-    writes cell + rank, k_fill_visits reads 12), 64 B per work item / tile run
-    (written + read), 40 B per ref of endpoint gather in the rasters, 40 + 8 L B
-    per camera segment in shading, 12 B per camera pixel (RGBA16F + R32F),
-    4 (K + 1) B per deep-opacity texel. Visits are counted as fine refs.
+    allocated cell (count + offset), 24 B per fine ref (written + read), 12 B per
+    binning task of cell-order key + material (written by k_visit), per visit
+    (counted as fine refs): 8 B record written by k_visit, 16 B read/written by
+    k_count_visits (record, rank, count), 20 B by k_fill_visits (record, rank,
+    task, offset read; task index written), 32 B by k_sort_cells (task index,
+    12 B key + material gathered, 16 B reference + key written); 64 B per work
+    item / tile run (written + read), 40 B per ref of endpoint gather in the
+    rasters, 40 + 8 L B per camera segment in shading, 12 B per camera pixel
+    (RGBA16F + R32F), 4 (K + 1) B per deep-opacity texel.
     """
     F = st.frustum_count
     P, S = st.total_points, st.total_strands
@@ -160,16 +163,18 @@ def algorithmic_bytes(st, w, n_lights: int, K: int, D: int) -> dict:
     dom = n_lights * 4 * (K + 1) * D * D
     per = {
         "k_fine": 20 * P + 16 * S + sum(28 * n for n in tasks),
-        "k_visit": sum(28 * n for n in tasks) + sum(8 * r for r in refs),
+        "k_visit": sum(40 * n for n in tasks) + sum(8 * r for r in refs),
         "k_count_visits": sum(16 * r for r in refs),
-        "k_fill_visits": sum((12 + 4 + 20 + 16) * r for r in refs),
+        "k_fill_visits": sum(20 * r for r in refs),
         "k_prefix_pages": sum(8 * 256 * p for p in pages),
-        "k_emit": sum(32 * (wk + t) for wk, t in zip(work, runs)),
+        "k_emit+k_sort_cells": sum(32 * (wk + t) + 32 * r for wk, t, r in zip(work, runs, refs)),
         "k_shadow": sum(52 * refs[f] + 32 * (work[f] + runs[f]) for f in range(1, F)) + dom,
         "k_shade": st.camera_tasks * (40 + 8 * n_lights),
         "k_raster": 52 * refs[0] + 32 * (work[0] + runs[0]) + 12 * WH,
     }
-    total = (20 * P + 16 * S + sum(56 * n + 8 * 256 * p + 24 * r + 32 * r + 64 * (wk + t) + 40 * r
+    # The frame's B_alg is the path's own formula (fixed before any kernel was
+    # written); the per-kernel figures above add this implementation's records.
+    total = (20 * P + 16 * S + sum(56 * n + 8 * 256 * p + 24 * r + 64 * (wk + t) + 40 * r
                                    for n, p, r, wk, t in zip(tasks, pages, refs, work, runs))
              + st.camera_tasks * (40 + 8 * n_lights) + 12 * WH + dom)
     b_min = 20 * P + 16 * S + 12 * WH + dom
@@ -189,7 +194,7 @@ SPAN_TO_KERNEL = {
     "strand_prepass/binning": "k_count_visits",
     "strand_prepass/prefix_fine_pages": "k_prefix_pages",
     "strand_prepass/fill_segment_refs": "k_fill_visits",
-    "strand_prepass/emit_raster_work": "k_emit",
+    "strand_prepass/emit_raster_work": "k_emit+k_sort_cells",
     "strand_shadow_rasterizer/rasterize": "k_shadow",
     "strand_shading/shade": "k_shade",
     "strand_rasterizer/rasterize": "k_raster",
@@ -282,7 +287,7 @@ def reference_arm(args):
 def fiber_arm(args):
     import torch
     import torch.distributed as dist
-    from bevy_strand_rasterizer_b200 import abi
+    from bevy_strand_rasterizer_b200 import abi, replicas
     from bevy_strand_rasterizer_b200.plugin import StrandRasterizerPlugin, image_from_tensor
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -294,7 +299,7 @@ def fiber_arm(args):
         dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
 
     w, packed, material, cam_cfg, lights = make_scene(args.workload)
-    plugin = StrandRasterizerPlugin(device=local, dom_slices=w.dom_layers)
+    plugin = StrandRasterizerPlugin(device=local, dom_slices=w.dom_layers, ref_capacity_factor=w.ref_capacity_factor)
     plugin.add_geometry(packed, material)
     stream = torch.cuda.Stream()
     H, W = w.height, w.width
@@ -304,10 +309,9 @@ def fiber_arm(args):
     scene_img = image_from_tensor(scene, abi.FMT_RGBA16F)
     out_img = image_from_tensor(out, abi.FMT_RGBA16F)
     light_cfgs = [c for c, _ in lights]
-    frame_base = rank * 100_003  # each replica renders its own orbit frames
 
     def step(k):
-        cam, lc = frame_structs(w, packed, frame_base + k, lights)
+        cam, lc = frame_structs(w, packed, replicas.frame_index(rank, k), lights)
         plugin.frame_begin_raw(cam_cfg, cam, light_cfgs, lc, stream)
         # The scene is opaque (alpha 1), so the blend onto `out` does not
         # depend on what `out` held before.
@@ -341,14 +345,11 @@ def fiber_arm(args):
     stream.synchronize()
     torch.cuda.synchronize()
     clk = clocks.stop()
-    elapsed = e0.elapsed_time(e1)
+    elapsed = replicas.max_over_ranks(e0.elapsed_time(e1), device="cuda")
     if world > 1:
-        t = torch.tensor([elapsed], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed = float(t.item())
         dist.barrier()
     segs = st.total_segments
-    value = segs * args.steps * world / (elapsed / 1000.0)
+    value = replicas.job_rate(segs * args.steps, world, elapsed / 1000.0)
     ms_per_step = elapsed / args.steps
 
     # Per-stage device times (events recorded inside the frame graph).
@@ -371,7 +372,7 @@ def fiber_arm(args):
     sh = C.c_void_p(stream.cuda_stream)
     with torch.cuda.stream(stream):
         for k in range(max(1, args.warmup)):
-            cam, lc = frame_structs(w, packed, frame_base + k, lights)
+            cam, lc = frame_structs(w, packed, replicas.frame_index(rank, k), lights)
             plugin.frame_begin_raw(cam_cfg, cam, light_cfgs, lc, stream)
             abi.check(lib.fiber_render_host(plugin.ctx, C.c_void_p(host_in.data_ptr()), None,
                                             C.c_void_p(host_out.data_ptr()), sh), "fiber_render_host")
@@ -379,18 +380,14 @@ def fiber_arm(args):
         e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e2.record(stream)
         for k in range(args.steps):
-            cam, lc = frame_structs(w, packed, frame_base + k, lights)
+            cam, lc = frame_structs(w, packed, replicas.frame_index(rank, k), lights)
             plugin.frame_begin_raw(cam_cfg, cam, light_cfgs, lc, stream)
             abi.check(lib.fiber_render_host(plugin.ctx, C.c_void_p(host_in.data_ptr()), None,
                                             C.c_void_p(host_out.data_ptr()), sh), "fiber_render_host")
         e3.record(stream)
     stream.synchronize()
-    e2e_ms = e2.elapsed_time(e3)
-    if world > 1:
-        t = torch.tensor([e2e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e_value = segs * args.steps * world / (e2e_ms / 1000.0)
+    e2e_ms = replicas.max_over_ranks(e2.elapsed_time(e3), device="cuda")
+    e2e_value = replicas.job_rate(segs * args.steps, world, e2e_ms / 1000.0)
     assert np.isfinite(host_out.float().numpy()).all()
 
     # Roofline of the dominant kernel (HBM-bound dataflow; no dense contraction).
@@ -421,7 +418,7 @@ def fiber_arm(args):
                                    f"{len(lights)} light(s) with {w.dom_size}^2 x {w.dom_layers} deep-opacity maps",
                        "tile_px": w.froxel, "parallelism": f"replicas x{world}",
                        "l2": "per-frame working set (tasks, refs, pages, DOM) > 126 MB L2",
-                       "stochastic_cull": "on (reference default)"},
+                       "stochastic_cull": "on (reference default)", "ref_capacity_factor": w.ref_capacity_factor},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "entry_point": "fiber_render_host", "ms_per_step": e2e_ms / args.steps},
             "roofline": {"bound": "hbm", "kernel": dom_kernel, "achieved": achieved, "peak": peak,

@@ -199,6 +199,9 @@ class Workload:
     depth_slices: int = 64
     froxel: int = 8
     orbit_frames: int = 200
+    # Fine-reference capacity = factor x binning capacity (the reference's default is 4).
+    # At 4K a curly scene's segments cross more cells than that holds.
+    ref_capacity_factor: int = 4
 
     def camera(self, frame: int = 0) -> CameraSpec:
         theta = 2.0 * math.pi * (frame % self.orbit_frames) / self.orbit_frames
@@ -220,5 +223,6 @@ def workload(name: str) -> Workload:
     if name == "medium":
         return Workload("medium", 100_000, 32, 1920, 1080, 2048, 8, [l1], seed=12, depth_slices=64)
     if name == "large":
-        return Workload("large", 500_000, 32, 3840, 2160, 4096, 8, [l1, l2], curly=True, seed=13, depth_slices=64)
+        return Workload("large", 500_000, 32, 3840, 2160, 4096, 8, [l1, l2], curly=True, seed=13, depth_slices=64,
+                        ref_capacity_factor=8)
     raise KeyError(name)
