@@ -73,7 +73,7 @@ __device__ __forceinline__ void slot_source(const uint32_t* s_prefix, const Roun
 // ===========================================================================
 // K16 deep-opacity shadow raster + K17 stampback.
 // ===========================================================================
-constexpr uint32_t kShadowCap = 1024;
+constexpr uint32_t kShadowCap = 768;
 constexpr uint32_t kShadowWords = kShadowCap / 32;
 constexpr int kMaxDomSlices = 16;
 
@@ -131,7 +131,7 @@ __device__ __forceinline__ bool band_candidate(const Band& B, float px, float py
     return !(fabsf(d) > B.thr) && !(s < B.slo) && !(s > B.shi);
 }
 
-__global__ void __launch_bounds__(256, 3) k_shadow(const FrameParams* __restrict__ Pp,
+__global__ void __launch_bounds__(256, 4) k_shadow(const FrameParams* __restrict__ Pp,
                                                 const InstanceView* __restrict__ inst, RenderArgs R) {
     const FrameParams& P = *Pp;
     extern __shared__ float s_dyn[];
@@ -413,7 +413,7 @@ constexpr uint16_t kEntryInvalid = 0x8000u;
 // redundantly, so they stay in step for the group blend. A group without a
 // candidate contributes transparent black and depth 0 in every lane, which
 // leaves the blend unchanged, so skipping it keeps the result.
-__global__ void __launch_bounds__(256, 3) k_raster(const FrameParams* __restrict__ Pp,
+__global__ void __launch_bounds__(256, 4) k_raster(const FrameParams* __restrict__ Pp,
                                                 const InstanceView* __restrict__ inst, RenderArgs R) {
     const FrameParams& P = *Pp;
     // Per staged entry: 64 B of projection, radii and shading texels, the run
@@ -647,11 +647,11 @@ void launch_shadow(const LaunchCtx& L, const RenderArgs& R, uint32_t K) {
         cudaFuncSetAttribute(k_shadow, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_bytes);
         if (dev >= 0 && dev < 64) configured[dev] = true;
     }
-    k_shadow<<<L.sm_count * 3, 256, shadow_smem_bytes(K), L.stream>>>(L.P, L.inst, R);
+    k_shadow<<<L.sm_count * 4, 256, shadow_smem_bytes(K), L.stream>>>(L.P, L.inst, R);
 }
 
 void launch_raster(const LaunchCtx& L, const RenderArgs& R) {
-    k_raster<<<L.sm_count * 3, 256, 0, L.stream>>>(L.P, L.inst, R);
+    k_raster<<<L.sm_count * 4, 256, 0, L.stream>>>(L.P, L.inst, R);
 }
 
 }  // namespace fiber
