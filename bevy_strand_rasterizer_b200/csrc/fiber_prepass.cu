@@ -610,7 +610,7 @@ __device__ __forceinline__ bool visits_unused(const PrepassArgs& A) {
 // the rest. When the records do not fit (or slots exceed 24 bits) the pass
 // still marks every page and raises visit_overflow, which hands count and fill
 // to the walking kernels.
-__global__ void __launch_bounds__(kVisitThreads, 3) k_visit(const FrameParams* __restrict__ Pp,
+__global__ void __launch_bounds__(kVisitThreads, 4) k_visit(const FrameParams* __restrict__ Pp,
                                                             const InstanceView* __restrict__ inst, PrepassArgs A) {
     const FrameParams& P = *Pp;
     __shared__ uint32_t s_buf[kVisitSlots * kVisitThreads];
