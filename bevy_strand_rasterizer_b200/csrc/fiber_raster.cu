@@ -403,18 +403,22 @@ __global__ void __launch_bounds__(256, 4) k_shadow(const FrameParams* __restrict
 
 // ===========================================================================
 // K19 camera colour raster.
+//
+// One 64-thread block per camera tile run, one thread per pixel. Each pixel
+// walks, in order, the groups of 4 (an item's entries 4g .. 4g+3 from the item
+// start) that hold a coverage candidate for it, and blends each group as the
+// reference's four workers do: (w0 over w1) over (w2 over w3), then final over
+// group, the same float operations in the same order, computed in one thread.
+// A group without a candidate contributes transparent black and depth 0,
+// which leaves the blend unchanged, so skipping it keeps the result.
 // ===========================================================================
-constexpr uint32_t kCamCap = 512;
+constexpr uint32_t kCamThreads = 64;  // = kPixelSlots
+constexpr uint32_t kCamCap = 128;
 constexpr uint32_t kCamWords = kCamCap / 32;
 constexpr uint16_t kEntryInvalid = 0x8000u;
 
-// One pixel's walk over the groups of 4 (an item's entries 4g .. 4g+3 from
-// the item start) that hold a candidate: the pixel's 4 lanes run it
-// redundantly, so they stay in step for the group blend. A group without a
-// candidate contributes transparent black and depth 0 in every lane, which
-// leaves the blend unchanged, so skipping it keeps the result.
-__global__ void __launch_bounds__(256, 4) k_raster(const FrameParams* __restrict__ Pp,
-                                                const InstanceView* __restrict__ inst, RenderArgs R) {
+__global__ void __launch_bounds__(kCamThreads) k_raster(const FrameParams* __restrict__ Pp,
+                                                        const InstanceView* __restrict__ inst, RenderArgs R) {
     const FrameParams& P = *Pp;
     // Per staged entry: 64 B of projection, radii and shading texels, the run
     // item and position in it (bit 15: behind the camera, never a candidate).
@@ -427,14 +431,13 @@ __global__ void __launch_bounds__(256, 4) k_raster(const FrameParams* __restrict
     __shared__ float2 s_pix[kPixelSlots];
     __shared__ uint32_t s_wbase[kMaxRunItems], s_wcount[kMaxRunItems], s_prefix[kMaxRunItems + 1];
     __shared__ RoundPlan s_plan;
-    __shared__ uint32_t s_more;
+    __shared__ uint32_t s_more, s_run;
 
     const uint32_t n_runs = *((volatile uint32_t*)&R.counters->camera_active);
-    const uint32_t slot = threadIdx.x >> 2, worker = threadIdx.x & 3u;
-    const uint32_t lane = threadIdx.x & 31u, wbase = lane & ~3u, warp = threadIdx.x >> 5;
+    const uint32_t slot = threadIdx.x;
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     const uint32_t cap = P.atlas_cap;
     const __half* hist = R.history[(P.hist_in & 1u) ^ 1u];
-    __shared__ uint32_t s_run;
     // Blocks claim runs from a counter, so long runs do not pile up on one block.
     for (;;) {
         __syncthreads();
@@ -461,7 +464,7 @@ __global__ void __launch_bounds__(256, 4) k_raster(const FrameParams* __restrict
             s_wbase[i] = wi.seg_ref_base;
             s_wcount[i] = wi.seg_ref_count;
         }
-        if (worker == 0u) s_pix[slot] = make_float2(pcx, pcy);
+        s_pix[slot] = make_float2(pcx, pcy);
         __syncthreads();
         float4 fin = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         float gdepth = 0.0f;
@@ -469,14 +472,13 @@ __global__ void __launch_bounds__(256, 4) k_raster(const FrameParams* __restrict
         uint32_t frags = 0;
         uint32_t pending = kInvalid;  // last item blended into, whose end test is still due
         uint32_t cur_item = 0u, cur_off = 0u;
-        // Early out (alpha > 0.98) at the end of an item; worker 0 holds the blend.
-        auto end_of_item = [&](bool due) {
-            if (due && worker == 0u && !done && fin.w > 0.98f) {
+        // Early out (alpha > 0.98) at the end of an item.
+        auto end_of_item = [&]() {
+            if (!done && fin.w > 0.98f) {
                 fin = make_float4(fin.x / fin.w, fin.y / fin.w, fin.z / fin.w, 1.0f);
                 done = true;
             }
-            done = __shfl_sync(0xFFFFFFFFu, done, wbase);
-            if (due) pending = kInvalid;
+            pending = kInvalid;
         };
         for (;;) {
             if (threadIdx.x == 0) {
@@ -538,95 +540,69 @@ __global__ void __launch_bounds__(256, 4) k_raster(const FrameParams* __restrict
                 s_pmask[q * kPixelSlots + lane + 32u] = hi;
             }
             __syncthreads();
-            uint32_t pos = 0u;         // next entry of this pixel's walk
-            bool exhausted = done;
-            while (!__all_sync(0xFFFFFFFFu, exhausted)) {
-                bool act = !exhausted;
-                uint32_t c = kInvalid;
-                if (act) {
-                    // first candidate entry >= pos
-                    uint32_t q = pos >> 5;
-                    uint32_t m = q < nq ? (s_pmask[q * kPixelSlots + slot] & (0xFFFFFFFFu << (pos & 31u))) : 0u;
-                    while (m == 0u && q + 1u < nq) m = s_pmask[(++q) * kPixelSlots + slot];
-                    if (m != 0u) c = q * 32u + (uint32_t)(__ffs(m) - 1);
-                    else { exhausted = true; act = false; }
+            uint32_t pos = 0u;  // next entry of this pixel's walk
+            while (!done) {
+                // first candidate entry >= pos
+                uint32_t q = pos >> 5;
+                uint32_t m = q < nq ? (s_pmask[q * kPixelSlots + slot] & (0xFFFFFFFFu << (pos & 31u))) : 0u;
+                while (m == 0u && q + 1u < nq) m = s_pmask[(++q) * kPixelSlots + slot];
+                if (m == 0u) break;
+                const uint32_t c = q * 32u + (uint32_t)(__ffs(m) - 1);
+                const uint32_t item = (uint32_t)((s_item[c] >> 2) & 0x3FFu);
+                if (pending != kInvalid && item > pending) {
+                    end_of_item();
+                    if (done) break;
                 }
-                const uint32_t item = act ? (uint32_t)((s_item[c] >> 2) & 0x3FFu) : 0u;
-                end_of_item(act && pending != kInvalid && item > pending);
-                if (done) { exhausted = true; act = false; }
-                float4 part = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-                float pd = 0.0f;
-                if (act) {
-                    const uint32_t lead = c - (s_item[c] & 3u);
-                    const uint32_t end = min(lead + 4u, s_prefix[item - rp.lo + 1u]);
-                    const uint32_t bi = lead + worker;
-                    pos = end;
-                    pending = item;
-                    if (bi < end && ((s_pmask[(bi >> 5) * kPixelSlots + slot] >> (bi & 31u)) & 1u)) {
-                        const float ax = sp0x[bi], ay = sp0y[bi], bx = sp1x[bi], by = sp1y[bi];
-                        const float rmax = srmax[bi];
-                        if (!(pcx < wmin(ax, bx) - rmax || pcy < wmin(ay, by) - rmax) &&
-                            !(pcx > wmax(ax, bx) + rmax || pcy > wmax(ay, by) + rmax)) {
-                            const float abx = bx - ax, aby = by - ay;
-                            float t = ((pcx - ax) * abx + (pcy - ay) * aby) * sinv[bi];
-                            if (t >= 0.0f && t <= 1.0f) {
-                                float fx = ax + abx * t, fy = ay + aby * t;
-                                float pz = wmix(sz0[bi], sz1[bi], t);
-                                float rr = wmix(srmin[bi], rmax, wclamp(normalize_depth01(pz), 0.0f, 1.0f));
-                                float dx = pcx - fx, dy = pcy - fy;
-                                float d2 = dx * dx + dy * dy;
-                                if (d2 < rr * rr) {
-                                    float cov = wclamp(1.0f - sqrtf(d2) / rr, 0.0f, 1.0f);
-                                    // perspective_correct_line_t (:149-154)
-                                    float aw0 = wmax(fabsf(sw0[bi]), 1e-6f), aw1 = wmax(fabsf(sw1[bi]), 1e-6f);
-                                    float tw = (t * aw0) / ((1.0f - t) * aw1 + t * aw0);
-                                    float4 c0 = load_half4(reinterpret_cast<const __half*>(&ss0[bi]));
-                                    float4 c1 = load_half4(reinterpret_cast<const __half*>(&ss1[bi]));
-                                    float sr = wmix(c0.x, c1.x, tw), sg = wmix(c0.y, c1.y, tw);
-                                    float sbl = wmix(c0.z, c1.z, tw), sa = wmix(c0.w, c1.w, tw);
-                                    float alpha = sa * cov;
-                                    float vsb = svis[bi];
-                                    part = make_float4(sr * vsb * alpha, sg * vsb * alpha, sbl * vsb * alpha, alpha);
-                                    pd = pz;
-                                    ++frags;
-                                }
-                            }
-                        }
-                    }
+                const uint32_t lead = c - (s_item[c] & 3u);
+                const uint32_t end = min(lead + 4u, s_prefix[item - rp.lo + 1u]);
+                pos = end;
+                pending = item;
+                float4 part[4];
+                float pd[4];
+#pragma unroll
+                for (uint32_t w = 0; w < 4u; ++w) {
+                    part[w] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                    pd[w] = 0.0f;
+                    const uint32_t bi = lead + w;
+                    if (bi >= end || !((s_pmask[(bi >> 5) * kPixelSlots + slot] >> (bi & 31u)) & 1u)) continue;
+                    const float ax = sp0x[bi], ay = sp0y[bi], bx = sp1x[bi], by = sp1y[bi];
+                    const float rmax = srmax[bi];
+                    if ((pcx < wmin(ax, bx) - rmax || pcy < wmin(ay, by) - rmax) ||
+                        (pcx > wmax(ax, bx) + rmax || pcy > wmax(ay, by) + rmax))
+                        continue;
+                    const float abx = bx - ax, aby = by - ay;
+                    float t = ((pcx - ax) * abx + (pcy - ay) * aby) * sinv[bi];
+                    if (!(t >= 0.0f && t <= 1.0f)) continue;
+                    float fx = ax + abx * t, fy = ay + aby * t;
+                    float pz = wmix(sz0[bi], sz1[bi], t);
+                    float rr = wmix(srmin[bi], rmax, wclamp(normalize_depth01(pz), 0.0f, 1.0f));
+                    float dx = pcx - fx, dy = pcy - fy;
+                    float d2 = dx * dx + dy * dy;
+                    if (!(d2 < rr * rr)) continue;
+                    float cov = wclamp(1.0f - sqrtf(d2) / rr, 0.0f, 1.0f);
+                    // perspective_correct_line_t (:149-154)
+                    float aw0 = wmax(fabsf(sw0[bi]), 1e-6f), aw1 = wmax(fabsf(sw1[bi]), 1e-6f);
+                    float tw = (t * aw0) / ((1.0f - t) * aw1 + t * aw0);
+                    float4 c0 = load_half4(reinterpret_cast<const __half*>(&ss0[bi]));
+                    float4 c1 = load_half4(reinterpret_cast<const __half*>(&ss1[bi]));
+                    float sr = wmix(c0.x, c1.x, tw), sg = wmix(c0.y, c1.y, tw);
+                    float sbl = wmix(c0.z, c1.z, tw), sa = wmix(c0.w, c1.w, tw);
+                    float alpha = sa * cov;
+                    float vsb = svis[bi];
+                    part[w] = make_float4(sr * vsb * alpha, sg * vsb * alpha, sbl * vsb * alpha, alpha);
+                    pd[w] = pz;
+                    ++frags;
                 }
                 // (w0 over w1) over (w2 over w3), depth max.
-                const uint32_t src = wbase + (worker | 1u);
-                float4 rhs;
-                rhs.x = __shfl_sync(0xFFFFFFFFu, part.x, src);
-                rhs.y = __shfl_sync(0xFFFFFFFFu, part.y, src);
-                rhs.z = __shfl_sync(0xFFFFFFFFu, part.z, src);
-                rhs.w = __shfl_sync(0xFFFFFFFFu, part.w, src);
-                float rd = __shfl_sync(0xFFFFFFFFu, pd, src);
-                float4 pair = part;
-                float pdd = pd;
-                if ((worker & 1u) == 0u) {
-                    pair = over(part, rhs);
-                    pdd = wmax(pd, rd);
-                }
-                float4 second;
-                second.x = __shfl_sync(0xFFFFFFFFu, pair.x, wbase + 2u);
-                second.y = __shfl_sync(0xFFFFFFFFu, pair.y, wbase + 2u);
-                second.z = __shfl_sync(0xFFFFFFFFu, pair.z, wbase + 2u);
-                second.w = __shfl_sync(0xFFFFFFFFu, pair.w, wbase + 2u);
-                float sdp = __shfl_sync(0xFFFFFFFFu, pdd, wbase + 2u);
-                if (worker == 0u && act) {
-                    fin = over(fin, over(pair, second));
-                    gdepth = wmax(gdepth, wmax(pdd, sdp));
-                }
+                fin = over(fin, over(over(part[0], part[1]), over(part[2], part[3])));
+                gdepth = wmax(gdepth, wmax(wmax(pd[0], pd[1]), wmax(pd[2], pd[3])));
             }
             // The last item blended into ends in this round unless the round
             // stops inside it.
-            end_of_item(pending != kInvalid && (pending + 1u < rp.hi || rp.completes));
-            if (__syncthreads_and(done)) break;
+            if (pending != kInvalid && (pending + 1u < rp.hi || rp.completes)) end_of_item();
+            if (!__syncthreads_or(!done)) break;
         }
-        frags += __shfl_xor_sync(0xFFFFFFFFu, frags, 1);
-        frags += __shfl_xor_sync(0xFFFFFFFFu, frags, 2);
-        if (worker == 0u && active) {
+        if (active) {
             float4 o = fin;
             if (o.w > 1e-6f && o.w < 1.0f) o = make_float4(o.x / o.w, o.y / o.w, o.z / o.w, o.w);
             size_t pi = (size_t)py * P.width + px;
@@ -634,7 +610,6 @@ __global__ void __launch_bounds__(256, 4) k_raster(const FrameParams* __restrict
             R.depth[pi] = gdepth;
             if (P.fragment_counts) R.fragments[pi] = frags;
         }
-        __syncthreads();
     }
 }
 
@@ -651,7 +626,7 @@ void launch_shadow(const LaunchCtx& L, const RenderArgs& R, uint32_t K) {
 }
 
 void launch_raster(const LaunchCtx& L, const RenderArgs& R) {
-    k_raster<<<L.sm_count * 4, 256, 0, L.stream>>>(L.P, L.inst, R);
+    k_raster<<<L.sm_count * 16, kCamThreads, 0, L.stream>>>(L.P, L.inst, R);
 }
 
 }  // namespace fiber
