@@ -72,13 +72,22 @@ __device__ __forceinline__ void slot_source(const uint32_t* s_prefix, const Roun
 
 // ===========================================================================
 // K16 deep-opacity shadow raster + K17 stampback.
+//
+// One 64-thread block per shadow tile run, one thread per pixel. The pixel's
+// thread walks its coverage candidates in entry order: pass 1 finds the
+// nearest covered depth, pass 2 accumulates the opacity of every covered
+// entry into the partial of the reference's depth worker that owns the entry
+// (worker w takes entries w, w+4, ... from each item's start), so each
+// worker's partial sees its entries in the reference's order; the four
+// partials combine in worker order as the reference does.
 // ===========================================================================
-constexpr uint32_t kShadowCap = 768;
+constexpr uint32_t kShadowThreads = 64;  // = kPixelSlots
+constexpr uint32_t kShadowCap = 256;
 constexpr uint32_t kShadowWords = kShadowCap / 32;
 constexpr int kMaxDomSlices = 16;
 
 size_t shadow_smem_bytes(uint32_t K) {
-    return (size_t)kShadowCap * 9 * sizeof(float) + (size_t)256 * K * sizeof(float);
+    return (size_t)kShadowCap * 9 * sizeof(float) + (size_t)kShadowThreads * 4u * K * sizeof(float);
 }
 
 // Coverage candidates. The exact test below covers pixel p (cov > 0) only if
@@ -131,8 +140,8 @@ __device__ __forceinline__ bool band_candidate(const Band& B, float px, float py
     return !(fabsf(d) > B.thr) && !(s < B.slo) && !(s > B.shi);
 }
 
-__global__ void __launch_bounds__(256, 4) k_shadow(const FrameParams* __restrict__ Pp,
-                                                const InstanceView* __restrict__ inst, RenderArgs R) {
+__global__ void __launch_bounds__(kShadowThreads) k_shadow(const FrameParams* __restrict__ Pp,
+                                                           const InstanceView* __restrict__ inst, RenderArgs R) {
     const FrameParams& P = *Pp;
     extern __shared__ float s_dyn[];
     float* sp0x = s_dyn;
@@ -144,22 +153,20 @@ __global__ void __launch_bounds__(256, 4) k_shadow(const FrameParams* __restrict
     float* srmin = sp1z + kShadowCap;
     float* srmax = srmin + kShadowCap;
     float* sabs = srmax + kShadowCap;
-    float* s_partial = sabs + kShadowCap;
+    float* s_partial = sabs + kShadowCap;  // [pixel][worker][K]
     __shared__ uint32_t s_wbase[kMaxRunItems], s_wcount[kMaxRunItems], s_prefix[kMaxRunItems + 1];
     __shared__ uint32_t s_pmask[kShadowWords * kPixelSlots];  // [word][pixel] candidate bits
-    __shared__ uint32_t s_wmask[4 * kShadowWords];            // [worker][word] entries of worker w
-    __shared__ uint16_t s_item[kShadowCap];                   // run item of each staged entry
+    __shared__ uint16_t s_item[kShadowCap];                   // run item << 2 | worker of each staged entry
     __shared__ float2 s_pix[kPixelSlots];
     __shared__ RoundPlan s_plan;
-    __shared__ uint32_t s_more;
+    __shared__ uint32_t s_more, s_run;
 
     const uint32_t first = *((volatile uint32_t*)&R.counters->camera_active);
     const uint32_t last = *((volatile uint32_t*)&R.counters->active_tiles);
     const uint32_t K = P.K, D = P.dom_size, S = P.shadow_map_size;
-    const uint32_t slot = threadIdx.x >> 2, worker = threadIdx.x & 3u;
+    const uint32_t slot = threadIdx.x;
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-    float* partial = s_partial + threadIdx.x * K;
-    __shared__ uint32_t s_run;
+    float* partial = s_partial + (size_t)slot * 4u * K;
 
     // Blocks claim runs from a counter, so long runs do not pile up on one block.
     for (;;) {
@@ -189,12 +196,12 @@ __global__ void __launch_bounds__(256, 4) k_shadow(const FrameParams* __restrict
             s_wbase[i] = wi.seg_ref_base;
             s_wcount[i] = valid_item ? wi.seg_ref_count : 0u;
         }
-        if (worker == 0u) s_pix[slot] = make_float2(pfx, pfy);
+        s_pix[slot] = make_float2(pfx, pfy);
         __syncthreads();
 
-        // Stage a round (projection, radii, run item, worker of each entry:
-        // worker w takes entries w, w+4, ... from each item's start), then build
-        // the candidate bits: warp per 32-entry word, one ballot per pixel.
+        // Stage a round (projection, radii, run item and worker of each entry),
+        // then build the candidate bits: warp per 32-entry word, one ballot per
+        // pixel.
         auto stage = [&](const RoundPlan& rp) {
             for (uint32_t s = threadIdx.x; s < rp.n; s += blockDim.x) {
                 uint32_t item, j;
@@ -231,19 +238,13 @@ __global__ void __launch_bounds__(256, 4) k_shadow(const FrameParams* __restrict
                 }
                 s_pmask[q * kPixelSlots + lane] = lo;
                 s_pmask[q * kPixelSlots + lane + 32u] = hi;
-                const uint32_t wk = v ? (s_item[s] & 3u) : 4u;
-#pragma unroll
-                for (uint32_t w = 0; w < 4u; ++w) {
-                    const unsigned bal = __ballot_sync(0xFFFFFFFFu, wk == w);
-                    if (lane == w) s_wmask[w * kShadowWords + q] = bal;
-                }
             }
         };
 
-        // This lane's candidates (pixel slot, worker) in entry order.
+        // This pixel's candidates in entry order.
         auto next_candidate = [&](uint32_t nq, uint32_t& q, uint32_t& m) -> uint32_t {
             while (m == 0u && q < nq) {
-                m = s_pmask[q * kPixelSlots + slot] & s_wmask[worker * kShadowWords + q];
+                m = s_pmask[q * kPixelSlots + slot];
                 ++q;
             }
             if (m == 0u) return kInvalid;
@@ -253,13 +254,11 @@ __global__ void __launch_bounds__(256, 4) k_shadow(const FrameParams* __restrict
         };
 
         // ---- Pass 1: nearest covered depth = max depth of the covered entries
-        // of the first run item holding one. The max does not depend on order,
-        // so the pixel's 4 lanes split its candidates by worker; a lane stops
-        // once its next candidate lies past the pixel's best item so far.
-        uint32_t best = kInvalid;      // this lane's first item with a covered entry
-        float zb = -1.0f;              // its max covered depth in that item
-        uint32_t pix_best = kInvalid;  // min of best over the pixel's 4 lanes
-        bool complete = !active;       // the pixel's best item is fully processed
+        // of the first run item holding one; the walk stops once the next
+        // candidate lies past that item.
+        uint32_t best = kInvalid;  // first item with a covered entry
+        float z0 = -1.0f;          // its max covered depth
+        bool complete = !active;   // the best item is fully processed
         uint32_t cur_item = 0u, cur_off = 0u;
         bool single_round = false, staged_all = false;
         for (bool first_round = true;; first_round = false) {
@@ -276,48 +275,35 @@ __global__ void __launch_bounds__(256, 4) k_shadow(const FrameParams* __restrict
             stage(rp);
             __syncthreads();
             staged_all = single_round;
-            const uint32_t nq = (rp.n + 31u) >> 5;
-            uint32_t q = 0u, m = 0u;
-            bool done = complete;
-            while (!__all_sync(0xFFFFFFFFu, done)) {
-                if (!done) {
-                    const uint32_t bi = next_candidate(nq, q, m);
-                    const uint32_t item = bi != kInvalid ? (uint32_t)(s_item[bi] >> 2) : kInvalid;
-                    if (bi == kInvalid || item > pix_best) {
-                        done = true;
-                    } else {
-                        float t = line_t(pfx, pfy, sp0x[bi], sp0y[bi], sp1x[bi], sp1y[bi]);
-                        if (!(t < 0.0f || t > 1.0f)) {
-                            float qx = wmix(sp0x[bi], sp1x[bi], t), qy = wmix(sp0y[bi], sp1y[bi], t);
-                            float qz = wmix(sp0z[bi], sp1z[bi], t);
-                            float rr = wmix(srmin[bi], srmax[bi], wclamp(qz, 0.0f, 1.0f));
-                            float dx = pfx - qx, dy = pfy - qy;
-                            float cov = wclamp(1.0f - sqrtf(dx * dx + dy * dy) / rr, 0.0f, 1.0f);
-                            if (cov > 0.0f) {
-                                if (best == kInvalid) { best = item; zb = wmax(-1.0f, qz); }
-                                else if (item == best) zb = wmax(zb, qz);
-                            }
-                        }
+            if (!complete) {
+                const uint32_t nq = (rp.n + 31u) >> 5;
+                uint32_t q = 0u, m = 0u;
+                for (uint32_t bi; (bi = next_candidate(nq, q, m)) != kInvalid;) {
+                    const uint32_t item = (uint32_t)(s_item[bi] >> 2);
+                    if (best != kInvalid && item > best) break;
+                    float t = line_t(pfx, pfy, sp0x[bi], sp0y[bi], sp1x[bi], sp1y[bi]);
+                    if (t < 0.0f || t > 1.0f) continue;
+                    float qx = wmix(sp0x[bi], sp1x[bi], t), qy = wmix(sp0y[bi], sp1y[bi], t);
+                    float qz = wmix(sp0z[bi], sp1z[bi], t);
+                    float rr = wmix(srmin[bi], srmax[bi], wclamp(qz, 0.0f, 1.0f));
+                    float dx = pfx - qx, dy = pfy - qy;
+                    float cov = wclamp(1.0f - sqrtf(dx * dx + dy * dy) / rr, 0.0f, 1.0f);
+                    if (cov > 0.0f) {
+                        if (best == kInvalid) { best = item; z0 = wmax(-1.0f, qz); }
+                        else z0 = wmax(z0, qz);
                     }
                 }
-                uint32_t pb = min(best, __shfl_xor_sync(0xFFFFFFFFu, best, 1));
-                pix_best = min(pb, __shfl_xor_sync(0xFFFFFFFFu, pb, 2));
+                complete = best != kInvalid && (best + 1u < rp.hi || rp.completes);
             }
-            complete = !active || (pix_best != kInvalid && (pix_best + 1u < rp.hi || rp.completes));
             if (__syncthreads_and(complete)) break;
         }
-        float zc = best == pix_best ? zb : -1.0f;
-        zc = wmax(zc, __shfl_xor_sync(0xFFFFFFFFu, zc, 1));
-        zc = wmax(zc, __shfl_xor_sync(0xFFFFFFFFu, zc, 2));
-        const bool found = active && pix_best != kInvalid;
-        const float z0 = zc;
+        const bool found = active && best != kInvalid;
 
-        // ---- Pass 2: opacity partials; worker w takes entries w, w+4, ... of each item.
-        for (uint32_t i = 0; i < K; ++i) partial[i] = 0.0f;
-        const bool alpha_active = active && found;
-        const float alpha_z0 = alpha_active ? z0 : 1.0f;
+        // ---- Pass 2: opacity partials, each covered entry into its worker's.
+        for (uint32_t i = 0; i < 4u * K; ++i) partial[i] = 0.0f;
+        const float alpha_z0 = found ? z0 : 1.0f;
         const float inv_span = 1.0f / wmax(1e-6f, alpha_z0);
-        if (__syncthreads_or(alpha_active)) {
+        if (__syncthreads_or(found)) {
             cur_item = 0u;
             cur_off = 0u;
             for (;;) {
@@ -332,7 +318,7 @@ __global__ void __launch_bounds__(256, 4) k_shadow(const FrameParams* __restrict
                     __syncthreads();
                 }
                 const RoundPlan rp = s_plan;
-                if (alpha_active) {
+                if (found) {
                     const uint32_t nq = (rp.n + 31u) >> 5;
                     uint32_t q = 0u, m = 0u;
                     for (uint32_t bi; (bi = next_candidate(nq, q, m)) != kInvalid;) {
@@ -350,11 +336,12 @@ __global__ void __launch_bounds__(256, 4) k_shadow(const FrameParams* __restrict
                         uint32_t si = min(f2u(floorf(tl)), K - 1u);
                         float wf = tl - floorf(tl);
                         float al = cov * sabs[bi] * 0.5f;
-                        float a0 = partial[si];
-                        partial[si] = wclamp(a0 + (1.0f - a0) * (1.0f - wf) * al, 0.0f, 1.0f);
+                        float* pw = partial + (uint32_t)(s_item[bi] & 3u) * K;
+                        float a0 = pw[si];
+                        pw[si] = wclamp(a0 + (1.0f - a0) * (1.0f - wf) * al, 0.0f, 1.0f);
                         if (si + 1u < K) {
-                            float a1 = partial[si + 1u];
-                            partial[si + 1u] = wclamp(a1 + (1.0f - a1) * wf * al, 0.0f, 1.0f);
+                            float a1 = pw[si + 1u];
+                            pw[si + 1u] = wclamp(a1 + (1.0f - a1) * wf * al, 0.0f, 1.0f);
                         }
                     }
                 }
@@ -362,9 +349,8 @@ __global__ void __launch_bounds__(256, 4) k_shadow(const FrameParams* __restrict
                 __syncthreads();
             }
         }
-        __syncwarp();
         // ---- Combine the 4 workers per slice, write the DOM, stamp the shadow map.
-        if (worker == 0u && active) {
+        if (active) {
             const size_t dom_px = (size_t)py * D + px;
             if (!found) {
                 R.dom_depth[(size_t)layer * D * D + dom_px] = 0.0f;
@@ -374,7 +360,7 @@ __global__ void __launch_bounds__(256, 4) k_shadow(const FrameParams* __restrict
                 float acc = 0.0f;
                 for (uint32_t i = 0; i < K; ++i) {
                     float a = 0.0f;
-                    for (uint32_t wk = 0; wk < 4u; ++wk) a = a + (1.0f - a) * s_partial[(threadIdx.x + wk) * K + i];
+                    for (uint32_t wk = 0; wk < 4u; ++wk) a = a + (1.0f - a) * partial[wk * K + i];
                     acc = acc + (1.0f - acc) * a;  // opaque_terminal_slice = K without an opaque depth
                     R.dom_opacity[((size_t)layer * K + i) * D * D + dom_px] = acc;
                 }
@@ -397,7 +383,6 @@ __global__ void __launch_bounds__(256, 4) k_shadow(const FrameParams* __restrict
                 }
             }
         }
-        __syncthreads();
     }
 }
 
@@ -622,7 +607,7 @@ void launch_shadow(const LaunchCtx& L, const RenderArgs& R, uint32_t K) {
         cudaFuncSetAttribute(k_shadow, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_bytes);
         if (dev >= 0 && dev < 64) configured[dev] = true;
     }
-    k_shadow<<<L.sm_count * 4, 256, shadow_smem_bytes(K), L.stream>>>(L.P, L.inst, R);
+    k_shadow<<<L.sm_count * 16, kShadowThreads, shadow_smem_bytes(K), L.stream>>>(L.P, L.inst, R);
 }
 
 void launch_raster(const LaunchCtx& L, const RenderArgs& R) {
