@@ -82,7 +82,7 @@ __device__ __forceinline__ void slot_source(const uint32_t* s_prefix, const Roun
 // partials combine in worker order as the reference does.
 // ===========================================================================
 constexpr uint32_t kShadowThreads = 64;  // = kPixelSlots
-constexpr uint32_t kShadowCap = 256;
+constexpr uint32_t kShadowCap = 128;
 constexpr uint32_t kShadowWords = kShadowCap / 32;
 constexpr int kMaxDomSlices = 16;
 
