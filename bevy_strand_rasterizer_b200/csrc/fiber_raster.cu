@@ -3,16 +3,18 @@
 // strand_rasterizer.wgsl:391-711 (SHADOWS) and :855-1044 (LINEAR),
 // shadow_dom_stampback.wgsl:74-123.
 //
-// One block per tile run: 64 pixel slots x 4 workers, a pixel's 4 workers in
-// adjacent lanes of one warp. The run's references are staged into shared
-// memory a round at a time by all 256 threads (per-reference projection,
-// radii, shading texels); a round holds whole work items, or one CAP-sized
-// chunk of an item longer than CAP (CAP is a multiple of 16, so the
-// reference's groups of 4 never straddle a round). Within a round the pixels
-// walk the work items warp-synchronously (shuffles only); block barriers
-// happen only between rounds. The blend order is the reference's: work items
-// near to far, references in groups of 4 from each item's start, (w0 over w1)
-// over (w2 over w3), early out after each item once alpha > 0.98.
+// One 64-thread block per tile run, one thread per pixel slot (the reference's
+// 64 slots; its 4 depth workers per pixel become the order in which one
+// thread applies the same operations). Blocks claim runs from a counter. The
+// run's references are staged into shared memory a round at a time
+// (per-reference projection, radii, shading texels); a round holds whole work
+// items, or one CAP-sized chunk of an item longer than CAP (CAP is a multiple
+// of 16, so the reference's groups of 4 never straddle a round). Each round
+// also builds per-pixel coverage-candidate bits from a conservative band
+// test, and each pixel walks only its candidates. Block barriers happen only
+// between rounds. The blend order is the reference's: work items near to far,
+// references in groups of 4 from each item's start, (w0 over w1) over (w2 over
+// w3), early out after each item once alpha > 0.98.
 #include "fiber_kernels.cuh"
 
 namespace fiber {
