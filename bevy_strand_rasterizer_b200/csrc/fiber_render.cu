@@ -15,7 +15,7 @@ __constant__ float c_leg_roots[10] = {-9.739065170e-01f, -8.650633693e-01f, -6.7
 __constant__ float c_leg_weights[10] = {6.667134166e-02f, 1.494513452e-01f, 2.190863639e-01f, 2.692667246e-01f,
                                         2.955242395e-01f, 2.955242395e-01f, 2.692667246e-01f, 2.190863639e-01f,
                                         1.494513452e-01f, 6.667134166e-02f};
-__constant__ float c_factorials[10] = {1.0f, 1.0f, 2.0f, 6.0f, 24.0f, 120.0f, 720.0f, 5040.0f, 40320.0f, 362880.0f};
+__constant__ float c_mp_den[5] = {1.0f, 4.0f, 64.0f, 2304.0f, 147456.0f};  // 4^i (i!)^2
 constexpr float kPi = 3.14159265359f;
 constexpr float kPiHalf = kPi / 2.0f;
 
@@ -67,9 +67,10 @@ __device__ __forceinline__ float fresnel_reflectance(float eta_i, float eta_t, f
 // -110 are exactly zero in binary32 and are skipped without changing the sum;
 // the test is written so that a NaN exponent is not skipped and still poisons
 // the sum, as exp(NaN) does in the reference. Only k with |phi - 2 pi k| below
-// sqrt(110 * 2 var) can pass it, so the loop runs over that window (widened
-// by one k on each side and by 1e-3 relative + 1e-3 absolute), in the same
-// increasing k order; a NaN phi takes the full range.
+// sqrt(110 * 2 var) can pass it, so the loop runs over that window (its reach
+// widened by 1e-3 relative + 1e-3 absolute, far beyond the rounding of the
+// bounds and of e), in the same increasing k order; a NaN phi takes the full
+// range.
 __device__ __forceinline__ float gaussian_detector(float beta, float phi_delta) {
     float var = beta * beta;
     if (var < 1e-6f) {
@@ -83,8 +84,8 @@ __device__ __forceinline__ float gaussian_detector(float beta, float phi_delta) 
     if (phi_delta == phi_delta) {
         const float reach = sqrtf(110.0f * two_var) * 1.001f + 1e-3f;
         const float inv_two_pi = 1.0f / (2.0f * kPi);
-        const float lo = wclamp(floorf((phi_delta - reach) * inv_two_pi) - 1.0f, -11.0f, 11.0f);
-        const float hi = wclamp(ceilf((phi_delta + reach) * inv_two_pi) + 1.0f, -11.0f, 11.0f);
+        const float lo = wclamp(floorf((phi_delta - reach) * inv_two_pi), -11.0f, 11.0f);
+        const float hi = wclamp(ceilf((phi_delta + reach) * inv_two_pi), -11.0f, 11.0f);
         k0 = max(k0, (int)lo);
         k1 = min(k1, (int)hi);
     }
@@ -139,12 +140,15 @@ __device__ F3 marschner(F3 L, F3 V, F3 U, const fiber_strand_material& m, float 
             float tol = 0.1f * (kPi / 180.0f);
             mp = fabsf(trs + ti) < tol ? 0.0f : 1e6f / tol;
         } else {
+            // sum_i x^(2i) / (4^i (i!)^2), i = 0..4: the powers of x as running
+            // products, the denominators as their exact values 1, 4, 64, 2304,
+            // 147456.
             float x = (cti * ctr) / v_long;
-            float y = 0.0f;
+            const float x2 = x * x;
+            float y = 0.0f, num = 1.0f;
             for (uint32_t i = 0; i < 5u; ++i) {
-                float num = powf(x, 2.0f * u2f(i));
-                float den = powf(4.0f, u2f(i)) * c_factorials[i] * c_factorials[i];
-                y = y + num / den;
+                y = y + num / c_mp_den[i];
+                num = num * x2;
             }
             mp = y * expf((sti * strs) / v_long);
         }
@@ -201,7 +205,7 @@ __device__ F3 marschner(F3 L, F3 V, F3 U, const fiber_strand_material& m, float 
     return f3(tot[0], tot[1], tot[2]);
 }
 
-__global__ void __launch_bounds__(128) k_shade(const FrameParams* __restrict__ Pp,
+__global__ void __launch_bounds__(128, 6) k_shade(const FrameParams* __restrict__ Pp,
                                                const InstanceView* __restrict__ inst, RenderArgs R) {
     const FrameParams& P = *Pp;
     __shared__ QuadTable s_quad;
