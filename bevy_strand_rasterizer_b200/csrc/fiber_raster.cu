@@ -99,13 +99,12 @@ size_t shadow_smem_bytes(uint32_t K) {
 // coordinate magnitude, hundreds of float ulps beyond the rounding of the
 // exact test and of this one, so every pixel the band rejects is one the exact
 // test leaves uncovered. Comparisons are written so that NaN never rejects;
-// segments shorter than 1e-6 px are tested as a disc around the first point.
+// a segment shorter than 1e-6 px is a candidate of every pixel (the exact
+// test decides), which keeps the per-pixel test free of branches.
 struct Band {
     float nx, ny, c;    // d = n . p - c
     float ux, uy, cu;   // s = u . p - cu
     float thr, slo, shi;
-    float ax, ay;
-    bool disc;
 };
 
 __device__ __forceinline__ Band make_band(float ax, float ay, float bx, float by, float z0, float z1, float rmin,
@@ -117,7 +116,6 @@ __device__ __forceinline__ Band make_band(float ax, float ay, float bx, float by
     B.thr = rb * 1.0001f + 1e-6f * rmax + slack;
     const float abx = bx - ax, aby = by - ay;
     const float l2 = abx * abx + aby * aby;
-    B.disc = !(l2 > 1e-12f);
     const float len = sqrtf(l2);
     B.ux = abx / len;
     B.uy = aby / len;
@@ -127,16 +125,17 @@ __device__ __forceinline__ Band make_band(float ax, float ay, float bx, float by
     B.cu = __fmaf_rn(B.ux, ax, B.uy * ay);
     B.slo = -slack;
     B.shi = len + slack;
-    B.ax = ax;
-    B.ay = ay;
+    if (!(l2 > 1e-12f)) {  // degenerate (or NaN): d = s = 0 within unbounded limits
+        const float inf = __int_as_float(0x7f800000);
+        B.nx = B.ny = B.c = B.ux = B.uy = B.cu = 0.0f;
+        B.thr = inf;
+        B.slo = -inf;
+        B.shi = inf;
+    }
     return B;
 }
 
 __device__ __forceinline__ bool band_candidate(const Band& B, float px, float py) {
-    if (B.disc) {
-        const float dx = px - B.ax, dy = py - B.ay;
-        return !(dx * dx + dy * dy > B.thr * B.thr);
-    }
     const float d = __fmaf_rn(B.nx, px, __fmaf_rn(B.ny, py, -B.c));
     const float s = __fmaf_rn(B.ux, px, __fmaf_rn(B.uy, py, -B.cu));
     return !(fabsf(d) > B.thr) && !(s < B.slo) && !(s > B.shi);
@@ -230,16 +229,12 @@ __global__ void __launch_bounds__(kShadowThreads) k_shadow(const FrameParams* __
                 const uint32_t e = v ? s : 0u;
                 const Band B = make_band(sp0x[e], sp0y[e], sp1x[e], sp1y[e], sp0z[e], sp1z[e], srmin[e], srmax[e],
                                          tile_max);
-                uint32_t lo = 0u, hi = 0u;
 #pragma unroll 8
                 for (uint32_t p = 0; p < kPixelSlots; ++p) {
                     const float2 pp = s_pix[p];
                     const unsigned bal = __ballot_sync(0xFFFFFFFFu, v && band_candidate(B, pp.x, pp.y));
-                    if (p == lane) lo = bal;
-                    if (p == lane + 32u) hi = bal;
+                    if (lane == 0u) s_pmask[q * kPixelSlots + p] = bal;
                 }
-                s_pmask[q * kPixelSlots + lane] = lo;
-                s_pmask[q * kPixelSlots + lane + 32u] = hi;
             }
         };
 
@@ -515,16 +510,12 @@ __global__ void __launch_bounds__(kCamThreads) k_raster(const FrameParams* __res
                 const uint32_t e = v ? s : 0u;
                 const Band B = make_band(sp0x[e], sp0y[e], sp1x[e], sp1y[e], normalize_depth01(sz0[e]),
                                          normalize_depth01(sz1[e]), srmin[e], srmax[e], tile_max);
-                uint32_t lo = 0u, hi = 0u;
 #pragma unroll 8
                 for (uint32_t p = 0; p < kPixelSlots; ++p) {
                     const float2 pp = s_pix[p];
                     const unsigned bal = __ballot_sync(0xFFFFFFFFu, v && band_candidate(B, pp.x, pp.y));
-                    if (p == lane) lo = bal;
-                    if (p == lane + 32u) hi = bal;
+                    if (lane == 0u) s_pmask[q * kPixelSlots + p] = bal;
                 }
-                s_pmask[q * kPixelSlots + lane] = lo;
-                s_pmask[q * kPixelSlots + lane + 32u] = hi;
             }
             __syncthreads();
             uint32_t pos = 0u;  // next entry of this pixel's walk
