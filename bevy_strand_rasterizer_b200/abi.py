@@ -34,7 +34,7 @@ FMT_RGBA16F, FMT_R32F, FMT_RGBA32F = 0, 1, 2
 (DUMP_FRUSTA, DUMP_RANGES, DUMP_KEEP, DUMP_LUT, DUMP_TASKS, DUMP_PROJECTED, DUMP_PAGE_TABLE,
  DUMP_PAGE_META, DUMP_COUNTS, DUMP_OFFSETS, DUMP_REFS, DUMP_ACTIVE_TILES, DUMP_WORK, DUMP_RUNS,
  DUMP_DOM_DEPTH, DUMP_DOM_OPACITY, DUMP_SHADOW_MAP, DUMP_ATLAS, DUMP_HISTORY, DUMP_COLOR,
- DUMP_DEPTH, DUMP_FRAGMENTS) = range(22)
+ DUMP_DEPTH, DUMP_FRAGMENTS, DUMP_OPAQUE_TILES) = range(23)
 
 
 class DevicePtr(C.Structure):
@@ -157,13 +157,14 @@ DUMP_DTYPES = {
     DUMP_RUNS: RASTER_TILE_RUN, DUMP_DOM_DEPTH: np.dtype("<f4"), DUMP_DOM_OPACITY: np.dtype("<f4"),
     DUMP_SHADOW_MAP: np.dtype("<f4"), DUMP_ATLAS: np.dtype("<f2"), DUMP_HISTORY: np.dtype("<f2"),
     DUMP_COLOR: np.dtype("<f2"), DUMP_DEPTH: np.dtype("<f4"), DUMP_FRAGMENTS: np.dtype("<u4"),
+    DUMP_OPAQUE_TILES: np.dtype("<u4"),
 }
 
 # Every symbol include/fiber.h declares (checked by tests/test_abi.py).
 EXPORTS = [
     "fiber_ctx_create", "fiber_ctx_destroy", "fiber_settings_default", "fiber_settings_set",
     "fiber_slab_alloc", "fiber_slab_upload", "fiber_slab_free", "fiber_instance_set", "fiber_frame_begin",
-    "fiber_prepass", "fiber_shadows", "fiber_shading", "fiber_raster", "fiber_composite", "fiber_frame_fused",
+    "fiber_opaque_depth", "fiber_prepass", "fiber_shadows", "fiber_shading", "fiber_raster", "fiber_composite", "fiber_frame_fused",
     "fiber_render_host", "fiber_stats_get", "fiber_dump", "fiber_output_image", "fiber_span_count", "fiber_span_name",
     "fiber_span_times", "fiber_status_string", "fiber_server_create", "fiber_server_add_scene",
     "fiber_server_start", "fiber_server_submit", "fiber_server_wait", "fiber_server_destroy", "fiber_server_now_ns",
@@ -199,6 +200,7 @@ def load_library(path: Path | str | None = None) -> C.CDLL:
         "fiber_slab_free": (C.c_int, [vp, u32, u32]),
         "fiber_instance_set": (C.c_int, [vp, pp(StrandInstance), u32]),
         "fiber_frame_begin": (C.c_int, [vp, pp(FroxelConfigC), pp(Camera), pp(FroxelConfigC), pp(Light), u32, vp]),
+        "fiber_opaque_depth": (C.c_int, [vp, pp(Image), u32, vp]),
         "fiber_prepass": (C.c_int, [vp, vp]),
         "fiber_shadows": (C.c_int, [vp, vp]),
         "fiber_shading": (C.c_int, [vp, vp]),

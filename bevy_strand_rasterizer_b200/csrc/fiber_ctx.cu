@@ -111,6 +111,9 @@ struct fiber_ctx {
     DevBuf d_lut, d_tasks, d_projected, d_page_table, d_page_meta, d_counts, d_offsets, d_cursors;
     DevBuf d_refs, d_ref_keys, d_active_flags, d_active_list, d_work, d_runs, d_big_cells;
     DevBuf d_visit_rec, d_visit_task, d_visit_rank, d_task_key, d_task_mat, d_cells_small, d_cells_large;
+    DevBuf d_opaque;  // (covered, farthest depth q) per camera fine tile
+    uint32_t camera_fine_tiles = 0;
+    bool opaque_frame = false;  // fiber_opaque_depth ran since fiber_frame_begin
     DevBuf d_dom_depth, d_dom_opacity, d_shadow_map, d_atlas, d_history[2];
     DevBuf d_color, d_depth, d_fragments, d_validate, d_host_scene, d_host_depth;
     int hist_cur = 0;
@@ -180,6 +183,7 @@ LaunchCtx launch_ctx(fiber_ctx* c, cudaStream_t s) {
     L.I = c->P.I;
     L.total_coarse_tiles = c->P.total_coarse_tiles;
     L.sm_count = c->sm_count;
+    L.opaque = c->opaque_frame;
     return L;
 }
 
@@ -213,6 +217,7 @@ PrepassArgs prepass_args(fiber_ctx* c) {
     A.task_mat = dp<uint32_t>(c->d_task_mat);
     A.cells_small = dp<uint2>(c->d_cells_small);
     A.cells_large = dp<uint2>(c->d_cells_large);
+    A.opaque_tiles = dp<uint2>(c->d_opaque);
     return A;
 }
 
@@ -262,10 +267,20 @@ fiber_status check_launch() {
     return e == cudaSuccess ? FIBER_OK : FIBER_ECUDA;
 }
 
-fiber_status run_prepass(fiber_ctx* c, cudaStream_t s) {
+// The camera's opaque depth for K0: R32F rows of width * samples floats.
+struct OpaqueSource {
+    const float* depth;
+    uint32_t pitch, samples;
+};
+
+fiber_status run_prepass(fiber_ctx* c, cudaStream_t s, const OpaqueSource* opaque = nullptr) {
     LaunchCtx L = launch_ctx(c, s);
     PrepassArgs A = prepass_args(c);
     record(c, 0, s);
+    if (opaque) {
+        launch_opaque(L, A, opaque->depth, opaque->pitch, opaque->samples, c->camera_fine_tiles);
+        L.opaque = true;
+    }
     launch_broad(L, A);
     launch_lut(L, A);
     record(c, 1, s);
@@ -316,6 +331,20 @@ fiber_status run_raster(fiber_ctx* c, cudaStream_t s) {
 
 uint32_t fmt_bytes(uint32_t fmt) {
     return fmt == FIBER_FMT_RGBA16F ? 8u : (fmt == FIBER_FMT_R32F ? 4u : 16u);
+}
+
+// Checks an opaque depth image against the camera (R32F, camera extent,
+// `samples` floats per pixel, rows 4-byte aligned and wide enough).
+fiber_status opaque_source(const fiber_ctx* c, const fiber_image* im, uint32_t samples, OpaqueSource& o) {
+    if (!im || !im->ptr || im->format != FIBER_FMT_R32F || (samples != 1u && samples != 4u)) return FIBER_EINVAL;
+    if (im->width != c->P.width || im->height != c->P.height) return FIBER_EINVAL;
+    const uint64_t row = (uint64_t)im->width * samples * 4u;
+    const uint64_t pitch = im->pitch ? im->pitch : row;
+    if (pitch < row || pitch % 4u || pitch > 0xFFFFFFFFull || (uintptr_t)im->ptr % 4u) return FIBER_EINVAL;
+    o.depth = static_cast<const float*>(im->ptr);
+    o.pitch = (uint32_t)pitch;
+    o.samples = samples;
+    return FIBER_OK;
 }
 
 fiber_status run_composite(fiber_ctx* c, const fiber_image* scene_color, const fiber_image* scene_depth,
@@ -437,7 +466,7 @@ fiber_status fiber_ctx_destroy(fiber_ctx* c) {
                       &c->d_history[0], &c->d_history[1], &c->d_color, &c->d_depth, &c->d_fragments,
                       &c->d_validate, &c->d_host_scene, &c->d_host_depth, &c->d_visit_rec,
                       &c->d_visit_task, &c->d_visit_rank, &c->d_task_key, &c->d_task_mat,
-                      &c->d_cells_small, &c->d_cells_large};
+                      &c->d_cells_small, &c->d_cells_large, &c->d_opaque};
     for (DevBuf* b : bufs) release(c, *b);
     for (int i = 0; i <= kSpanCount; ++i)
         if (c->ev[i]) cudaEventDestroy(c->ev[i]);
@@ -619,7 +648,10 @@ fiber_status fiber_frame_begin(fiber_ctx* c, const fiber_froxel_config* cam_cfg,
         bucket += d.bucket_count;
         coarse += d.coarse_depth_tile_count;
         fine += tx * ty;
-        if (f == 0) cam_tiles = coarse;
+        if (f == 0) {
+            cam_tiles = coarse;
+            c->camera_fine_tiles = tx * ty;
+        }
         P.frusta[f] = d;
         std::memcpy(P.clip[f], f == 0 ? cam->clip_from_world : lights[f - 1].clip_from_world, 64);
     }
@@ -729,6 +761,7 @@ fiber_status fiber_frame_begin(fiber_ctx* c, const fiber_froxel_config* cam_cfg,
     // Non-empty cells: at most one per kept reference and one per cell.
     ENSURE(c->d_cells_small, std::min<uint64_t>(ref_cap, page_cap * kPageSize) * sizeof(uint2), false);
     ENSURE(c->d_cells_large, (ref_cap / 9 + 1) * sizeof(uint2), false);
+    ENSURE(c->d_opaque, (uint64_t)c->camera_fine_tiles * sizeof(uint2), false);
     ENSURE(c->d_dom_depth, L * D * D * 4, false);
     ENSURE(c->d_dom_opacity, L * K * D * D * 4, true);
     ENSURE(c->d_shadow_map, L * S * S * 4, false);
@@ -769,7 +802,22 @@ fiber_status fiber_frame_begin(fiber_ctx* c, const fiber_froxel_config* cam_cfg,
     }
     c->last_stream = s;
     c->frame_ready = true;
+    c->opaque_frame = false;
     return FIBER_OK;
+}
+
+fiber_status fiber_opaque_depth(fiber_ctx* c, const fiber_image* depth, uint32_t samples, void* stream) {
+    if (!c) return FIBER_EINVAL;
+    if (!c->frame_ready) return FIBER_ENOTREADY;
+    OpaqueSource o;
+    fiber_status st = opaque_source(c, depth, samples, o);
+    if (st != FIBER_OK) return st;
+    cudaSetDevice(c->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    c->last_stream = s;
+    launch_opaque(launch_ctx(c, s), prepass_args(c), o.depth, o.pitch, o.samples, c->camera_fine_tiles);
+    c->opaque_frame = true;
+    return check_launch();
 }
 
 fiber_status fiber_prepass(fiber_ctx* c, void* stream) {
@@ -823,8 +871,14 @@ fiber_status fiber_frame_fused(fiber_ctx* c, const fiber_image* scene_color, con
     cudaStream_t s = (cudaStream_t)stream_;
     c->last_stream = s;
     const bool composite = scene_color && out;
+    OpaqueSource opaque{};
+    if (scene_depth) {
+        fiber_status st = opaque_source(c, scene_depth, 1u, opaque);
+        if (st != FIBER_OK) return st;
+    }
+    const OpaqueSource* op = scene_depth ? &opaque : nullptr;
     if (!s) {  // the legacy stream cannot be captured: run the nodes directly
-        fiber_status st = run_prepass(c, s);
+        fiber_status st = run_prepass(c, s, op);
         if (st == FIBER_OK) st = run_shadows(c, s);
         if (st == FIBER_OK) st = run_shading(c, s);
         if (st == FIBER_OK) st = run_raster(c, s);
@@ -836,13 +890,14 @@ fiber_status fiber_frame_fused(fiber_ctx* c, const fiber_image* scene_color, con
     // the device FrameParams), so one captured graph serves every frame of the
     // same shape and buffers. The shape is whatever the host bakes into the
     // launches: grid sizes (instances, coarse tiles), the shadow's shared
-    // memory (K) and whether it runs (lights), and the composite's image
-    // extents, pitches and formats.
+    // memory (K) and whether it runs (lights), the composite's image
+    // extents, pitches and formats, and whether the walks cull against opaque
+    // tiles (their kernel variant).
     auto pitch_of = [](const fiber_image* im) -> uint64_t {
         return im ? ((uint64_t)im->pitch << 32) | (uint64_t)im->format : 0u;
     };
     uint64_t key[kGraphKeyWords] = {c->buffer_generation,
-                                    (uint64_t)(composite ? 1 : 0),
+                                    (uint64_t)(composite ? 1 : 0) | (uint64_t)(op || c->opaque_frame ? 2 : 0),
                                     (uint64_t)(uintptr_t)(scene_color ? scene_color->ptr : nullptr),
                                     (uint64_t)(uintptr_t)(scene_depth ? scene_depth->ptr : nullptr),
                                     (uint64_t)(uintptr_t)(out ? out->ptr : nullptr),
@@ -862,7 +917,7 @@ fiber_status fiber_frame_fused(fiber_ctx* c, const fiber_image* scene_color, con
         cudaGraph_t g = nullptr;
         FIBER_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
         const int hist_before = c->hist_cur;
-        fiber_status st = run_prepass(c, s);
+        fiber_status st = run_prepass(c, s, op);
         if (st == FIBER_OK) st = run_shadows(c, s);
         if (st == FIBER_OK) st = run_shading(c, s);
         if (st == FIBER_OK) st = run_raster(c, s);
@@ -1111,6 +1166,16 @@ fiber_status fiber_dump(fiber_ctx* c, uint32_t what, void* host, uint64_t capaci
         case FIBER_DUMP_COLOR: src = c->d_color.p; bytes = W * H * 8; break;
         case FIBER_DUMP_DEPTH: src = c->d_depth.p; bytes = W * H * 4; break;
         case FIBER_DUMP_FRAGMENTS: src = c->d_fragments.p; bytes = W * H * 4; break;
+        case FIBER_DUMP_OPAQUE_TILES:
+            // The reference clears the tiles when no opaque depth is bound.
+            bytes = (uint64_t)c->camera_fine_tiles * sizeof(uint2);
+            if (!h.opaque_bound) {
+                if (written) *written = bytes;
+                if (host && capacity >= bytes) std::memset(host, 0, bytes);
+                return host && capacity < bytes ? FIBER_EINVAL : FIBER_OK;
+            }
+            src = c->d_opaque.p;
+            break;
         default: return FIBER_EINVAL;
     }
     if (written) *written = bytes;

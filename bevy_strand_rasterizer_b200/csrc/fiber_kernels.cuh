@@ -79,6 +79,7 @@ struct PrepassArgs {
     uint32_t* task_mat;            // [task_capacity] material index of the task's reference
     uint2* cells_small;            // (ref base, count) of cells with 1..8 references
     uint2* cells_large;            // (ref base, count) of cells with more than 8
+    uint2* opaque_tiles;           // [camera fine tiles] (fully covered, quantised farthest opaque depth)
 };
 
 // Device buffers of the shadow, shading, raster and composite stages.
@@ -116,8 +117,11 @@ struct LaunchCtx {
     const InstanceView* inst;     // device copy
     uint32_t I, total_coarse_tiles;
     int sm_count;
+    bool opaque;                  // K0 wrote this frame's opaque fine tiles
 };
 
+void launch_opaque(const LaunchCtx& L, const PrepassArgs& A, const float* depth, uint32_t pitch, uint32_t samples,
+                   uint32_t tiles);
 void launch_broad(const LaunchCtx& L, const PrepassArgs& A);
 void launch_lut(const LaunchCtx& L, const PrepassArgs& A);
 void launch_fine(const LaunchCtx& L, const PrepassArgs& A);

@@ -2,6 +2,7 @@
 // src/nodes/prepass.rs:27-233 -> run_prepass, src/pipelines/prepass.rs:818-1397).
 //
 // Stage map (reference entry point -> kernel here):
+//   reduce_opaque_depth (opaque_depth_reduce.wgsl:36-86)                -> k_opaque_reduce
 //   broad_prepass + broad_strand_prepass (strand_prepass.wgsl:684-782) -> k_broad, folded into k_fine
 //   coarse_interval_pass + build_depth_warp_lut (:835-1014)           -> k_lut
 //   fine_prepass (:1016-1140)                                           -> k_fine (single-pass compaction)
@@ -19,6 +20,46 @@
 #include "fiber_kernels.cuh"
 
 namespace fiber {
+
+// ===========================================================================
+// K0 opaque depth reduce: per camera fine tile, whether every pixel holds
+// opaque depth (reversed-Z: > 0 after the min over the pixel's samples) and
+// the farthest such depth (the min), quantised. One warp per tile; lanes
+// stride over the tile's pixels so a warp reads whole image rows. The result
+// is a count and a min, so the lane order cannot change it.
+// ===========================================================================
+__global__ void __launch_bounds__(256) k_opaque_reduce(const FrameParams* __restrict__ Pp, PrepassArgs A,
+                                                       const float* __restrict__ depth, uint32_t pitch,
+                                                       uint32_t samples) {
+    const fiber_frustum_desc& d = Pp->frusta[0];
+    const uint32_t tx = (d.screen_width + d.froxel_size_x - 1u) / d.froxel_size_x;
+    const uint32_t ty = (d.screen_height + d.froxel_size_y - 1u) / d.froxel_size_y;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+    if (blockIdx.x == 0 && threadIdx.x == 0) A.counters->opaque_bound = 1u;
+    for (uint32_t t = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); t < tx * ty; t += warps) {
+        const uint32_t x0 = (t % tx) * d.froxel_size_x, y0 = (t / tx) * d.froxel_size_y;
+        const uint32_t w = min(x0 + d.froxel_size_x, d.screen_width) - x0;
+        const uint32_t n = w * (min(y0 + d.froxel_size_y, d.screen_height) - y0);
+        uint32_t covered = 0u;
+        float farthest = 1.0f;
+        for (uint32_t p = lane; p < n; p += 32u) {
+            const uint32_t x = x0 + p % w, y = y0 + p / w;
+            const float* px = reinterpret_cast<const float*>(reinterpret_cast<const char*>(depth) + (size_t)y * pitch) +
+                              (size_t)x * samples;
+            float z = __ldg(px);
+            for (uint32_t q = 1u; q < samples; ++q) z = wmin(z, __ldg(px + q));
+            if (z > 0.0f) {
+                ++covered;
+                farthest = wmin(farthest, z);
+            }
+        }
+        covered = __reduce_add_sync(0xFFFFFFFFu, covered);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) farthest = wmin(farthest, __shfl_xor_sync(0xFFFFFFFFu, farthest, o));
+        if (lane == 0u) A.opaque_tiles[t] = make_uint2(covered == n && n > 0u ? 1u : 0u, quantize_depth01(farthest));
+    }
+}
 
 // ===========================================================================
 // K1 broad prepass: coarse range + keep probabilities per (instance, frustum)
@@ -454,10 +495,20 @@ struct FillSink {
     }
 };
 
+// opq: the opaque fine tiles of the camera (null when none are bound).
 template <class Sink>
 __device__ __forceinline__ void walk_page(const PrepassArgs& A, F3 p0, F3 p1, const fiber_frustum_desc& d,
-                                          uint32_t tile, uint32_t local, Sink& sink) {
+                                          uint32_t tile, uint32_t local, const uint2* opq, Sink& sink) {
     uint32_t ccx = local % d.coarse_tiles_x, ccy = local / d.coarse_tiles_x;
+    // fine_tile_occluded_by_opaque (:551-573) applies to the camera only. The
+    // opaque tiles hold the camera's fine tiles alone, so the camera's
+    // fine_depth_tile_base (0) is not added.
+    if (d.kind != 0u) opq = nullptr;
+    uint32_t ftx = 0u, fty = 0u;
+    if (opq) {
+        ftx = (d.screen_width + d.froxel_size_x - 1u) / d.froxel_size_x;
+        fty = (d.screen_height + d.froxel_size_y - 1u) / d.froxel_size_y;
+    }
     uint32_t cpx = max(1u, d.froxel_size_x * kCoarseExtent);
     uint32_t cpy = max(1u, d.froxel_size_y * kCoarseExtent);
     float ox = u2f(ccx * cpx), oy = u2f(ccy * cpy);
@@ -498,9 +549,17 @@ __device__ __forceinline__ void walk_page(const PrepassArgs& A, F3 p0, F3 p1, co
         uint32_t safety = 0;
         for (;;) {
             if (safety > kCoarseExtent + kCoarseExtent + kDepthSlices + 3u) break;
-            // fine_tile_occluded_by_opaque (:551-573): no opaque depth tiles are
-            // bound on this path, so the cull never fires.
-            sink.cell((uint32_t)((fc[2] * 4 + fc[1]) * 4 + fc[0]));
+            // A covered fine tile whose farthest opaque depth is in front of
+            // this slice's nearest depth (reversed-Z: z_max) hides the cell.
+            bool occluded = false;
+            if (opq) {
+                const uint32_t fx = ccx * kCoarseExtent + (uint32_t)fc[0], fy = ccy * kCoarseExtent + (uint32_t)fc[1];
+                if (fx < ftx && fy < fty) {
+                    const uint2 o = __ldg(opq + (size_t)fy * ftx + fx);
+                    occluded = o.x != 0u && zmax <= dequantize_depth01(o.y) - 1e-4f;
+                }
+            }
+            if (!occluded) sink.cell((uint32_t)((fc[2] * 4 + fc[1]) * 4 + fc[0]));
             if (fc[0] == f1[0] && fc[1] == f1[1] && fc[2] == f1[2]) break;
             float m = wmin(wmin(tm[0], tm[1]), tm[2]);  // canonical_min_mask
             int a = tm[0] == m ? 0 : (tm[1] == m ? 1 : 2);
@@ -556,7 +615,8 @@ __device__ __forceinline__ bool task_walk(const FrameParams& P, const PrepassArg
 // Coarse-tile 2-D DDA over the task's clipped range; each coarse tile is
 // walked by walk_page.
 template <class Sink>
-__device__ __forceinline__ void walk_task(const FrameParams& P, const PrepassArgs& A, const TaskWalk& w, Sink& sink) {
+__device__ __forceinline__ void walk_task(const FrameParams& P, const PrepassArgs& A, const TaskWalk& w,
+                                          const uint2* opq, Sink& sink) {
     const fiber_frustum_desc& d = P.frusta[w.f];
     const float sw = u2f(d.screen_width), sh = u2f(d.screen_height);
     const uint32_t cpx = max(1u, d.froxel_size_x * kCoarseExtent);
@@ -586,7 +646,7 @@ __device__ __forceinline__ void walk_task(const FrameParams& P, const PrepassArg
         if (fx < (int32_t)min_cx || fx > (int32_t)max_cx || fy < (int32_t)min_cy || fy > (int32_t)max_cy) break;
         uint32_t local = (uint32_t)fy * d.coarse_tiles_x + (uint32_t)fx;
         if (local < d.coarse_depth_tile_count)
-            walk_page(A, w.p0, w.p1, d, d.coarse_depth_tile_base + local, local, sink);
+            walk_page(A, w.p0, w.p1, d, d.coarse_depth_tile_base + local, local, opq, sink);
         if (fx == ex && fy == ey) break;
         if (tx <= ty) { fx += sx; tx += ddx; } else { fy += sy; ty += ddy; }
         ++safety;
@@ -610,6 +670,9 @@ __device__ __forceinline__ bool visits_unused(const PrepassArgs& A) {
 // the rest. When the records do not fit (or slots exceed 24 bits) the pass
 // still marks every page and raises visit_overflow, which hands count and fill
 // to the walking kernels.
+// kOpaque: the frame has opaque fine tiles (K0 ran); the variant without them
+// carries no cull code.
+template <bool kOpaque>
 __global__ void __launch_bounds__(kVisitThreads, 4) k_visit(const FrameParams* __restrict__ Pp,
                                                             const InstanceView* __restrict__ inst, PrepassArgs A) {
     const FrameParams& P = *Pp;
@@ -619,6 +682,7 @@ __global__ void __launch_bounds__(kVisitThreads, 4) k_visit(const FrameParams* _
     const uint32_t n = *((volatile uint32_t*)&A.counters->tasks);
     const uint32_t n_cap = min(n, P.task_capacity);
     const bool records = P.visit_records != 0u;
+    const uint2* opq = kOpaque ? A.opaque_tiles : nullptr;
     if (!records && blockIdx.x == 0 && threadIdx.x == 0) atomicOr(&A.counters->visit_overflow, 1u);
     for (uint32_t k0 = blockIdx.x * kVisitThreads; k0 < n_cap; k0 += gridDim.x * kVisitThreads) {
         const uint32_t k = k0 + threadIdx.x;
@@ -632,7 +696,7 @@ __global__ void __launch_bounds__(kVisitThreads, 4) k_visit(const FrameParams* _
             const InstanceView& in = inst[w.i];
             A.task_key[k] = ref_sort_key((w.depths & 0xFFFFu) + (w.depths >> 16u), w.i, w.seg);
             A.task_mat[k] = w.strand < in.n_meta ? in.meta[w.strand].material_idx : 0u;
-            walk_task(P, A, w, vs);
+            walk_task(P, A, w, opq, vs);
         }
         if (!records) continue;
         uint32_t total;
@@ -657,7 +721,7 @@ __global__ void __launch_bounds__(kVisitThreads, 4) k_visit(const FrameParams* _
             }
             if (vs.n > kVisitSlots) {
                 SpillSink sp{A.visit_rec, A.visit_task, at, k, vs.n, 0u, 0u};
-                walk_task(P, A, w, sp);
+                walk_task(P, A, w, opq, sp);
             }
         }
         __syncthreads();  // s_buf and s_base are rewritten by the next round
@@ -701,22 +765,23 @@ __global__ void __launch_bounds__(256) k_fill_visits(PrepassArgs A) {
 }
 
 // K9 / K11 walking form, for frames whose visit records did not fit.
-template <int PASS>
+template <int PASS, bool kOpaque>
 __global__ void __launch_bounds__(256) k_traverse(const FrameParams* __restrict__ Pp,
                                                   const InstanceView* __restrict__ inst, PrepassArgs A) {
     if (!visits_unused(A)) return;
     const FrameParams& P = *Pp;
     const uint32_t n = *((volatile uint32_t*)&A.counters->tasks);
     const uint32_t n_cap = min(n, P.task_capacity);
+    const uint2* opq = kOpaque ? A.opaque_tiles : nullptr;
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n_cap; k += gridDim.x * blockDim.x) {
         TaskWalk w;
         if (!task_walk(P, A, k, w)) continue;
         if (PASS == kCount) {
             CountSink cs{A.page_table, A.counts, 0u};
-            walk_task(P, A, w, cs);
+            walk_task(P, A, w, opq, cs);
         } else {
             FillSink fs{&A, 0u, 0u, 0u, k};
-            walk_task(P, A, w, fs);
+            walk_task(P, A, w, opq, fs);
         }
     }
 }
@@ -1223,6 +1288,13 @@ __global__ void __launch_bounds__(256) k_sort_big_cells(PrepassArgs A) {
 // ---------------------------------------------------------------------------
 // Launch wrappers
 // ---------------------------------------------------------------------------
+void launch_opaque(const LaunchCtx& L, const PrepassArgs& A, const float* depth, uint32_t pitch, uint32_t samples,
+                   uint32_t tiles) {
+    unsigned blocks = ceil_div_host(tiles, 8);
+    if (blocks > (unsigned)L.sm_count * 16u) blocks = (unsigned)L.sm_count * 16u;
+    if (blocks == 0u) blocks = 1u;
+    k_opaque_reduce<<<blocks, 256, 0, L.stream>>>(L.P, A, depth, pitch, samples);
+}
 void launch_broad(const LaunchCtx& L, const PrepassArgs& A) {
     k_broad<<<ceil_div_host(L.I, 64), 64, 0, L.stream>>>(L.P, L.inst, A);
 }
@@ -1233,7 +1305,8 @@ void launch_fine(const LaunchCtx& L, const PrepassArgs& A) {
     k_fine<<<L.sm_count * 6, kFineThreads, 0, L.stream>>>(L.P, L.inst, A);
 }
 void launch_visit(const LaunchCtx& L, const PrepassArgs& A) {
-    k_visit<<<L.sm_count * 8, kVisitThreads, 0, L.stream>>>(L.P, L.inst, A);
+    if (L.opaque) k_visit<true><<<L.sm_count * 8, kVisitThreads, 0, L.stream>>>(L.P, L.inst, A);
+    else k_visit<false><<<L.sm_count * 8, kVisitThreads, 0, L.stream>>>(L.P, L.inst, A);
 }
 void launch_alloc(const LaunchCtx& L, const PrepassArgs& A) {
     k_alloc_pages<<<L.sm_count * 4, kScanThreads, 0, L.stream>>>(L.P, A);
@@ -1243,14 +1316,16 @@ void launch_zero_pages(const LaunchCtx& L, const PrepassArgs& A) {
 }
 void launch_count(const LaunchCtx& L, const PrepassArgs& A) {
     k_count_visits<<<L.sm_count * 8, 256, 0, L.stream>>>(A);
-    k_traverse<kCount><<<L.sm_count * 8, 256, 0, L.stream>>>(L.P, L.inst, A);
+    if (L.opaque) k_traverse<kCount, true><<<L.sm_count * 8, 256, 0, L.stream>>>(L.P, L.inst, A);
+    else k_traverse<kCount, false><<<L.sm_count * 8, 256, 0, L.stream>>>(L.P, L.inst, A);
 }
 void launch_prefix(const LaunchCtx& L, const PrepassArgs& A) {
     k_prefix_pages<<<L.sm_count * 6, 256, 0, L.stream>>>(L.P, A);
 }
 void launch_fill(const LaunchCtx& L, const PrepassArgs& A) {
     k_fill_visits<<<L.sm_count * 8, 256, 0, L.stream>>>(A);
-    k_traverse<kFill><<<L.sm_count * 8, 256, 0, L.stream>>>(L.P, L.inst, A);
+    if (L.opaque) k_traverse<kFill, true><<<L.sm_count * 8, 256, 0, L.stream>>>(L.P, L.inst, A);
+    else k_traverse<kFill, false><<<L.sm_count * 8, 256, 0, L.stream>>>(L.P, L.inst, A);
 }
 void launch_compact_active(const LaunchCtx& L, const PrepassArgs& A) {
     k_compact_active<<<L.sm_count * 4, kScanThreads, 0, L.stream>>>(L.P, A);

@@ -317,6 +317,14 @@ class StrandRasterizerPlugin:
                                              _stream_handle(stream)), "fiber_frame_begin")
 
     # Render-graph nodes ------------------------------------------------------
+    def depth_reduce(self, opaque_depth: abi.Image, samples: int = 1, stream=None):
+        """reduce_opaque_depth (src/pipelines/prepass.rs:780-815): the camera's
+        opaque depth (R32F, reversed-Z, `samples` floats per pixel) to the
+        per-fine-tile pairs the prepass culls against. Call after frame_begin,
+        before work_preparation_pass."""
+        abi.check(self.lib.fiber_opaque_depth(self.ctx, C.byref(opaque_depth), samples, _stream_handle(stream)),
+                  "fiber_opaque_depth")
+
     def work_preparation_pass(self, stream=None):
         abi.check(self.lib.fiber_prepass(self.ctx, _stream_handle(stream)), "fiber_prepass")
 
@@ -334,7 +342,15 @@ class StrandRasterizerPlugin:
                                            C.byref(scene_depth) if scene_depth is not None else None,
                                            C.byref(out), _stream_handle(stream)), "fiber_composite")
 
-    def render_nodes(self, scene_color=None, scene_depth=None, out=None, stream=None):
+    def render_nodes(self, scene_color=None, scene_depth=None, out=None, stream=None, opaque_samples: int = 1,
+                     opaque_depth=None):
+        """Every node in order. The opaque-tile reduce reads opaque_depth
+        (`opaque_samples` per pixel) when given, else scene_depth at 1 sample,
+        as the reference's prepass node reads the view's depth prepass."""
+        if opaque_depth is not None:
+            self.depth_reduce(opaque_depth, opaque_samples, stream)
+        elif scene_depth is not None:
+            self.depth_reduce(scene_depth, 1, stream)
         self.work_preparation_pass(stream)
         self.strand_shadow_rasterizer_pass(stream)
         self.strand_shading_pass(stream)

@@ -284,7 +284,9 @@ typedef enum fiber_dump_what {
     FIBER_DUMP_HISTORY = 18,      /* half[I*cap*2] shadow history (next)        */
     FIBER_DUMP_COLOR = 19,        /* half[W*H*4] strand colour (RGBA16F)        */
     FIBER_DUMP_DEPTH = 20,        /* float[W*H] strand depth                    */
-    FIBER_DUMP_FRAGMENTS = 21     /* u32[W*H] per-pixel fragment counts         */
+    FIBER_DUMP_FRAGMENTS = 21,    /* u32[W*H] per-pixel fragment counts         */
+    FIBER_DUMP_OPAQUE_TILES = 22  /* (covered u32, farthest depth q u32)[camera fine
+                                     tiles]; all zero when no opaque depth was given */
 } fiber_dump_what;
 
 typedef struct fiber_ctx fiber_ctx;
@@ -334,6 +336,18 @@ fiber_status fiber_frame_begin(fiber_ctx* ctx,
 /* ------------------------------------------------------------------------ */
 /* Render-graph node contracts (src/nodes/<node>.rs)                         */
 /* ------------------------------------------------------------------------ */
+/* reduce_opaque_depth (src/shaders/opaque_depth_reduce.wgsl:36-86, run by
+ * src/nodes/prepass.rs:111-145 before the prepass dispatches): reduces the
+ * camera's opaque depth to one (fully covered, farthest depth) pair per camera
+ * fine tile. `depth` is R32F, reversed-Z (0 = nothing drawn), the camera's
+ * width x height, with `samples` (1 or 4) consecutive floats per pixel, so a
+ * row holds width * samples floats. Call after fiber_frame_begin and before
+ * fiber_prepass; the prepass then drops the fine cells of a covered tile whose
+ * depth slice lies wholly behind the farthest opaque depth
+ * (fine_tile_occluded_by_opaque, src/shaders/strand_prepass.wgsl:551-573).
+ * A frame without this call culls nothing. fiber_frame_fused and
+ * fiber_render_host run it themselves on scene_depth (1 sample). */
+fiber_status fiber_opaque_depth(fiber_ctx* ctx, const fiber_image* depth, uint32_t samples, void* stream);
 /* work_preparation_pass (src/nodes/prepass.rs:27-233). */
 fiber_status fiber_prepass(fiber_ctx* ctx, void* stream);
 /* strand_shadow_rasterizer_pass incl. stampback (src/nodes/shadows.rs:29-221). */
@@ -348,7 +362,8 @@ fiber_status fiber_raster(fiber_ctx* ctx, uint32_t view, void* stream);
 fiber_status fiber_composite(fiber_ctx* ctx, uint32_t view, const fiber_image* scene_color,
                              const fiber_image* scene_depth, fiber_image* out, void* stream);
 /* All nodes of one frame in order, replayed from a CUDA graph after the first
- * call with the same frame shape. */
+ * call with the same frame shape. A scene_depth also feeds the opaque-tile
+ * reduce (fiber_opaque_depth at 1 sample) ahead of the prepass. */
 fiber_status fiber_frame_fused(fiber_ctx* ctx, const fiber_image* scene_color,
                                const fiber_image* scene_depth, fiber_image* out, void* stream);
 

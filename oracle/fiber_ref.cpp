@@ -280,6 +280,8 @@ struct fref_frame {
     std::vector<float> depth;
     std::vector<uint32_t> fragments;
     std::vector<float> composite;
+    std::vector<uint32_t> opaque_tiles;  // (covered, farthest q) per camera fine tile
+    bool opaque_bound = false;
     uint32_t overflow = 0;
     uint32_t n_cam_tasks = 0;
     uint64_t total_segments = 0, total_points = 0, total_strands = 0;
@@ -551,6 +553,53 @@ void stage_fine(Ctx& c) {
         if (fr->frusta[f].kind == 0u) fr->n_cam_tasks += fr->frustum_task_base[f + 1] - fr->frustum_task_base[f];
 }
 
+// ---- K0 reduce_opaque_depth (opaque_depth_reduce.wgsl:36-86) ---------------
+// depth: the camera's opaque depth, reversed-Z, `samples` floats per pixel,
+// rows of width * samples floats. Without one the tiles stay cleared
+// (src/nodes/prepass.rs:140-145) and nothing is culled.
+void stage_opaque(Ctx& c, const float* depth, uint32_t samples) {
+    fref_frame* fr = c.fr;
+    const fiber_frustum_desc& d = fr->frusta[0];  // the camera, kind 0
+    const uint32_t tx = ceil_div(d.screen_width, d.froxel_size_x), ty = ceil_div(d.screen_height, d.froxel_size_y);
+    fr->opaque_tiles.assign((size_t)tx * ty * 2, 0u);
+    fr->opaque_bound = depth != nullptr;
+    if (!depth) return;
+    for (uint32_t t = 0; t < tx * ty; ++t) {
+        const uint32_t x0 = (t % tx) * d.froxel_size_x, y0 = (t / tx) * d.froxel_size_y;
+        const uint32_t x1 = std::min(x0 + d.froxel_size_x, d.screen_width);
+        const uint32_t y1 = std::min(y0 + d.froxel_size_y, d.screen_height);
+        uint32_t covered = 0, total = 0;
+        float farthest = 1.0f;
+        for (uint32_t y = y0; y < y1; ++y) {
+            for (uint32_t x = x0; x < x1; ++x) {
+                ++total;
+                const float* px = depth + ((size_t)y * d.screen_width + x) * samples;
+                float z = px[0];
+                for (uint32_t q = 1; q < samples; ++q) z = wmin(z, px[q]);
+                if (z > 0.0f) {
+                    ++covered;
+                    farthest = wmin(farthest, z);
+                }
+            }
+        }
+        fr->opaque_tiles[(size_t)t * 2] = covered == total && total > 0u ? 1u : 0u;
+        fr->opaque_tiles[(size_t)t * 2 + 1] = quantize_depth01(farthest);
+    }
+}
+
+// fine_tile_occluded_by_opaque (strand_prepass.wgsl:551-573); the tiles hold
+// the camera's fine tiles only, whose fine_depth_tile_base is 0.
+bool fine_tile_occluded(const fref_frame* fr, const fiber_frustum_desc& d, uint32_t fx, uint32_t fy,
+                        float nearest_depth) {
+    if (!fr->opaque_bound || d.kind != 0u) return false;
+    const uint32_t tx = ceil_div(d.screen_width, d.froxel_size_x), ty = ceil_div(d.screen_height, d.froxel_size_y);
+    if (fx >= tx || fy >= ty) return false;
+    const size_t idx = (size_t)d.fine_depth_tile_base + (size_t)fy * tx + fx;
+    if (idx * 2 >= fr->opaque_tiles.size()) return false;
+    if (fr->opaque_tiles[idx * 2] == 0u) return false;
+    return nearest_depth <= dequantize_depth01(fr->opaque_tiles[idx * 2 + 1]) - 1e-4f;
+}
+
 // ---- K7/K9/K11 coarse + fine traversal (strand_prepass.wgsl:1251-1696) ------
 enum class Pass { Mark, Count, Fill };
 
@@ -655,9 +704,11 @@ struct Traverse {
             uint32_t safety = 0;
             for (;;) {
                 if (safety > kCoarseExtent + kCoarseExtent + kDepthSlices + 3u) break;
-                // Opaque fine-tile cull (fine_tile_occluded_by_opaque, :551-573):
-                // no opaque depth tiles are bound on this path, so it never culls.
-                cell(v, page, (uint32_t)fc[0], (uint32_t)fc[1], (uint32_t)fc[2]);
+                // Opaque fine-tile cull (:1539-1553 count/fill): the cell is
+                // skipped, the walk goes on. zmax is the slice's nearest depth.
+                if (!fine_tile_occluded(fr, d, ccx * kCoarseExtent + (uint32_t)fc[0],
+                                        ccy * kCoarseExtent + (uint32_t)fc[1], zmax))
+                    cell(v, page, (uint32_t)fc[0], (uint32_t)fc[1], (uint32_t)fc[2]);
                 if (fc[0] == f1[0] && fc[1] == f1[1] && fc[2] == f1[2]) break;
                 int a = min_axis(v3(tm[0], tm[1], tm[2]));
                 fc[a] += step[a];
@@ -1496,6 +1547,16 @@ fref_frame* fref_run(const fref_instance* inst, uint32_t n_inst, const fiber_fro
                      const fiber_light* lights, uint32_t n_lights, const fiber_settings* settings,
                      const fref_capacities* caps, const uint16_t* history_prev,
                      const float* scene_color, const float* scene_depth, int threads) {
+    return fref_run_opaque(inst, n_inst, camera_cfg, camera, light_cfgs, lights, n_lights, settings, caps,
+                           history_prev, scene_color, scene_depth, nullptr, 0u, threads);
+}
+
+fref_frame* fref_run_opaque(const fref_instance* inst, uint32_t n_inst, const fiber_froxel_config* camera_cfg,
+                            const fiber_camera* camera, const fiber_froxel_config* light_cfgs,
+                            const fiber_light* lights, uint32_t n_lights, const fiber_settings* settings,
+                            const fref_capacities* caps, const uint16_t* history_prev,
+                            const float* scene_color, const float* scene_depth, const float* opaque_depth,
+                            uint32_t opaque_samples, int threads) {
 #ifdef _OPENMP
     if (threads > 0) omp_set_num_threads(threads);
 #else
@@ -1543,6 +1604,7 @@ fref_frame* fref_run(const fref_instance* inst, uint32_t n_inst, const fiber_fro
     fr->S = n_lights ? (settings->shadow_map_size ? settings->shadow_map_size : fr->D) : 0u;
 
     double t0 = now_ms();
+    stage_opaque(c, opaque_depth, std::max(1u, opaque_samples));
     stage_broad(c);
     stage_lut(c);
     double t1 = now_ms();
@@ -1603,6 +1665,7 @@ uint64_t fref_get(const fref_frame* f, uint32_t what, void* host, uint64_t cap) 
         case FIBER_DUMP_COLOR: return copy_out(f->color, host, cap);
         case FIBER_DUMP_DEPTH: return copy_out(f->depth, host, cap);
         case FIBER_DUMP_FRAGMENTS: return copy_out(f->fragments, host, cap);
+        case FIBER_DUMP_OPAQUE_TILES: return copy_out(f->opaque_tiles, host, cap);
         case FREF_COMPOSITE: return copy_out(f->composite, host, cap);
         case FREF_REF_KEYS: return copy_out(f->ref_keys, host, cap);
         case FREF_STAGE_MS: {

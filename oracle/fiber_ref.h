@@ -56,6 +56,17 @@ fref_frame* fref_run(const fref_instance* inst, uint32_t n_inst,
                      const float* scene_color_rgba, const float* scene_depth,
                      int threads);
 
+/* fref_run with the camera's opaque depth for the opaque-tile reduce and cull:
+ * reversed-Z, `opaque_samples` (1 or 4) floats per pixel, rows of
+ * width * samples floats; NULL culls nothing. */
+fref_frame* fref_run_opaque(const fref_instance* inst, uint32_t n_inst,
+                            const fiber_froxel_config* camera_cfg, const fiber_camera* camera,
+                            const fiber_froxel_config* light_cfgs, const fiber_light* lights,
+                            uint32_t n_lights, const fiber_settings* settings,
+                            const fref_capacities* caps, const uint16_t* history_prev,
+                            const float* scene_color_rgba, const float* scene_depth,
+                            const float* opaque_depth, uint32_t opaque_samples, int threads);
+
 /* Copies one output (fiber_dump_what numbering, plus FREF_* extras) into
  * host; returns the byte size (host may be NULL to query). */
 uint64_t fref_get(const fref_frame* f, uint32_t what, void* host, uint64_t capacity);

@@ -60,7 +60,8 @@ def build_scene(name="tiny", frame=0, strands=None, points=None, width=None, hei
     return Scene(assets, camera_cfg, cam, light_cfgs, lights_c, st)
 
 
-def run_gpu(scene: Scene, plugin=None, fused=False, stream=None, scene_color=None, out=None):
+def run_gpu(scene: Scene, plugin=None, fused=False, stream=None, scene_color=None, out=None, scene_depth=None,
+            opaque_depth=None, opaque_samples=1):
     from bevy_strand_rasterizer_b200.plugin import StrandRasterizerPlugin
     if plugin is None:
         plugin = StrandRasterizerPlugin()
@@ -69,9 +70,10 @@ def run_gpu(scene: Scene, plugin=None, fused=False, stream=None, scene_color=Non
             plugin.add_geometry(packed, material, w)
     plugin.frame_begin_raw(scene.camera_cfg, scene.cam, scene.light_cfgs, scene.lights_c, stream)
     if fused:
-        plugin.frame_fused(scene_color, None, out, stream)
+        plugin.frame_fused(scene_color, scene_depth, out, stream)
     else:
-        plugin.render_nodes(scene_color, None, out, stream)
+        plugin.render_nodes(scene_color, scene_depth, out, stream, opaque_samples=opaque_samples,
+                            opaque_depth=opaque_depth)
     return plugin
 
 
@@ -79,6 +81,43 @@ def run_ref(scene: Scene, **kw):
     from oracle_bridge import run_oracle
     return run_oracle(scene.assets, scene.camera_cfg, scene.cam, scene.light_cfgs, scene.lights_c, scene.settings,
                       **kw)
+
+
+def opaque_plane(width: int, height: int, level: float, samples: int = 1, seed: int = 0) -> np.ndarray:
+    """A seeded opaque depth image (H, W, samples), reversed-Z: a wall at
+    `level` over the left 60% of the screen, a ramp from 0 to 2*level across
+    the bottom quarter, nothing elsewhere. With several samples one sample in
+    ~3% of the wall's pixels is left empty, so some tiles of the wall are not
+    fully covered, and the others jitter by a few ulps around the level."""
+    rng = np.random.default_rng(seed)
+    d = np.zeros((height, width, samples), np.float32)
+    d[:, : int(width * 0.6), :] = level
+    ramp = np.linspace(0.0, 2.0 * level, width, dtype=np.float32)
+    d[int(height * 0.75):, :, :] = ramp[None, :, None]
+    if samples > 1:
+        jitter = rng.integers(-3, 4, size=d.shape).astype(np.float32) * np.float32(1e-7)
+        d = np.where(d > 0, d + jitter, d).astype(np.float32)
+        holes = rng.random((height, width)) < 0.03
+        d[holes, rng.integers(0, samples)] = 0.0
+    return d
+
+
+def opaque_tiles_numpy(depth: np.ndarray, froxel: int) -> np.ndarray:
+    """reduce_opaque_depth (src/shaders/opaque_depth_reduce.wgsl:36-86) in
+    numpy: (covered, quantised farthest depth) per fine tile."""
+    h, w = depth.shape[:2]
+    z = depth.reshape(h, w, -1).min(axis=2)
+    ty, tx = -(-h // froxel), -(-w // froxel)
+    out = np.zeros((ty * tx, 2), np.uint32)
+    for t in range(ty * tx):
+        y0, x0 = (t // tx) * froxel, (t % tx) * froxel
+        blk = z[y0:y0 + froxel, x0:x0 + froxel]
+        cov = blk > 0
+        far = np.float32(min(1.0, float(blk[cov].min()))) if cov.any() else np.float32(1.0)
+        out[t, 0] = 1 if cov.all() else 0
+        # quantize_depth01: the product rounds to f32 first, then to even
+        out[t, 1] = np.uint32(np.rint(np.float32(np.clip(far, 0, 1)) * np.float32(16777215.0)))
+    return out
 
 
 def psnr(a: np.ndarray, b: np.ndarray, peak: float = 1.0) -> float:

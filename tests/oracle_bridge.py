@@ -54,6 +54,8 @@ def oracle_lib():
                                  C.POINTER(abi.Camera), C.POINTER(abi.FroxelConfigC), C.POINTER(abi.Light),
                                  C.c_uint32, C.POINTER(abi.Settings), C.POINTER(FrefCaps), C.c_void_p, C.c_void_p,
                                  C.c_void_p, C.c_int]
+        lib.fref_run_opaque.restype = C.c_void_p
+        lib.fref_run_opaque.argtypes = lib.fref_run.argtypes[:-1] + [C.c_void_p, C.c_uint32, C.c_int]
         lib.fref_get.restype = C.c_uint64
         lib.fref_get.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint64]
         lib.fref_stats.restype = None
@@ -144,8 +146,10 @@ class OracleFrame:
 
 def run_oracle(assets, camera_cfg, cam: abi.Camera, light_cfgs, lights_c, settings: abi.Settings,
                history_prev: np.ndarray | None = None, scene_color: np.ndarray | None = None,
-               scene_depth: np.ndarray | None = None, threads: int = 0) -> OracleFrame:
-    """assets: list of (PackedStrandBuffers, StrandMaterial, world_from_local[16])."""
+               scene_depth: np.ndarray | None = None, threads: int = 0, opaque_depth: np.ndarray | None = None,
+               opaque_samples: int = 1) -> OracleFrame:
+    """assets: list of (PackedStrandBuffers, StrandMaterial, world_from_local[16]).
+    opaque_depth: the camera's opaque depth, (H, W, samples) or (H, W) float32."""
     lib = oracle_lib()
     n = len(assets)
     insts = (FrefInstance * max(1, n))()
@@ -179,8 +183,10 @@ def run_oracle(assets, camera_cfg, cam: abi.Camera, light_cfgs, lights_c, settin
     hp = None if history_prev is None else np.ascontiguousarray(history_prev.view(np.uint16))
     sc = None if scene_color is None else np.ascontiguousarray(scene_color, np.float32)
     sd = None if scene_depth is None else np.ascontiguousarray(scene_depth, np.float32)
-    h = lib.fref_run(insts, n, C.byref(camera_cfg.to_c()), C.byref(cam), cfgs, lights_c, nl, C.byref(settings),
-                     C.byref(caps), hp.ctypes.data if hp is not None else None,
-                     sc.ctypes.data if sc is not None else None, sd.ctypes.data if sd is not None else None, threads)
+    od = None if opaque_depth is None else np.ascontiguousarray(opaque_depth, np.float32)
+    h = lib.fref_run_opaque(insts, n, C.byref(camera_cfg.to_c()), C.byref(cam), cfgs, lights_c, nl,
+                            C.byref(settings), C.byref(caps), hp.ctypes.data if hp is not None else None,
+                            sc.ctypes.data if sc is not None else None, sd.ctypes.data if sd is not None else None,
+                            od.ctypes.data if od is not None else None, opaque_samples, threads)
     del keep
     return OracleFrame(h)

@@ -25,7 +25,7 @@ EXACT = [
     abi.DUMP_FRUSTA, abi.DUMP_RANGES, abi.DUMP_KEEP, abi.DUMP_LUT, abi.DUMP_TASKS, abi.DUMP_PROJECTED,
     abi.DUMP_PAGE_TABLE, abi.DUMP_PAGE_META, abi.DUMP_COUNTS, abi.DUMP_OFFSETS, abi.DUMP_REFS,
     abi.DUMP_ACTIVE_TILES, abi.DUMP_WORK, abi.DUMP_RUNS, abi.DUMP_DOM_DEPTH, abi.DUMP_DOM_OPACITY,
-    abi.DUMP_SHADOW_MAP, abi.DUMP_FRAGMENTS,
+    abi.DUMP_SHADOW_MAP, abi.DUMP_FRAGMENTS, abi.DUMP_OPAQUE_TILES,
 ]
 NAMES = {v: k for k, v in vars(abi).items() if k.startswith("DUMP_") and isinstance(v, int)}
 
@@ -55,9 +55,9 @@ def _close(gpu, ref, what, mask=None):
     return err, p
 
 
-def _compare(scene, fused=False):
-    plugin = run_gpu(scene, fused=fused)
-    ref = run_ref(scene)
+def _compare(scene, fused=False, gpu_kw=None, ref_kw=None):
+    plugin = run_gpu(scene, fused=fused, **(gpu_kw or {}))
+    ref = run_ref(scene, **(ref_kw or {}))
     s = plugin.stats()
     rs = ref.stats()
     for k in ("binning_tasks", "camera_tasks", "allocated_pages", "fine_refs", "active_tiles", "camera_runs",
@@ -113,6 +113,50 @@ def test_parity_ref_overflow():
     for what in (abi.DUMP_PAGE_META, abi.DUMP_COUNTS, abi.DUMP_ACTIVE_TILES, abi.DUMP_RUNS, abi.DUMP_WORK):
         _exact(plugin.dump(what), ref.get(what), what)
     plugin.close()
+
+
+def _depth_image(depth: np.ndarray):
+    import torch
+    t = torch.from_numpy(np.ascontiguousarray(depth, np.float32)).cuda()
+    h, w = depth.shape[:2]
+    img = abi.Image(C.c_void_p(t.data_ptr()), w, h, t[0].numel() * 4, abi.FMT_R32F)
+    return t, img
+
+
+@pytest.mark.parametrize("samples", [1, 4])
+def test_parity_opaque_depth(samples):
+    # K0 + the prepass cull: an opaque wall at the strands' median depth over
+    # part of the screen (and, at 4 samples, holes that leave tiles uncovered).
+    from common import opaque_plane
+    scene = build_scene("tiny", settings_overrides={"fragment_counts_enabled": 1})
+    cfg = scene.camera_cfg
+    depth = opaque_plane(cfg.screen_width, cfg.screen_height, 0.2, samples, seed=3)
+    keep, img = _depth_image(depth)
+    s = _compare(scene, gpu_kw=dict(opaque_depth=img, opaque_samples=samples),
+                 ref_kw=dict(opaque_depth=depth, opaque_samples=samples))
+    base = run_ref(scene).stats()
+    assert 0 < s.fine_refs < base.fine_refs
+    del keep
+
+
+def test_parity_opaque_depth_fused():
+    # fiber_frame_fused reduces its scene_depth (1 sample) ahead of the
+    # prepass; the next frame without a depth must cull nothing again.
+    from common import opaque_plane
+    scene = build_scene("tiny", settings_overrides={"fragment_counts_enabled": 1, "history_enabled": 0})
+    cfg = scene.camera_cfg
+    depth = opaque_plane(cfg.screen_width, cfg.screen_height, 0.2, 1, seed=5)[:, :, 0]
+    keep, img = _depth_image(depth)
+    _compare(scene, fused=True, gpu_kw=dict(scene_depth=img), ref_kw=dict(opaque_depth=depth))
+    p = run_gpu(scene, fused=True, scene_depth=img)
+    culled = p.stats().fine_refs
+    run_gpu(scene, plugin=p, fused=True)
+    ref = run_ref(scene)
+    assert p.stats().fine_refs == ref.stats().fine_refs > culled
+    _exact(p.dump(abi.DUMP_REFS), ref.get(abi.DUMP_REFS), abi.DUMP_REFS)
+    _exact(p.dump(abi.DUMP_OPAQUE_TILES), ref.get(abi.DUMP_OPAQUE_TILES), abi.DUMP_OPAQUE_TILES)
+    p.close()
+    del keep
 
 
 def test_fused_graph_follows_frame_shape():

@@ -78,7 +78,7 @@ def test_thread_count_independent():
     scene = build_scene("tiny", frame=11)
     a = run_ref(scene, threads=1)
     b = run_ref(scene, threads=4)
-    for w in range(22):
+    for w in range(abi.DUMP_OPAQUE_TILES + 1):
         assert np.array_equal(a.get(w).view(np.uint8), b.get(w).view(np.uint8)), w
 
 
@@ -99,3 +99,52 @@ def test_cull_off_keeps_every_segment():
     s = run_ref(scene).stats()
     # camera-only frame: every on-screen segment is a binning task and is shaded
     assert s.frustum_count == 1 and s.camera_tasks == s.binning_tasks > 0 and s.shadow_runs == 0
+
+
+@pytest.mark.parametrize("samples", [1, 4])
+def test_opaque_cull(tiny, samples):
+    """reduce_opaque_depth + fine_tile_occluded_by_opaque: the tiles match an
+    independent numpy restatement; page marks are untouched; a camera cell
+    keeps all of its references or loses all of them, exactly when its fine
+    tile is covered and its slice ends behind the farthest opaque depth; the
+    shadow frusta are untouched."""
+    from common import opaque_plane, opaque_tiles_numpy
+    scene = build_scene("tiny")
+    cfg = scene.camera_cfg
+    depth = opaque_plane(cfg.screen_width, cfg.screen_height, 0.2, samples, seed=3)
+    r = run_ref(scene, opaque_depth=depth, opaque_samples=samples)
+    tiles = r.get(abi.DUMP_OPAQUE_TILES).reshape(-1, 2)
+    assert np.array_equal(tiles, opaque_tiles_numpy(depth, cfg.froxel_size_x))
+    assert 0 < int(tiles[:, 0].sum()) < tiles.shape[0]
+    assert not tiny.get(abi.DUMP_OPAQUE_TILES).any()  # no opaque depth: cleared
+    assert np.array_equal(r.get(abi.DUMP_PAGE_TABLE), tiny.get(abi.DUMP_PAGE_TABLE))
+    s, b = r.stats(), tiny.stats()
+    assert 0 < s.fine_refs < b.fine_refs
+    assert list(s.frustum_refs)[1:] == list(b.frustum_refs)[1:]
+
+    frusta = r.get(abi.DUMP_FRUSTA)
+    cam = frusta[0]
+    lut = r.get(abi.DUMP_LUT)
+    pm = r.get(abi.DUMP_PAGE_META)
+    cc, cb = r.get(abi.DUMP_COUNTS).reshape(-1, 256), tiny.get(abi.DUMP_COUNTS).reshape(-1, 256)
+    ftx = -(-int(cam["screen_width"]) // int(cam["froxel_size_x"]))
+    fty = -(-int(cam["screen_height"]) // int(cam["froxel_size_y"]))
+    culled_cells = 0
+    for p in range(pm.shape[0]):
+        tile, z = int(pm["coarse_tile_id"][p]), int(pm["coarse_z"][p])
+        if tile >= int(cam["coarse_depth_tile_count"]):
+            assert np.array_equal(cc[p], cb[p])
+            continue
+        zmax = np.float32(lut["z_max_q"][tile * 16 + z]) / np.float32(16777215.0)
+        ccx, ccy = tile % int(cam["coarse_tiles_x"]), tile // int(cam["coarse_tiles_x"])
+        for cell in range(256):
+            fx, fy = ccx * 4 + cell % 4, ccy * 4 + (cell // 4) % 4
+            hidden = False
+            if fx < ftx and fy < fty:
+                cov, q = tiles[fy * ftx + fx]
+                far = np.float32(q) / np.float32(16777215.0)
+                hidden = bool(cov) and zmax <= np.float32(far - np.float32(1e-4))
+            want = 0 if hidden else cb[p, cell]
+            assert cc[p, cell] == want, (p, cell)
+            culled_cells += int(hidden and cb[p, cell] > 0)
+    assert culled_cells > 0
