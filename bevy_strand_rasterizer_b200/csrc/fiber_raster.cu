@@ -135,10 +135,78 @@ __device__ __forceinline__ Band make_band(float ax, float ay, float bx, float by
     return B;
 }
 
-__device__ __forceinline__ bool band_candidate(const Band& B, float px, float py) {
-    const float d = __fmaf_rn(B.nx, px, __fmaf_rn(B.ny, py, -B.c));
-    const float s = __fmaf_rn(B.ux, px, __fmaf_rn(B.uy, py, -B.cu));
-    return !(fabsf(d) > B.thr) && !(s < B.slo) && !(s > B.shi);
+// 32 x 32 bit transpose across the warp: lane i holds row i on entry, lane p
+// holds column p on return (bit i = bit p of lane i's row). Each stage swaps
+// one bit of the lane index with the same bit of the bit position.
+template <uint32_t J, uint32_t M>
+__device__ __forceinline__ uint32_t transpose_stage(uint32_t x, uint32_t lane) {
+    const uint32_t y = __shfl_xor_sync(0xFFFFFFFFu, x, J);
+    return (lane & J) ? ((x & ~M) | ((y >> J) & M)) : ((x & M) | ((y & M) << J));
+}
+__device__ __forceinline__ uint32_t warp_transpose32(uint32_t x, uint32_t lane) {
+    x = transpose_stage<16u, 0x0000FFFFu>(x, lane);
+    x = transpose_stage<8u, 0x00FF00FFu>(x, lane);
+    x = transpose_stage<4u, 0x0F0F0F0Fu>(x, lane);
+    x = transpose_stage<2u, 0x33333333u>(x, lane);
+    return transpose_stage<1u, 0x55555555u>(x, lane);
+}
+
+// Columns i (pixel centre x0 + i) of one pixel row where a linear function
+// f = f0 + g i lies in [lo, hi]: [ilo, ihi] as floats, unclamped. A slope
+// below 1e-20 makes the test the same for the whole row.
+__device__ __forceinline__ void row_interval(float f0, float g, float lo, float hi, float& ilo, float& ihi) {
+    if (fabsf(g) > 1e-20f) {
+        const float inv = 1.0f / g;
+        const float a = (lo - f0) * inv, b = (hi - f0) * inv;
+        ilo = fminf(a, b) - 1e-3f;
+        ihi = fmaxf(a, b) + 1e-3f;
+    } else {
+        const bool in = !(f0 < lo) && !(f0 > hi);
+        ilo = in ? -1.0f : 1.0f;
+        ihi = in ? 1e30f : -1.0f;
+    }
+}
+
+// Candidate bits of one 32-entry word: lane = entry (valid if v), against the
+// tile's pixel slots p = j fsx + i (p < 64), pixel centres (x0 + i, y0 + j).
+// Per pixel row the band is an interval of columns: |d| <= thr gives one
+// through the row's normal distance at column 0 and the slope nx, and
+// slo <= s <= shi another through u; their intersection sets the row's bits.
+// The 64-bit per-entry masks are then transposed to per-pixel words, written
+// to out[p]. The interval ends are widened by 1e-3 column beyond the band's
+// own slack, so the set is a superset of the per-pixel band test. An entry
+// with a non-finite band parameter (degenerate or NaN segments) is a
+// candidate of every pixel.
+__device__ __forceinline__ void candidate_word(const Band& B, bool v, float x0, float y0, uint32_t fsx, uint32_t fsy,
+                                               uint32_t lane, uint32_t* out) {
+    unsigned long long bits = 0ull;
+    if (v) {
+        const bool finite = isfinite(B.nx) && isfinite(B.ny) && isfinite(B.c) && isfinite(B.ux) && isfinite(B.uy) &&
+                            isfinite(B.cu) && isfinite(B.thr) && isfinite(B.slo) && isfinite(B.shi);
+        if (!finite) {
+            bits = ~0ull;
+        } else {
+            const uint32_t cols = min(fsx, 64u);
+            const uint32_t rows = min(fsy, (64u + fsx - 1u) / fsx);
+            const float cmax = u2f(cols - 1u);
+            for (uint32_t j = 0; j < rows; ++j) {
+                const float ys = y0 + u2f(j);
+                const float dj = __fmaf_rn(B.nx, x0, __fmaf_rn(B.ny, ys, -B.c));
+                const float sj = __fmaf_rn(B.ux, x0, __fmaf_rn(B.uy, ys, -B.cu));
+                float dlo, dhi, slo, shi;
+                row_interval(dj, B.nx, -B.thr, B.thr, dlo, dhi);
+                row_interval(sj, B.ux, B.slo, B.shi, slo, shi);
+                const float lo = fmaxf(ceilf(fmaxf(dlo, slo)), 0.0f);
+                const float hi = fminf(floorf(fminf(dhi, shi)), cmax);
+                if (lo <= hi) {
+                    const uint32_t il = f2u(lo), ih = f2u(hi);
+                    bits |= (((2ull << ih) - 1ull) & ~((1ull << il) - 1ull)) << (j * fsx);
+                }
+            }
+        }
+    }
+    out[lane] = warp_transpose32((uint32_t)bits, lane);
+    out[32u + lane] = warp_transpose32((uint32_t)(bits >> 32), lane);
 }
 
 __global__ void __launch_bounds__(kShadowThreads) k_shadow(const FrameParams* __restrict__ Pp,
@@ -154,11 +222,11 @@ __global__ void __launch_bounds__(kShadowThreads) k_shadow(const FrameParams* __
     float* srmin = sp1z + kShadowCap;
     float* srmax = srmin + kShadowCap;
     float* sabs = srmax + kShadowCap;
-    float* s_partial = sabs + kShadowCap;  // [pixel][worker][K]
+    // [worker][K][pixel]: a warp's 32 pixels hit 32 banks whatever the slice.
+    float* s_partial = sabs + kShadowCap;
     __shared__ uint32_t s_wbase[kMaxRunItems], s_wcount[kMaxRunItems], s_prefix[kMaxRunItems + 1];
     __shared__ uint32_t s_pmask[kShadowWords * kPixelSlots];  // [word][pixel] candidate bits
     __shared__ uint16_t s_item[kShadowCap];                   // run item << 2 | worker of each staged entry
-    __shared__ float2 s_pix[kPixelSlots];
     __shared__ RoundPlan s_plan;
     __shared__ uint32_t s_more, s_run;
 
@@ -167,7 +235,7 @@ __global__ void __launch_bounds__(kShadowThreads) k_shadow(const FrameParams* __
     const uint32_t K = P.K, D = P.dom_size, S = P.shadow_map_size;
     const uint32_t slot = threadIdx.x;
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-    float* partial = s_partial + (size_t)slot * 4u * K;
+    float* partial = s_partial + slot;  // partial[(w K + i) kShadowThreads]
 
     // Blocks claim runs from a counter, so long runs do not pile up on one block.
     for (;;) {
@@ -197,12 +265,11 @@ __global__ void __launch_bounds__(kShadowThreads) k_shadow(const FrameParams* __
             s_wbase[i] = wi.seg_ref_base;
             s_wcount[i] = valid_item ? wi.seg_ref_count : 0u;
         }
-        s_pix[slot] = make_float2(pfx, pfy);
+        const float x0 = u2f(tx * d.froxel_size_x) + 0.5f, y0 = u2f(ty * d.froxel_size_y) + 0.5f;
         __syncthreads();
 
         // Stage a round (projection, radii, run item and worker of each entry),
-        // then build the candidate bits: warp per 32-entry word, one ballot per
-        // pixel.
+        // then build the candidate bits: warp per 32-entry word.
         auto stage = [&](const RoundPlan& rp) {
             for (uint32_t s = threadIdx.x; s < rp.n; s += blockDim.x) {
                 uint32_t item, j;
@@ -229,12 +296,7 @@ __global__ void __launch_bounds__(kShadowThreads) k_shadow(const FrameParams* __
                 const uint32_t e = v ? s : 0u;
                 const Band B = make_band(sp0x[e], sp0y[e], sp1x[e], sp1y[e], sp0z[e], sp1z[e], srmin[e], srmax[e],
                                          tile_max);
-#pragma unroll 8
-                for (uint32_t p = 0; p < kPixelSlots; ++p) {
-                    const float2 pp = s_pix[p];
-                    const unsigned bal = __ballot_sync(0xFFFFFFFFu, v && band_candidate(B, pp.x, pp.y));
-                    if (lane == 0u) s_pmask[q * kPixelSlots + p] = bal;
-                }
+                candidate_word(B, v, x0, y0, d.froxel_size_x, d.froxel_size_y, lane, s_pmask + q * kPixelSlots);
             }
         };
 
@@ -297,7 +359,7 @@ __global__ void __launch_bounds__(kShadowThreads) k_shadow(const FrameParams* __
         const bool found = active && best != kInvalid;
 
         // ---- Pass 2: opacity partials, each covered entry into its worker's.
-        for (uint32_t i = 0; i < 4u * K; ++i) partial[i] = 0.0f;
+        for (uint32_t i = 0; i < 4u * K; ++i) partial[i * kShadowThreads] = 0.0f;
         const float alpha_z0 = found ? z0 : 1.0f;
         const float inv_span = 1.0f / wmax(1e-6f, alpha_z0);
         if (__syncthreads_or(found)) {
@@ -333,12 +395,12 @@ __global__ void __launch_bounds__(kShadowThreads) k_shadow(const FrameParams* __
                         uint32_t si = min(f2u(floorf(tl)), K - 1u);
                         float wf = tl - floorf(tl);
                         float al = cov * sabs[bi] * 0.5f;
-                        float* pw = partial + (uint32_t)(s_item[bi] & 3u) * K;
-                        float a0 = pw[si];
-                        pw[si] = wclamp(a0 + (1.0f - a0) * (1.0f - wf) * al, 0.0f, 1.0f);
+                        float* pw = partial + ((uint32_t)(s_item[bi] & 3u) * K + si) * kShadowThreads;
+                        float a0 = pw[0];
+                        pw[0] = wclamp(a0 + (1.0f - a0) * (1.0f - wf) * al, 0.0f, 1.0f);
                         if (si + 1u < K) {
-                            float a1 = pw[si + 1u];
-                            pw[si + 1u] = wclamp(a1 + (1.0f - a1) * wf * al, 0.0f, 1.0f);
+                            float a1 = pw[kShadowThreads];
+                            pw[kShadowThreads] = wclamp(a1 + (1.0f - a1) * wf * al, 0.0f, 1.0f);
                         }
                     }
                 }
@@ -357,7 +419,7 @@ __global__ void __launch_bounds__(kShadowThreads) k_shadow(const FrameParams* __
                 float acc = 0.0f;
                 for (uint32_t i = 0; i < K; ++i) {
                     float a = 0.0f;
-                    for (uint32_t wk = 0; wk < 4u; ++wk) a = a + (1.0f - a) * partial[wk * K + i];
+                    for (uint32_t wk = 0; wk < 4u; ++wk) a = a + (1.0f - a) * partial[(wk * K + i) * kShadowThreads];
                     acc = acc + (1.0f - acc) * a;  // opaque_terminal_slice = K without an opaque depth
                     R.dom_opacity[((size_t)layer * K + i) * D * D + dom_px] = acc;
                 }
@@ -410,7 +472,6 @@ __global__ void __launch_bounds__(kCamThreads) k_raster(const FrameParams* __res
     __shared__ uint2 ss0[kCamCap], ss1[kCamCap];
     __shared__ uint16_t s_item[kCamCap];
     __shared__ uint32_t s_pmask[kCamWords * kPixelSlots];  // [word][pixel] candidate bits
-    __shared__ float2 s_pix[kPixelSlots];
     __shared__ uint32_t s_wbase[kMaxRunItems], s_wcount[kMaxRunItems], s_prefix[kMaxRunItems + 1];
     __shared__ RoundPlan s_plan;
     __shared__ uint32_t s_more, s_run;
@@ -446,7 +507,7 @@ __global__ void __launch_bounds__(kCamThreads) k_raster(const FrameParams* __res
             s_wbase[i] = wi.seg_ref_base;
             s_wcount[i] = wi.seg_ref_count;
         }
-        s_pix[slot] = make_float2(pcx, pcy);
+        const float x0 = u2f(tx * d.froxel_size_x) + 0.5f, y0 = u2f(ty * d.froxel_size_y) + 0.5f;
         __syncthreads();
         float4 fin = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         float gdepth = 0.0f;
@@ -501,8 +562,8 @@ __global__ void __launch_bounds__(kCamThreads) k_raster(const FrameParams* __res
                 s_item[s] = tag;
             }
             __syncthreads();
-            // Candidate bits: warp per 32-entry word, one ballot per pixel. The
-            // radius bound uses the normalised depth the exact test clamps.
+            // Candidate bits: warp per 32-entry word. The radius bound uses the
+            // normalised depth the exact test clamps.
             const uint32_t nq = (rp.n + 31u) >> 5;
             for (uint32_t q = warp; q < nq; q += blockDim.x >> 5) {
                 const uint32_t s = q * 32u + lane;
@@ -510,12 +571,7 @@ __global__ void __launch_bounds__(kCamThreads) k_raster(const FrameParams* __res
                 const uint32_t e = v ? s : 0u;
                 const Band B = make_band(sp0x[e], sp0y[e], sp1x[e], sp1y[e], normalize_depth01(sz0[e]),
                                          normalize_depth01(sz1[e]), srmin[e], srmax[e], tile_max);
-#pragma unroll 8
-                for (uint32_t p = 0; p < kPixelSlots; ++p) {
-                    const float2 pp = s_pix[p];
-                    const unsigned bal = __ballot_sync(0xFFFFFFFFu, v && band_candidate(B, pp.x, pp.y));
-                    if (lane == 0u) s_pmask[q * kPixelSlots + p] = bal;
-                }
+                candidate_word(B, v, x0, y0, d.froxel_size_x, d.froxel_size_y, lane, s_pmask + q * kPixelSlots);
             }
             __syncthreads();
             uint32_t pos = 0u;  // next entry of this pixel's walk
