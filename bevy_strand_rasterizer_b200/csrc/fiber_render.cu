@@ -52,50 +52,64 @@ __device__ float sample_dom(const FrameParams& P, const RenderArgs& R, F3 pw, ui
     return wclamp(1.0f - op, 0.08f, 1.0f);
 }
 
-__device__ __forceinline__ float fresnel_reflectance(float eta_i, float eta_t, float cos_theta_i) {
+// fresnel_reflectance (:370-381) with eta_i = 1; ratio = 1 / eta_t is passed
+// in. The quotients use the hardware reciprocal path (__fdividef): shading is
+// compared within a tolerance, not bit for bit, and is stored as binary16.
+__device__ __forceinline__ float fresnel_reflectance(float eta_t, float ratio, float cos_theta_i) {
     float ci = fabsf(cos_theta_i);
     float cic = wclamp(0.0f, 1.0f, ci);  // WGSL clamp(0.0, 1.0, x) = min(1.0, x)
     float sin_i_sq = 1.0f - cic * cic;
-    float ratio = eta_i / eta_t;
     float cos_t = sqrtf(1.0f - ratio * ratio * sin_i_sq);
-    float rpar = ((eta_t * ci) - (eta_i * cos_t)) / ((eta_t * ci) + (eta_i * cos_t));
-    float rper = ((eta_i * ci) - (eta_t * cos_t)) / ((eta_i * ci) + (eta_t * cos_t));
+    float rpar = __fdividef((eta_t * ci) - cos_t, (eta_t * ci) + cos_t);
+    float rper = __fdividef(ci - (eta_t * cos_t), ci + (eta_t * cos_t));
     return (rpar * rpar + rper * rper) * 0.5f;
 }
 
+// gaussian_detector (:425-462) for one azimuthal width beta: the terms that
+// depend on beta alone, evaluated once per shaded segment.
+struct Detector {
+    float var, norm, neg_inv_two_var, reach;
+};
+
+__device__ __forceinline__ Detector make_detector(float beta) {
+    Detector g;
+    g.var = beta * beta;
+    const float two_var = 2.0f * g.var;
+    g.norm = 1.0f / (sqrtf(2.0f * kPi) * beta);
+    g.neg_inv_two_var = -1.0f / two_var;
+    g.reach = sqrtf(110.0f * two_var) * 1.001f + 1e-3f;
+    return g;
+}
+
 // Sum of the 21 wrapped Gaussians (k = -10..10). Terms whose exponent is below
-// -110 are exactly zero in binary32 and are skipped without changing the sum;
-// the test is written so that a NaN exponent is not skipped and still poisons
-// the sum, as exp(NaN) does in the reference. Only k with |phi - 2 pi k| below
+// -110 are zero in binary32 and are skipped without changing the sum; the test
+// is written so that a NaN exponent is not skipped and still poisons the sum,
+// as exp(NaN) does in the reference. Only k with |phi - 2 pi k| below
 // sqrt(110 * 2 var) can pass it, so the loop runs over that window (its reach
-// widened by 1e-3 relative + 1e-3 absolute, far beyond the rounding of the
-// bounds and of e), in the same increasing k order; a NaN phi takes the full
-// range.
-__device__ __forceinline__ float gaussian_detector(float beta, float phi_delta) {
-    float var = beta * beta;
-    if (var < 1e-6f) {
+// widened by 1e-3 relative + 1e-3 absolute), in the same increasing k order; a
+// NaN phi takes the full range. The exponent is a product with -1 / (2 var)
+// and exp is the hardware exp2 path (__expf), within the shading tolerance.
+__device__ __forceinline__ float gaussian_detector(const Detector& g, float phi_delta) {
+    if (g.var < 1e-6f) {
         float two_pi = 2.0f * kPi;
         float m = phi_delta - two_pi * truncf(phi_delta / two_pi);
         return fabsf(m) < 1e-3f ? 0.0f : 1e6f;
     }
-    float norm = 1.0f / (sqrtf(2.0f * kPi) * beta);
-    float two_var = 2.0f * var;
     int k0 = -10, k1 = 10;
     if (phi_delta == phi_delta) {
-        const float reach = sqrtf(110.0f * two_var) * 1.001f + 1e-3f;
         const float inv_two_pi = 1.0f / (2.0f * kPi);
-        const float lo = wclamp(floorf((phi_delta - reach) * inv_two_pi), -11.0f, 11.0f);
-        const float hi = wclamp(ceilf((phi_delta + reach) * inv_two_pi), -11.0f, 11.0f);
+        const float lo = wclamp(floorf((phi_delta - g.reach) * inv_two_pi), -11.0f, 11.0f);
+        const float hi = wclamp(ceilf((phi_delta + g.reach) * inv_two_pi), -11.0f, 11.0f);
         k0 = max(k0, (int)lo);
         k1 = min(k1, (int)hi);
     }
     float total = 0.0f;
     for (int k = k0; k <= k1; ++k) {
         float angle = phi_delta - 2.0f * kPi * (float)k;
-        float e = -angle * angle / two_var;
-        if (!(e <= -110.0f)) total = total + expf(e);
+        float e = (angle * angle) * g.neg_inv_two_var;
+        if (!(e <= -110.0f)) total = total + __expf(e);
     }
-    return norm * total;
+    return g.norm * total;
 }
 
 // Per quadrature point i, terms that depend on the root alone: h (the clamped
@@ -114,7 +128,8 @@ __device__ __forceinline__ void fill_quad_table(QuadTable& t) {
     }
 }
 
-__device__ F3 marschner(F3 L, F3 V, F3 U, const fiber_strand_material& m, float occlusion, const QuadTable& qt) {
+__device__ F3 marschner(F3 L, F3 V, F3 U, const fiber_strand_material& m, float occlusion, const QuadTable& qt,
+                        const Detector& det_azim) {
     float theta_i = acosf(dot3(L, U));
     float theta_r = acosf(dot3(L, V));
     float dUL = dot3(U, L), dVL = dot3(V, L);
@@ -125,8 +140,6 @@ __device__ F3 marschner(F3 L, F3 V, F3 U, const fiber_strand_material& m, float 
     float phi = ang * (sd > 0.0f ? 1.0f : (sd < 0.0f ? -1.0f : 0.0f));
     float sig[3] = {1.0f - m.absorption_color[0], 1.0f - m.absorption_color[1], 1.0f - m.absorption_color[2]};
     float v_long = m.alpha * m.alpha;
-    float v_azim = m.beta * m.beta;
-    float beta_azim = sqrtf(v_azim);
     float vis = wclamp(1.0f - occlusion, 0.0f, 1.0f);
     float direct = wmix(0.18f, 1.0f, vis);
     // Mp (:470-523): I0 series (5 terms) x exp(), without the csch factor.
@@ -160,6 +173,8 @@ __device__ F3 marschner(F3 L, F3 V, F3 U, const fiber_strand_material& m, float 
     float sti = sinf(theta_i);
     float ctd = cosf(theta_d);
     float eta_prime = sqrtf(wmax(0.0f, m.eta * m.eta - sti * sti)) / ctd;
+    const float inv_eta_prime = 1.0f / eta_prime;
+    const float inv_eta = 1.0f / m.eta;
     float mup[3] = {sig[0] / ctd, sig[1] / ctd, sig[2] / ctd};
     const float cos_td = ctd;  // cos(theta_d), the same evaluation
     // The quadrature point's Fresnel, absorption and azimuth terms depend on
@@ -172,12 +187,12 @@ __device__ F3 marschner(F3 L, F3 V, F3 U, const fiber_strand_material& m, float 
     for (uint32_t i = 0; i < 10u; ++i) {
         const float h = qt.h[i];
         // A (:383-413)
-        const float x_t = h / eta_prime;
+        const float x_t = h * inv_eta_prime;
         float gamma_t = asinf(x_t);
         float gamma_i = qt.gi[i];
-        float fr = fresnel_reflectance(1.0f, m.eta, acosf(cos_td * qt.cgi[i]));
-        float c2 = 1.0f + cosf(2.0f * gamma_t);
-        float T[3] = {expf(-2.0f * mup[0] * c2), expf(-2.0f * mup[1] * c2), expf(-2.0f * mup[2] * c2)};
+        float fr = fresnel_reflectance(m.eta, inv_eta, acosf(cos_td * qt.cgi[i]));
+        float c2 = 1.0f + __cosf(2.0f * gamma_t);
+        float T[3] = {__expf(-2.0f * mup[0] * c2), __expf(-2.0f * mup[1] * c2), __expf(-2.0f * mup[2] * c2)};
         float f_ = 1.0f - fr;
         // Phi (:464-468)
         float gt2 = fabsf(x_t) <= 1.0f ? gamma_t : asinf(wclamp(x_t, -1.0f, 1.0f));
@@ -194,7 +209,7 @@ __device__ F3 marschner(F3 L, F3 V, F3 U, const fiber_strand_material& m, float 
                 for (int q = 0; q < 3; ++q) A[q] = k * (T[q] * T[q]);
             }
             float shift = 2.0f * u2f(p) * gt2 - 2.0f * asin_h + u2f(p) * kPi;
-            float det = gaussian_detector(beta_azim, phi - shift);
+            float det = gaussian_detector(det_azim, phi - shift);
             for (int q = 0; q < 3; ++q) acc[p][q] = acc[p][q] + A[q] * det * c_leg_weights[i];
         }
     }
@@ -242,10 +257,11 @@ __global__ void __launch_bounds__(128, 6) k_shade(const FrameParams* __restrict_
         float vis = prev > 0.0f ? wmix(cur, prev, 0.88f) : cur;
         reinterpret_cast<__half2*>(hist_next)[hidx] = __halves2half2(__float2half_rn(vis), __float2half_rn(cur));
         float occ = 1.0f - vis;
+        const Detector det_azim = make_detector(sqrtf(mat.beta * mat.beta));
         for (uint32_t j = 0; j < P.L; ++j) {
             const float* ld = P.light_dir[j];
             F3 L = nrm3(f3(ld[0], ld[1], ld[2]));
-            F3 b = marschner(L, V, U, mat, occ, s_quad);
+            F3 b = marschner(L, V, U, mat, occ, s_quad, det_azim);
             float bb[3] = {b.x, b.y, b.z};
             for (int q = 0; q < 3; ++q) {
                 float c = bb[q] * (P.light_color[j][q] / 255.0f);
