@@ -414,17 +414,27 @@ constexpr uint32_t kVisitSlots = 32;  // buffered visits per task; p99 is about 
 constexpr uint32_t kThreadSortMax = 8;
 constexpr uint32_t kWarpSortMax = 256;
 
-__device__ __forceinline__ uint32_t lut_slice(const fiber_coarse_depth_lut_entry* e, float z) {
-    uint32_t zq = quantize_depth01(z);
-    uint32_t best = kInvalid, best_d = 0xFFFFFFFFu;
+// lut_slice for both clipped end points at once: per end point, the first
+// populated slice whose [z_min_q, z_max_q] holds its quantised depth, else the
+// first populated slice nearest to it, else kInvalid. One unrolled pass over
+// the 16 entries without an early exit, so their loads issue together.
+__device__ __forceinline__ void lut_slices(const fiber_coarse_depth_lut_entry* e, float za, float zb, uint32_t& sa,
+                                           uint32_t& sb) {
+    const uint32_t qa = quantize_depth01(za), qb = quantize_depth01(zb);
+    uint32_t fa = kInvalid, fb = kInvalid, ba = kInvalid, bb = kInvalid, da = 0xFFFFFFFFu, db = 0xFFFFFFFFu;
+#pragma unroll
     for (uint32_t i = 0; i < kDepthSlices; ++i) {
-        fiber_coarse_depth_lut_entry x = e[i];
-        if (x.virtual_count_q == 0u) continue;
-        if (zq >= x.z_min_q && zq <= x.z_max_q) return i;
-        uint32_t dist = zq > x.z_max_q ? zq - x.z_max_q : x.z_min_q - zq;
-        if (dist < best_d) { best_d = dist; best = i; }
+        const uint4 x = __ldg(reinterpret_cast<const uint4*>(e) + i);  // z_min_q, z_max_q, -, virtual_count_q
+        if (x.w == 0u) continue;
+        if (qa >= x.x && qa <= x.y && fa == kInvalid) fa = i;
+        if (qb >= x.x && qb <= x.y && fb == kInvalid) fb = i;
+        const uint32_t ea = qa > x.y ? qa - x.y : x.x - qa;  // meaningful only while nothing holds qa
+        const uint32_t eb = qb > x.y ? qb - x.y : x.x - qb;
+        if (ea < da) { da = ea; ba = i; }
+        if (eb < db) { db = eb; bb = i; }
     }
-    return best;
+    sa = fa != kInvalid ? fa : ba;
+    sb = fb != kInvalid ? fb : bb;
 }
 
 // Sinks. page_slot(pti) returns whether to walk the slot's fine cells.
@@ -518,7 +528,8 @@ __device__ __forceinline__ void walk_page(const PrepassArgs& A, F3 p0, F3 p1, co
     F3 c0, c1;
     if (!clip_segment(p0, p1, f3(ox, oy, 0.0f), bmax, c0, c1)) return;
     const fiber_coarse_depth_lut_entry* lut = A.lut + (size_t)tile * kDepthSlices;
-    uint32_t z0s = lut_slice(lut, c0.z), z1s = lut_slice(lut, c1.z);
+    uint32_t z0s, z1s;
+    lut_slices(lut, c0.z, c1.z, z0s, z1s);
     if (z0s == kInvalid || z1s == kInvalid) return;
     for (uint32_t cz = min(z0s, z1s); cz <= max(z0s, z1s); ++cz) {
         fiber_coarse_depth_lut_entry e = lut[cz];
