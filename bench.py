@@ -51,6 +51,8 @@ def parse_args():
     p.add_argument("--served-rate", type=float, default=200.0, help="Poisson arrival rate, requests/s")
     p.add_argument("--served-seconds", type=float, default=5.0, help="length of the arrival stream")
     p.add_argument("--served-saturate", type=int, default=256, help="requests submitted at once for throughput")
+    p.add_argument("--no-batched", action="store_true", help="skip the batched-mode measurement")
+    p.add_argument("--batched-views", type=int, default=64, help="independent views in one batch launch")
     return p.parse_args()
 
 
@@ -438,6 +440,8 @@ def fiber_arm(args):
     plugin.close()
     if line is not None and world == 1 and not args.no_served:
         line["served"] = served_section(args)
+    if line is not None and world == 1 and not args.no_batched:
+        line["batched"] = batched_section(args)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -497,6 +501,67 @@ def served_section(args) -> dict:
     result["sustainable_rps"] = sustain[0]
     result["frames_per_s_ratio"] = result["served"]["batch"]["frames_per_s"] / result["plain"]["batch"]["frames_per_s"]
     return result
+
+
+def batched_section(args, reps: int = 5) -> dict:
+    """The batched configuration: independent views (strands log-uniform in
+    [1k, 200k] at 16 or 32 points, 256^2 to 1080p, one light with a 512^2 to
+    2048^2 deep-opacity map) rendered by one graph launch per pass after the
+    autotuner picked the branch count and view order, against the same views
+    as a loop of plain frames (per view: frame tables, then its own frame
+    graph). Both are timed with CUDA events on one stream over `reps` passes,
+    after a warm-up pass, inputs resident on the device."""
+    import torch
+
+    from bevy_strand_rasterizer_b200 import batched
+
+    t = time.time()
+    specs = batched.batched_views(args.batched_views)
+    packed = [batched.view_strands(v) for v in specs]
+    gen_s = time.time() - t
+    t = time.time()
+    plugins = [batched.view_plugin(v, p) for v, p in zip(specs, packed)]
+    setup_s = time.time() - t
+    segments = int(sum(int(np.maximum(p.meta["count"].astype(np.int64) - 1, 0).sum()) for p in packed))
+    stream = torch.cuda.Stream()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timed(fn) -> float:
+        fn()  # warm-up pass (captures the graphs)
+        stream.synchronize()
+        ev0.record(stream)
+        for _ in range(reps):
+            fn()
+        ev1.record(stream)
+        ev1.synchronize()
+        return ev0.elapsed_time(ev1) / reps
+
+    def plain_pass():
+        for v, p in zip(specs, plugins):
+            batched.plain_frame(p, v, stream)
+
+    plain_ms = timed(plain_pass)
+    batch = batched.FiberBatch(plugins)
+    t = time.time()
+    best = batch.tune(stream)
+    tune_s = time.time() - t
+    batch_ms = timed(lambda: batch.launch(stream))
+    batch.close()
+    for p in plugins:
+        p.close()
+    n = len(specs)
+
+    def rates(ms):
+        return {"ms_per_pass": ms, "frames_per_s": n * 1e3 / ms, "segments_per_s": segments * 1e3 / ms}
+
+    return {"views": n, "segments_per_pass": segments, "strands": [v.strands for v in specs],
+            "resolutions": sorted({f"{v.camera.width}x{v.camera.height}" for v in specs}),
+            "scene_gen_s": gen_s, "setup_s": setup_s, "tune_s": tune_s, "passes": reps,
+            "plain": rates(plain_ms),
+            "batch": dict(rates(batch_ms), tuning={"branches": int(best.branches),
+                                                   "order": "lpt" if best.order else "index",
+                                                   "tuned_ms": float(best.ms)}),
+            "frames_per_s_ratio": plain_ms / batch_ms}
 
 
 def main():

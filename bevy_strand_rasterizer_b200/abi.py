@@ -160,6 +160,13 @@ DUMP_DTYPES = {
     DUMP_OPAQUE_TILES: np.dtype("<u4"),
 }
 
+BATCH_ORDER_INDEX, BATCH_ORDER_LPT = 0, 1
+
+
+class BatchTuning(C.Structure):
+    _fields_ = [("branches", u32), ("order", u32), ("ms", f32), ("pad", u32)]
+
+
 # Every symbol include/fiber.h declares (checked by tests/test_abi.py).
 EXPORTS = [
     "fiber_ctx_create", "fiber_ctx_destroy", "fiber_settings_default", "fiber_settings_set",
@@ -168,6 +175,8 @@ EXPORTS = [
     "fiber_render_host", "fiber_stats_get", "fiber_dump", "fiber_output_image", "fiber_span_count", "fiber_span_name",
     "fiber_span_times", "fiber_status_string", "fiber_server_create", "fiber_server_add_scene",
     "fiber_server_start", "fiber_server_submit", "fiber_server_wait", "fiber_server_destroy", "fiber_server_now_ns",
+    "fiber_batch_create", "fiber_batch_set_tuning", "fiber_batch_get_tuning", "fiber_batch_launch",
+    "fiber_batch_tune", "fiber_batch_destroy", "fiber_batch_plan",
     "fiber_prefix_pages_noalloc",
 ]
 
@@ -222,6 +231,13 @@ def load_library(path: Path | str | None = None) -> C.CDLL:
         "fiber_server_wait": (C.c_int, [vp, C.c_uint64, pp(ServerResult)]),
         "fiber_server_destroy": (C.c_int, [vp]),
         "fiber_server_now_ns": (C.c_uint64, []),
+        "fiber_batch_create": (C.c_int, [pp(vp), u32, pp(vp)]),
+        "fiber_batch_set_tuning": (C.c_int, [vp, pp(BatchTuning)]),
+        "fiber_batch_get_tuning": (C.c_int, [vp, pp(BatchTuning)]),
+        "fiber_batch_launch": (C.c_int, [vp, vp]),
+        "fiber_batch_tune": (C.c_int, [vp, vp, pp(BatchTuning)]),
+        "fiber_batch_destroy": (C.c_int, [vp]),
+        "fiber_batch_plan": (C.c_int, [pp(f32), u32, u32, u32, pp(u32)]),
         "fiber_prefix_pages_noalloc": (C.c_int, [vp, u32, vp, vp, vp, vp]),
     }
     for name, (res, args) in sig.items():

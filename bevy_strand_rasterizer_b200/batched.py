@@ -1,0 +1,125 @@
+"""The batched configuration: many independent views, each with its own strand
+set, camera, light and resolution, rendered by one CUDA graph launch
+(fiber_batch_*), and the same views as a loop of plain frames for comparison.
+
+Views: strand counts log-uniform in [1k, 200k] at 16 or 32 points per strand
+(straight scalp hair), a resolution from {256^2, 512^2, 1280x720, 1920x1080},
+a camera on a sphere of radius 0.4-1.0 m (upper hemisphere) looking at the
+origin, and one directional light from the upper hemisphere with a 512^2,
+1024^2 or 2048^2 deep-opacity map. The temporal shadow history is off, so a
+view's image is the same alone, in the plain loop and in the batch.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import abi
+from .plugin import FroxelConfig, PackedStrandBuffers, StrandRasterizerPlugin, _stream_handle, pack_strand_set
+from .scene import CameraSpec, LightSpec, scalp_hair
+from .served import DOM_SIZES, RESOLUTIONS, _hemisphere
+
+STRAND_RANGE = (1_000, 200_000)
+POINTS = (16, 32)
+
+
+@dataclass
+class ViewSpec:
+    strands: int
+    points: int
+    seed: int
+    camera: CameraSpec
+    camera_cfg: FroxelConfig
+    light: LightSpec
+    light_cfg: FroxelConfig
+
+
+def batched_views(n: int = 64, seed: int = 2000, strand_range=STRAND_RANGE) -> list[ViewSpec]:
+    rng = np.random.default_rng(seed)
+    lo, hi = math.log(strand_range[0]), math.log(strand_range[1])
+    views = []
+    for v in range(n):
+        strands = int(round(math.exp(rng.uniform(lo, hi))))
+        points = POINTS[int(rng.integers(0, len(POINTS)))]
+        w, h = RESOLUTIONS[int(rng.integers(0, len(RESOLUTIONS)))]
+        dom = DOM_SIZES[int(rng.integers(0, len(DOM_SIZES)))]
+        eye = _hemisphere(rng) * rng.uniform(0.4, 1.0)
+        cam = CameraSpec(eye=tuple(float(x) for x in eye), width=w, height=h)
+        light = LightSpec(tuple(float(x) for x in _hemisphere(rng)), size=dom)
+        views.append(ViewSpec(strands, points, seed + 1 + v, cam, FroxelConfig(w, h, 8, 8, 64), light,
+                              FroxelConfig(dom, dom, 8, 8, 64)))
+    return views
+
+
+def view_strands(spec: ViewSpec) -> PackedStrandBuffers:
+    return pack_strand_set(scalp_hair(spec.strands, spec.points, spec.seed))
+
+
+def view_plugin(spec: ViewSpec, packed: PackedStrandBuffers, device: int = 0, **kw) -> StrandRasterizerPlugin:
+    """A context holding the view's strand set with its frame tables uploaded."""
+    kw.setdefault("history", False)
+    kw.setdefault("dom_slices", 8)
+    p = StrandRasterizerPlugin(device=device, **kw)
+    p.add_geometry(packed)
+    p.frame_begin(spec.camera_cfg, spec.camera, [(spec.light_cfg, spec.light)])
+    return p
+
+
+def plain_frame(plugin: StrandRasterizerPlugin, spec: ViewSpec, stream=None):
+    """The plain per-view frame the batch is compared with: frame tables, then
+    the frame's nodes replayed from the context's own graph."""
+    plugin.frame_begin(spec.camera_cfg, spec.camera, [(spec.light_cfg, spec.light)], stream)
+    plugin.frame_fused(None, None, None, stream)
+
+
+class FiberBatch:
+    """fiber_batch over the contexts of `plugins` (which must outlive it)."""
+
+    def __init__(self, plugins: list[StrandRasterizerPlugin]):
+        self.lib = abi.load_library()
+        self.plugins = list(plugins)
+        arr = (C.c_void_p * len(plugins))(*[p.ctx.value for p in plugins])
+        self.handle = C.c_void_p()
+        abi.check(self.lib.fiber_batch_create(arr, len(plugins), C.byref(self.handle)), "fiber_batch_create")
+
+    def launch(self, stream):
+        abi.check(self.lib.fiber_batch_launch(self.handle, _stream_handle(stream)), "fiber_batch_launch")
+
+    def tune(self, stream) -> abi.BatchTuning:
+        best = abi.BatchTuning()
+        abi.check(self.lib.fiber_batch_tune(self.handle, _stream_handle(stream), C.byref(best)), "fiber_batch_tune")
+        return best
+
+    @property
+    def tuning(self) -> abi.BatchTuning:
+        t = abi.BatchTuning()
+        abi.check(self.lib.fiber_batch_get_tuning(self.handle, C.byref(t)), "fiber_batch_get_tuning")
+        return t
+
+    def set_tuning(self, branches: int, order: int = abi.BATCH_ORDER_INDEX):
+        t = abi.BatchTuning(branches, order, 0.0, 0)
+        abi.check(self.lib.fiber_batch_set_tuning(self.handle, C.byref(t)), "fiber_batch_set_tuning")
+
+    def close(self):
+        if self.handle:
+            self.lib.fiber_batch_destroy(self.handle)
+            self.handle = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def plan(costs, branches: int, order: int = abi.BATCH_ORDER_LPT) -> np.ndarray:
+    """fiber_batch_plan: the branch of each view (host only)."""
+    lib = abi.load_library()
+    c = np.ascontiguousarray(costs, np.float32)
+    out = np.zeros(len(c), np.uint32)
+    abi.check(lib.fiber_batch_plan(c.ctypes.data_as(C.POINTER(C.c_float)), len(c), branches, order,
+                                   out.ctypes.data_as(C.POINTER(C.c_uint32))), "fiber_batch_plan")
+    return out

@@ -14,7 +14,7 @@ from pathlib import Path
 PKG_DIR = Path(__file__).resolve().parent
 CSRC = PKG_DIR / "csrc"
 LIB_PATH = PKG_DIR / "libfiber.so"
-SOURCES = ["fiber_prepass.cu", "fiber_raster.cu", "fiber_render.cu", "fiber_ctx.cu", "fiber_server.cu", "fiber_noalloc.cu"]
+SOURCES = ["fiber_prepass.cu", "fiber_raster.cu", "fiber_render.cu", "fiber_ctx.cu", "fiber_server.cu", "fiber_batch.cu", "fiber_noalloc.cu"]
 HEADERS = ["fiber_device.cuh", "fiber_kernels.cuh", "fiber_internal.h"]
 
 NVCC_FLAGS = [

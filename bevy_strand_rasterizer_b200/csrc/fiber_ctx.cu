@@ -114,6 +114,9 @@ struct fiber_ctx {
     DevBuf d_opaque;  // (covered, farthest depth q) per camera fine tile
     uint32_t camera_fine_tiles = 0;
     bool opaque_frame = false;  // fiber_opaque_depth ran since fiber_frame_begin
+    // A batch graph advanced this context's epoch on the device: the next
+    // fiber_frame_begin clears the look-back words and restarts the epoch.
+    bool epoch_dirty = false;
     DevBuf d_dom_depth, d_dom_opacity, d_shadow_map, d_atlas, d_history[2];
     DevBuf d_color, d_depth, d_fragments, d_validate, d_host_scene, d_host_depth;
     int hist_cur = 0;
@@ -265,6 +268,42 @@ void record(fiber_ctx* c, int span, cudaStream_t s) {
 fiber_status check_launch() {
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? FIBER_OK : FIBER_ECUDA;
+}
+
+// Per-frame clears of src/plugin.rs:1145-1208 that follow the frame-table
+// upload: counters, page table, active flags, colour / depth / fragment
+// targets and the DOM depth + stampback target.
+fiber_status frame_resets(fiber_ctx* c, cudaStream_t s) {
+    const FrameParams& P = c->P;
+    const uint64_t table = (uint64_t)P.total_coarse_tiles * kDepthSlices;
+    const uint64_t W = P.width, H = P.height, L = P.L, D = P.dom_size, S = P.shadow_map_size;
+    FIBER_CUDA(cudaMemsetAsync(c->d_counters.p, 0, sizeof(FrameCounters), s));
+    FIBER_CUDA(cudaMemsetAsync(c->d_page_table.p, 0, table * 4, s));
+    FIBER_CUDA(cudaMemsetAsync(c->d_active_flags.p, 0, table * 4, s));
+    FIBER_CUDA(cudaMemsetAsync(c->d_color.p, 0, W * H * 8, s));
+    FIBER_CUDA(cudaMemsetAsync(c->d_depth.p, 0, W * H * 4, s));
+    if (P.fragment_counts) FIBER_CUDA(cudaMemsetAsync(c->d_fragments.p, 0, W * H * 4, s));
+    if (L) {
+        FIBER_CUDA(cudaMemsetAsync(c->d_dom_depth.p, 0, L * D * D * 4, s));
+        FIBER_CUDA(cudaMemsetAsync(c->d_shadow_map.p, 0, L * S * S * 4, s));
+    }
+    return FIBER_OK;
+}
+
+// The device half of fiber_frame_begin for a frame replayed from a graph: the
+// next look-back epoch (on wrap-around the status words are cleared first, as
+// the host does) and the shadow-history ping-pong flip. One block.
+__global__ void k_frame_advance(FrameParams* P, unsigned long long* lb, uint64_t lb_words) {
+    __shared__ uint32_t s_epoch;
+    if (threadIdx.x == 0) s_epoch = (P->epoch + 1u) & 0x3FFFFFFFu;
+    __syncthreads();
+    const uint32_t e = s_epoch;
+    if (e == 0u)
+        for (uint64_t i = threadIdx.x; i < lb_words; i += blockDim.x) lb[i] = 0ull;
+    if (threadIdx.x == 0) {
+        P->epoch = e == 0u ? 1u : e;
+        P->hist_in ^= 1u;
+    }
 }
 
 // The camera's opaque depth for K0: R32F rows of width * samples floats.
@@ -781,6 +820,8 @@ fiber_status fiber_frame_begin(fiber_ctx* c, const fiber_froxel_config* cam_cfg,
     ENSURE(c->d_fragments, W * H * 4, false);
 #undef ENSURE
     c->epoch = (c->epoch + 1u) & 0x3FFFFFFFu;
+    if (c->epoch_dirty) c->epoch = 0u;  // a batch graph moved the device epoch on
+    c->epoch_dirty = false;
     if (c->epoch == 0u) {  // epoch wrapped: old words could alias, clear them
         cudaMemsetAsync(c->d_lb.p, 0, c->d_lb.bytes, s);
         c->epoch = 1u;
@@ -790,16 +831,8 @@ fiber_status fiber_frame_begin(fiber_ctx* c, const fiber_froxel_config* cam_cfg,
     // Per-frame uploads and resets (src/plugin.rs:1145-1208).
     FIBER_CUDA(cudaMemcpyAsync(c->d_params.p, &P, sizeof(P), cudaMemcpyHostToDevice, s));
     if (I) FIBER_CUDA(cudaMemcpyAsync(c->d_inst.p, c->views.data(), I * sizeof(InstanceView), cudaMemcpyHostToDevice, s));
-    FIBER_CUDA(cudaMemsetAsync(c->d_counters.p, 0, sizeof(FrameCounters), s));
-    FIBER_CUDA(cudaMemsetAsync(c->d_page_table.p, 0, table * 4, s));
-    FIBER_CUDA(cudaMemsetAsync(c->d_active_flags.p, 0, fine_tiles * 4, s));
-    FIBER_CUDA(cudaMemsetAsync(c->d_color.p, 0, W * H * 8, s));
-    FIBER_CUDA(cudaMemsetAsync(c->d_depth.p, 0, W * H * 4, s));
-    if (P.fragment_counts) FIBER_CUDA(cudaMemsetAsync(c->d_fragments.p, 0, W * H * 4, s));
-    if (L) {
-        FIBER_CUDA(cudaMemsetAsync(c->d_dom_depth.p, 0, L * D * D * 4, s));
-        FIBER_CUDA(cudaMemsetAsync(c->d_shadow_map.p, 0, L * S * S * 4, s));
-    }
+    e = frame_resets(c, s);
+    if (e != FIBER_OK) return e;
     c->last_stream = s;
     c->frame_ready = true;
     c->opaque_frame = false;
@@ -1020,6 +1053,45 @@ fiber_status fiber_ctx_frame_status(fiber_ctx* c, cudaStream_t s) {
     if (w[0] != 0u) return FIBER_EOVERFLOW;
     return FIBER_OK;
 }
+
+fiber_status fiber_ctx_enqueue_frame(fiber_ctx* c, cudaStream_t s) {
+    if (!c) return FIBER_EINVAL;
+    if (!c->frame_ready) return FIBER_ENOTREADY;
+    k_frame_advance<<<1, 256, 0, s>>>(dp<FrameParams>(c->d_params), dp<unsigned long long>(c->d_lb),
+                                      (uint64_t)(c->d_lb.bytes / 8));
+    fiber_status st = check_launch();
+    if (st == FIBER_OK) st = frame_resets(c, s);
+    const int hist_before = c->hist_cur;
+    if (st == FIBER_OK) st = run_prepass(c, s);
+    if (st == FIBER_OK) st = run_shadows(c, s);
+    if (st == FIBER_OK) st = run_shading(c, s);
+    if (st == FIBER_OK) st = run_raster(c, s);
+    record(c, 13, s);
+    c->hist_cur = hist_before;  // the device flips the history in k_frame_advance
+    return st;
+}
+
+void fiber_ctx_shape_key(const fiber_ctx* c, uint64_t key[kFrameShapeWords]) {
+    const FrameParams& P = c->P;
+    key[0] = c->buffer_generation;
+    key[1] = ((uint64_t)P.I << 32) | P.total_coarse_tiles;
+    key[2] = ((uint64_t)P.K << 32) | P.L;
+    key[3] = ((uint64_t)P.width << 32) | P.height;
+    key[4] = ((uint64_t)P.dom_size << 32) | P.shadow_map_size;
+    key[5] = ((uint64_t)P.fragment_counts << 32) | (c->frame_ready ? 1u : 0u);
+}
+
+void fiber_ctx_mark_replayed(fiber_ctx* c, cudaStream_t s) {
+    c->epoch_dirty = true;
+    c->last_stream = s;  // readbacks wait for the batch launch
+}
+
+uint64_t fiber_ctx_frame_cost(const fiber_ctx* c) {
+    return c->total_segments * (uint64_t)c->P.F + (uint64_t)c->P.width * c->P.height +
+           (uint64_t)c->P.L * c->P.dom_size * c->P.dom_size;
+}
+
+int fiber_ctx_device(const fiber_ctx* c) { return c->device; }
 
 fiber_status fiber_ctx_render_host_nodes(fiber_ctx* c, const void* scene_host, void* out_host, cudaStream_t s) {
     if (!c || !scene_host || !out_host) return FIBER_EINVAL;

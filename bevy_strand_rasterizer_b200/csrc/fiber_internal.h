@@ -29,3 +29,21 @@ uint64_t fiber_ctx_allocated(const fiber_ctx* c);
 // After the frame on `s` completed: ETIMEDOUT if a bounded device wait gave
 // up, EOVERFLOW if a queue dropped work, else OK. Reads two counter words.
 fiber_status fiber_ctx_frame_status(fiber_ctx* c, cudaStream_t s);
+
+// Batched mode (fiber_batch.cu). One replayable frame of a context on `s`,
+// for capture into a batch graph: a device-side frame advance (next look-back
+// epoch, shadow-history flip), the per-frame clears, then the prepass, shadow,
+// shading and raster nodes. The frame tables are the ones the last
+// fiber_frame_begin uploaded.
+fiber_status fiber_ctx_enqueue_frame(fiber_ctx* c, cudaStream_t s);
+// What the captured launches bake in (buffers, grid sizes, clear extents); a
+// batch graph is recaptured when any of its views' keys changes.
+constexpr int kFrameShapeWords = 6;
+void fiber_ctx_shape_key(const fiber_ctx* c, uint64_t key[kFrameShapeWords]);
+// After a batch graph ran a context's frame: the host epoch no longer follows
+// the device's, so the next fiber_frame_begin restarts it; readbacks of the
+// context wait for `s`, the stream the batch ran on.
+void fiber_ctx_mark_replayed(fiber_ctx* c, cudaStream_t s);
+// Predicted frame cost: segments x frusta + camera pixels + DOM texels.
+uint64_t fiber_ctx_frame_cost(const fiber_ctx* c);
+int fiber_ctx_device(const fiber_ctx* c);

@@ -475,6 +475,55 @@ fiber_status fiber_server_destroy(fiber_server* srv);
 uint64_t fiber_server_now_ns(void);
 
 /* ------------------------------------------------------------------------ */
+/* Batched mode: many independent views rendered by one CUDA graph launch.   */
+/* No counterpart in the reference (a Bevy app records each view's nodes in  */
+/* turn); it is the batched configuration of the path's specification.       */
+/* ------------------------------------------------------------------------ */
+/* Each view is a context the caller creates and fills with the ordinary
+ * calls (fiber_settings_set, slabs, fiber_instance_set, fiber_frame_begin).
+ * fiber_batch_launch replays one frame of every view (prepass, shadows,
+ * shading, raster; no composite) from a single graph captured on first use,
+ * with the views spread over `branches` concurrent graph branches. Each
+ * replayed frame advances its look-back epoch and shadow history on the
+ * device, so replays repeat without host work per view. The graph is
+ * recaptured when a view's frame shape changes (fiber_frame_begin with new
+ * sizes, reallocated buffers) or the tuning changes. A context used in a
+ * batch may still render alone; its next fiber_frame_begin restarts its
+ * epoch. Outputs are read per view with fiber_dump / fiber_output_image. */
+typedef struct fiber_batch fiber_batch;
+
+typedef enum fiber_batch_order {
+    FIBER_BATCH_ORDER_INDEX = 0,  /* view v on branch v mod branches, in index order   */
+    FIBER_BATCH_ORDER_LPT = 1     /* longest predicted frame first, to the least loaded
+                                     branch (frame cost: segments x frusta + pixels +
+                                     DOM texels)                                        */
+} fiber_batch_order;
+
+typedef struct fiber_batch_tuning {
+    uint32_t branches;  /* concurrent graph branches, 1..32                        */
+    uint32_t order;     /* fiber_batch_order                                        */
+    float ms;           /* fiber_batch_tune: measured batch time of this choice     */
+    uint32_t pad;
+} fiber_batch_tuning;
+
+/* views: n contexts on one device, borrowed (they must outlive the batch).
+ * The initial tuning is one branch in index order. */
+fiber_status fiber_batch_create(fiber_ctx* const* views, uint32_t n, fiber_batch** out);
+fiber_status fiber_batch_set_tuning(fiber_batch* batch, const fiber_batch_tuning* tuning);
+fiber_status fiber_batch_get_tuning(const fiber_batch* batch, fiber_batch_tuning* tuning);
+/* One frame of every view; `stream` must not be the legacy stream. */
+fiber_status fiber_batch_launch(fiber_batch* batch, void* stream);
+/* The autotuner: times every branch count (powers of two up to the view
+ * count, at most 32) in both view orders over a few replays on `stream` with
+ * CUDA events, keeps the fastest and returns it. Renders those frames. */
+fiber_status fiber_batch_tune(fiber_batch* batch, void* stream, fiber_batch_tuning* best);
+fiber_status fiber_batch_destroy(fiber_batch* batch);
+/* Host only (no device): the branch of each view for the given frame costs,
+ * branch count and order, as fiber_batch_launch assigns them. */
+fiber_status fiber_batch_plan(const float* costs, uint32_t n, uint32_t branches, uint32_t order,
+                              uint32_t* assign);
+
+/* ------------------------------------------------------------------------ */
 /* Page prefix without device allocation (no counterpart in the reference)   */
 /* ------------------------------------------------------------------------ */
 /* The froxel-page prefix of fiber_prepass as a standalone call for callers
