@@ -191,6 +191,53 @@ __device__ __forceinline__ bool clip_segment(F3 p0, F3 p1, F3 bmin, F3 bmax, F3&
     return true;
 }
 
+// clip_segment with the direction's reciprocals computed once: the clips of
+// one segment against several boxes share p1 - p0 and so share them. Same
+// operations as clip_axis, so the same results bit for bit.
+struct ClipDir {
+    F3 d;
+    float inv[3];  // 1 / d per axis (unused where |d| < 1e-6)
+};
+__device__ __forceinline__ ClipDir clip_dir(F3 p0, F3 p1) {
+    ClipDir c;
+    c.d = f3(p1.x - p0.x, p1.y - p0.y, p1.z - p0.z);
+    c.inv[0] = fabsf(c.d.x) < 1e-6f ? 0.0f : 1.0f / c.d.x;
+    c.inv[1] = fabsf(c.d.y) < 1e-6f ? 0.0f : 1.0f / c.d.y;
+    c.inv[2] = fabsf(c.d.z) < 1e-6f ? 0.0f : 1.0f / c.d.z;
+    return c;
+}
+__device__ __forceinline__ bool clip_axis_pre(float p, float d, float inv_d, float mn, float mx, float& tmin,
+                                              float& tmax) {
+    if (fabsf(d) < 1e-6f) return !(p < mn || p > mx);
+    float a = (mn - p) * inv_d;
+    float b = (mx - p) * inv_d;
+    if (a > b) { float t = a; a = b; b = t; }
+    tmin = wmax(tmin, a);
+    tmax = wmin(tmax, b);
+    return !(tmin > tmax);
+}
+__device__ __forceinline__ bool clip_segment_pre(F3 p0, const ClipDir& c, F3 bmin, F3 bmax, F3& o0, F3& o1) {
+    const F3 d = c.d;
+    float tmin = 0.0f, tmax = 1.0f;
+    if (!clip_axis_pre(p0.x, d.x, c.inv[0], bmin.x, bmax.x, tmin, tmax)) return false;
+    if (!clip_axis_pre(p0.y, d.y, c.inv[1], bmin.y, bmax.y, tmin, tmax)) return false;
+    if (!clip_axis_pre(p0.z, d.z, c.inv[2], bmin.z, bmax.z, tmin, tmax)) return false;
+    o0 = f3(p0.x + d.x * tmin, p0.y + d.y * tmin, p0.z + d.z * tmin);
+    o1 = f3(p0.x + d.x * tmax, p0.y + d.y * tmax, p0.z + d.z * tmax);
+    return true;
+}
+
+// v / n in binary32. For a power of two n = 2^k both v / n and v * 2^-k are
+// the correctly rounded value of the same real number, so the product (2^-k
+// built from its exponent bits) replaces the division bit for bit.
+__device__ __forceinline__ float div_by(float v, uint32_t n) {
+    if ((n & (n - 1u)) == 0u && n != 0u && n < (1u << 31)) {
+        const int k = __ffs((int)n) - 1;
+        return v * __int_as_float((127 - k) << 23);
+    }
+    return v / u2f(n);
+}
+
 __device__ __forceinline__ uint32_t frustum_for_tile(const FrameParams& P, uint32_t tile) {
     for (uint32_t f = 0; f < P.F; ++f) {
         const fiber_frustum_desc& d = P.frusta[f];

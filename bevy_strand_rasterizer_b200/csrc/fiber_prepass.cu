@@ -505,9 +505,10 @@ struct FillSink {
     }
 };
 
-// opq: the opaque fine tiles of the camera (null when none are bound).
+// opq: the opaque fine tiles of the camera (null when none are bound); pd:
+// the segment's clip direction (p1 - p0 and its reciprocals).
 template <class Sink>
-__device__ __forceinline__ void walk_page(const PrepassArgs& A, F3 p0, F3 p1, const fiber_frustum_desc& d,
+__device__ __forceinline__ void walk_page(const PrepassArgs& A, F3 p0, const ClipDir& pd, const fiber_frustum_desc& d,
                                           uint32_t tile, uint32_t local, const uint2* opq, Sink& sink) {
     uint32_t ccx = local % d.coarse_tiles_x, ccy = local / d.coarse_tiles_x;
     // fine_tile_occluded_by_opaque (:551-573) applies to the camera only. The
@@ -526,7 +527,8 @@ __device__ __forceinline__ void walk_page(const PrepassArgs& A, F3 p0, F3 p1, co
     float tmy = wmin(oy + u2f(cpy), u2f(d.screen_height)) - 1e-3f;
     F3 bmax = f3(wmax(ox, tmx), wmax(oy, tmy), 1.0f);
     F3 c0, c1;
-    if (!clip_segment(p0, p1, f3(ox, oy, 0.0f), bmax, c0, c1)) return;
+    if (!clip_segment_pre(p0, pd, f3(ox, oy, 0.0f), bmax, c0, c1)) return;
+    const ClipDir cd = clip_dir(c0, c1);  // shared by the slice clips below
     const fiber_coarse_depth_lut_entry* lut = A.lut + (size_t)tile * kDepthSlices;
     uint32_t z0s, z1s;
     lut_slices(lut, c0.z, c1.z, z0s, z1s);
@@ -536,12 +538,14 @@ __device__ __forceinline__ void walk_page(const PrepassArgs& A, F3 p0, F3 p1, co
         if (e.virtual_count_q == 0u) continue;
         float zmin = dequantize_depth01(e.z_min_q), zmax = dequantize_depth01(e.z_max_q);
         F3 d0, d1;
-        if (!clip_segment(c0, c1, f3(ox, oy, zmin), f3(bmax.x, bmax.y, zmax), d0, d1)) continue;
+        if (!clip_segment_pre(c0, cd, f3(ox, oy, zmin), f3(bmax.x, bmax.y, zmax), d0, d1)) continue;
         if (!sink.page_slot(tile * kDepthSlices + cz)) continue;
         float zspan = wmax(zmax - zmin, 1.0f / (float)kDepthQuantMax);
-        float fsx = u2f(d.froxel_size_x), fsy = u2f(d.froxel_size_y);
-        float l0[3] = {(d0.x - ox) / fsx, (d0.y - oy) / fsy, wclamp((d0.z - zmin) / zspan, 0.0f, 0.999999f) * 16.0f};
-        float l1[3] = {(d1.x - ox) / fsx, (d1.y - oy) / fsy, wclamp((d1.z - zmin) / zspan, 0.0f, 0.999999f) * 16.0f};
+        const uint32_t fsx = d.froxel_size_x, fsy = d.froxel_size_y;
+        float l0[3] = {div_by(d0.x - ox, fsx), div_by(d0.y - oy, fsy),
+                       wclamp((d0.z - zmin) / zspan, 0.0f, 0.999999f) * 16.0f};
+        float l1[3] = {div_by(d1.x - ox, fsx), div_by(d1.y - oy, fsy),
+                       wclamp((d1.z - zmin) / zspan, 0.0f, 0.999999f) * 16.0f};
         int32_t f1[3], fc[3], step[3];
         float tm[3], dd[3];
 #pragma unroll
@@ -636,8 +640,9 @@ __device__ __forceinline__ void walk_task(const FrameParams& P, const PrepassArg
     F3 bmin = f3(u2f(min_cx * cpx), u2f(min_cy * cpy), 0.0f);
     F3 bmax = f3(wmin(u2f((max_cx + 1u) * cpx), sw) - 1e-3f, wmin(u2f((max_cy + 1u) * cpy), sh) - 1e-3f, 1.0f);
     F3 c0, c1;
-    if (!clip_segment(w.p0, w.p1, bmin, bmax, c0, c1)) return;
-    float x0 = c0.x / u2f(cpx), y0 = c0.y / u2f(cpy), x1 = c1.x / u2f(cpx), y1 = c1.y / u2f(cpy);
+    const ClipDir pd = clip_dir(w.p0, w.p1);  // shared by every coarse tile's clip
+    if (!clip_segment_pre(w.p0, pd, bmin, bmax, c0, c1)) return;
+    float x0 = div_by(c0.x, cpx), y0 = div_by(c0.y, cpy), x1 = div_by(c1.x, cpx), y1 = div_by(c1.y, cpy);
     int32_t fx = iclamp(f2i(floorf(x0)), (int32_t)min_cx, (int32_t)max_cx);
     int32_t fy = iclamp(f2i(floorf(y0)), (int32_t)min_cy, (int32_t)max_cy);
     int32_t ex = iclamp(f2i(floorf(x1)), (int32_t)min_cx, (int32_t)max_cx);
@@ -657,7 +662,7 @@ __device__ __forceinline__ void walk_task(const FrameParams& P, const PrepassArg
         if (fx < (int32_t)min_cx || fx > (int32_t)max_cx || fy < (int32_t)min_cy || fy > (int32_t)max_cy) break;
         uint32_t local = (uint32_t)fy * d.coarse_tiles_x + (uint32_t)fx;
         if (local < d.coarse_depth_tile_count)
-            walk_page(A, w.p0, w.p1, d, d.coarse_depth_tile_base + local, local, opq, sink);
+            walk_page(A, w.p0, pd, d, d.coarse_depth_tile_base + local, local, opq, sink);
         if (fx == ex && fy == ey) break;
         if (tx <= ty) { fx += sx; tx += ddx; } else { fy += sy; ty += ddy; }
         ++safety;
