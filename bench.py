@@ -52,6 +52,8 @@ def parse_args():
     p.add_argument("--served-seconds", type=float, default=5.0, help="length of the arrival stream")
     p.add_argument("--served-saturate", type=int, default=256, help="requests submitted at once for throughput")
     p.add_argument("--no-batched", action="store_true", help="skip the batched-mode measurement")
+    p.add_argument("--binning-backend", default="segment", choices=["segment", "page-csr"],
+                   help="FineBinningBackend: segment-owned scatter (default) or the page CSR")
     p.add_argument("--batched-views", type=int, default=64, help="independent views in one batch launch")
     return p.parse_args()
 
@@ -301,7 +303,10 @@ def fiber_arm(args):
         dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
 
     w, packed, material, cam_cfg, lights = make_scene(args.workload)
-    plugin = StrandRasterizerPlugin(device=local, dom_slices=w.dom_layers, ref_capacity_factor=w.ref_capacity_factor)
+    from bevy_strand_rasterizer_b200.plugin import FineBinningBackend
+    backend = FineBinningBackend.PageCsr if args.binning_backend == "page-csr" else FineBinningBackend.SegmentScatter
+    plugin = StrandRasterizerPlugin(device=local, dom_slices=w.dom_layers, ref_capacity_factor=w.ref_capacity_factor,
+                                    backend=backend)
     plugin.add_geometry(packed, material)
     stream = torch.cuda.Stream()
     H, W = w.height, w.width
@@ -420,7 +425,8 @@ def fiber_arm(args):
                                    f"{len(lights)} light(s) with {w.dom_size}^2 x {w.dom_layers} deep-opacity maps",
                        "tile_px": w.froxel, "parallelism": f"replicas x{world}",
                        "l2": "per-frame working set (tasks, refs, pages, DOM) > 126 MB L2",
-                       "stochastic_cull": "on (reference default)", "ref_capacity_factor": w.ref_capacity_factor},
+                       "stochastic_cull": "on (reference default)", "ref_capacity_factor": w.ref_capacity_factor,
+                       "fine_binning_backend": args.binning_backend},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "entry_point": "fiber_render_host", "ms_per_step": e2e_ms / args.steps},
             "roofline": {"bound": "hbm", "kernel": dom_kernel, "achieved": achieved, "peak": peak,

@@ -112,6 +112,7 @@ struct fiber_ctx {
     DevBuf d_refs, d_ref_keys, d_active_flags, d_active_list, d_work, d_runs, d_big_cells;
     DevBuf d_visit_rec, d_visit_task, d_visit_rank, d_task_key, d_task_mat, d_cells_small, d_cells_large;
     DevBuf d_opaque;  // (covered, farthest depth q) per camera fine tile
+    DevBuf d_page_nvis, d_page_vbase, d_page_bucket;  // page-CSR backend
     uint32_t camera_fine_tiles = 0;
     bool opaque_frame = false;  // fiber_opaque_depth ran since fiber_frame_begin
     // A batch graph advanced this context's epoch on the device: the next
@@ -221,6 +222,11 @@ PrepassArgs prepass_args(fiber_ctx* c) {
     A.cells_small = dp<uint2>(c->d_cells_small);
     A.cells_large = dp<uint2>(c->d_cells_large);
     A.opaque_tiles = dp<uint2>(c->d_opaque);
+    if (c->settings.fine_binning_backend == 1u) {
+        A.page_nvis = dp<uint32_t>(c->d_page_nvis);
+        A.page_vbase = dp<uint32_t>(c->d_page_vbase);
+        A.page_bucket = dp<uint2>(c->d_page_bucket);
+    }
     return A;
 }
 
@@ -331,13 +337,19 @@ fiber_status run_prepass(fiber_ctx* c, cudaStream_t s, const OpaqueSource* opaqu
     set_stage(c, A, kStageAlloc);
     launch_alloc(L, A);
     launch_zero_pages(L, A);
+    // FineBinningBackend (src/pipelines/prepass.rs:1261-1295): segment-owned
+    // count / prefix / fill, or the page CSR with page-owned cell building.
+    const bool csr = c->settings.fine_binning_backend == 1u;
     record(c, 4, s);
-    launch_count(L, A);
+    if (csr) launch_page_csr_count(L, A);
+    else launch_count(L, A);
     record(c, 5, s);
     set_stage(c, A, kStagePrefix);
-    launch_prefix(L, A);
+    launch_prefix(L, A, csr);
+    if (csr) launch_build_pages(L, A);
     record(c, 6, s);
-    launch_fill(L, A);
+    if (csr) launch_fill_walk(L, A);
+    else launch_fill(L, A);
     record(c, 7, s);
     set_stage(c, A, kStageActive);
     launch_compact_active(L, A);
@@ -505,7 +517,8 @@ fiber_status fiber_ctx_destroy(fiber_ctx* c) {
                       &c->d_history[0], &c->d_history[1], &c->d_color, &c->d_depth, &c->d_fragments,
                       &c->d_validate, &c->d_host_scene, &c->d_host_depth, &c->d_visit_rec,
                       &c->d_visit_task, &c->d_visit_rank, &c->d_task_key, &c->d_task_mat,
-                      &c->d_cells_small, &c->d_cells_large, &c->d_opaque};
+                      &c->d_cells_small, &c->d_cells_large, &c->d_opaque, &c->d_page_nvis, &c->d_page_vbase,
+                      &c->d_page_bucket};
     for (DevBuf* b : bufs) release(c, *b);
     for (int i = 0; i <= kSpanCount; ++i)
         if (c->ev[i]) cudaEventDestroy(c->ev[i]);
@@ -517,9 +530,10 @@ fiber_status fiber_settings_set(fiber_ctx* c, const fiber_settings* s) {
     if (!c || !s) return FIBER_EINVAL;
     if (s->dom_slices == 0u || s->dom_slices > 16u) return FIBER_EINVAL;
     if (s->ref_capacity_factor == 0u || s->page_capacity_divisor == 0u) return FIBER_EINVAL;
-    if (s->fine_binning_backend != 0u) return FIBER_EINVAL;  // only SegmentScatter is built
+    if (s->fine_binning_backend > 1u) return FIBER_EINVAL;  // SegmentScatter or PageCsr
     c->settings = *s;
     c->frame_ready = false;
+    c->buffer_generation++;  // the captured frame graphs follow the settings' kernel sequence
     return FIBER_OK;
 }
 
@@ -801,6 +815,11 @@ fiber_status fiber_frame_begin(fiber_ctx* c, const fiber_froxel_config* cam_cfg,
     ENSURE(c->d_cells_small, std::min<uint64_t>(ref_cap, page_cap * kPageSize) * sizeof(uint2), false);
     ENSURE(c->d_cells_large, (ref_cap / 9 + 1) * sizeof(uint2), false);
     ENSURE(c->d_opaque, (uint64_t)c->camera_fine_tiles * sizeof(uint2), false);
+    if (st.fine_binning_backend == 1u) {
+        ENSURE(c->d_page_nvis, page_cap * 4, false);
+        ENSURE(c->d_page_vbase, page_cap * 4, false);
+        ENSURE(c->d_page_bucket, visit_cap * sizeof(uint2), false);
+    }
     ENSURE(c->d_dom_depth, L * D * D * 4, false);
     ENSURE(c->d_dom_opacity, L * K * D * D * 4, true);
     ENSURE(c->d_shadow_map, L * S * S * 4, false);

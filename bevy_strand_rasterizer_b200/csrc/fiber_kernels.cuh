@@ -80,6 +80,10 @@ struct PrepassArgs {
     uint2* cells_small;            // (ref base, count) of cells with 1..8 references
     uint2* cells_large;            // (ref base, count) of cells with more than 8
     uint2* opaque_tiles;           // [camera fine tiles] (fully covered, quantised farthest opaque depth)
+    // Page-CSR backend only (null otherwise).
+    uint32_t* page_nvis;           // [page_capacity] visits per page
+    uint32_t* page_vbase;          // [page_capacity] first bucket entry of each page
+    uint2* page_bucket;            // [ref_capacity] (task, cell) of each visit, grouped by page
 };
 
 // Device buffers of the shadow, shading, raster and composite stages.
@@ -129,7 +133,10 @@ void launch_visit(const LaunchCtx& L, const PrepassArgs& A);
 void launch_alloc(const LaunchCtx& L, const PrepassArgs& A);
 void launch_zero_pages(const LaunchCtx& L, const PrepassArgs& A);
 void launch_count(const LaunchCtx& L, const PrepassArgs& A);
-void launch_prefix(const LaunchCtx& L, const PrepassArgs& A);
+void launch_prefix(const LaunchCtx& L, const PrepassArgs& A, bool csr = false);
+void launch_page_csr_count(const LaunchCtx& L, const PrepassArgs& A);
+void launch_build_pages(const LaunchCtx& L, const PrepassArgs& A);
+void launch_fill_walk(const LaunchCtx& L, const PrepassArgs& A);
 void launch_fill(const LaunchCtx& L, const PrepassArgs& A);
 void launch_compact_active(const LaunchCtx& L, const PrepassArgs& A);
 void launch_emit(const LaunchCtx& L, const PrepassArgs& A);

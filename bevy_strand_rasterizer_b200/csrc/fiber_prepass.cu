@@ -861,13 +861,73 @@ __global__ void k_zero_pages(PrepassArgs A) {
     uint4* c = reinterpret_cast<uint4*>(A.counts);
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
         c[k] = make_uint4(0u, 0u, 0u, 0u);
+    if (A.page_nvis)
+        for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < pages; k += gridDim.x * blockDim.x)
+            A.page_nvis[k] = 0u;
 }
 
 // ===========================================================================
 // K10: per page exclusive scan of the 256 cell counts; page ref bases from a
 // look-back over pages (page order); active fine-tile flags.
 // ===========================================================================
-__global__ void __launch_bounds__(256) k_prefix_pages(const FrameParams* __restrict__ Pp, PrepassArgs A) {
+
+// The page's cell offsets (this thread's cell count c in, its exclusive offset
+// out), the page's reference base from a look-back over pages in page order,
+// its metadata and overflow flag (s_flags) and base (s_pbase). Ends with a
+// block barrier.
+__device__ __forceinline__ uint32_t page_prefix(const FrameParams& P, const PrepassArgs& A, uint32_t page,
+                                                uint32_t pages, uint32_t c, uint32_t* s_warp, uint32_t& s_flags,
+                                                uint32_t& s_pbase) {
+    const size_t g = (size_t)page * kPageSize + threadIdx.x;
+    uint32_t total;
+    const uint32_t excl = block_exclusive_scan<256>(c, s_warp, total);
+    A.offsets[g] = excl;
+    A.cursors[g] = 0u;
+    uint32_t base = 0u;
+    if (threadIdx.x < 32u) base = lb_exclusive_warp(A.lb_status, page, P.epoch, total, &A.counters->error);
+    if (threadIdx.x == 0) {
+        fiber_fine_page_meta pm = A.page_meta[page];
+        uint32_t flags = 0u;
+        if (total > 0u && (uint64_t)base + total > (uint64_t)P.ref_capacity) {
+            flags = 1u;
+            atomicOr(&A.counters->overflow, 4u);
+        }
+        pm.seg_ref_base = total > 0u ? base : 0u;
+        pm.seg_ref_count = flags ? 0u : total;
+        pm.flags = flags;
+        A.page_meta[page] = pm;
+        s_flags = flags;
+        s_pbase = base;
+        if (page == pages - 1u) A.counters->refs = base + total;
+    }
+    __syncthreads();
+    return excl;
+}
+
+// append_active_fine_tile (:2207-2238) for a page: each of its 16 fine tiles
+// with a non-empty cell that lies on screen.
+__device__ __forceinline__ void page_active_tiles(const FrameParams& P, const PrepassArgs& A, uint32_t page,
+                                                  const uint32_t* s_counts) {
+    if (threadIdx.x >= 16u) return;
+    const uint32_t lt = threadIdx.x;
+    bool has = false;
+    for (uint32_t z = 0; z < kDepthSlices; ++z) has = has || s_counts[z * 16u + lt] > 0u;
+    if (!has) return;
+    fiber_fine_page_meta pm = A.page_meta[page];
+    uint32_t f = frustum_for_tile(P, pm.coarse_tile_id);
+    if (f == kInvalid) return;
+    const fiber_frustum_desc& d = P.frusta[f];
+    uint32_t lc = pm.coarse_tile_id - d.coarse_depth_tile_base;
+    uint32_t fx = (lc % d.coarse_tiles_x) * kCoarseExtent + lt % kCoarseExtent;
+    uint32_t fy = (lc / d.coarse_tiles_x) * kCoarseExtent + lt / kCoarseExtent;
+    if (fx < ceil_div(d.screen_width, d.froxel_size_x) && fy < ceil_div(d.screen_height, d.froxel_size_y))
+        A.active_flags[(size_t)pm.coarse_tile_id * 16u + lt] = 1u;
+}
+
+// csr: a page-CSR frame, where k_build_pages does this work unless the visit
+// records went unused.
+__global__ void __launch_bounds__(256) k_prefix_pages(const FrameParams* __restrict__ Pp, PrepassArgs A, bool csr) {
+    if (csr && !visits_unused(A)) return;
     const FrameParams& P = *Pp;
     __shared__ uint32_t s_tile, s_base, s_pbase, s_small, s_large;
     __shared__ uint32_t s_warp[33];
@@ -881,28 +941,7 @@ __global__ void __launch_bounds__(256) k_prefix_pages(const FrameParams* __restr
         const size_t g = (size_t)page * kPageSize + threadIdx.x;
         uint32_t c = A.counts[g];
         s_counts[threadIdx.x] = c;
-        uint32_t total;
-        uint32_t excl = block_exclusive_scan<256>(c, s_warp, total);
-        A.offsets[g] = excl;
-        A.cursors[g] = 0u;
-        uint32_t base = 0u;
-        if (threadIdx.x < 32u) base = lb_exclusive_warp(A.lb_status, page, P.epoch, total, &A.counters->error);
-        if (threadIdx.x == 0) {
-            fiber_fine_page_meta pm = A.page_meta[page];
-            uint32_t flags = 0u;
-            if (total > 0u && (uint64_t)base + total > (uint64_t)P.ref_capacity) {
-                flags = 1u;
-                atomicOr(&A.counters->overflow, 4u);
-            }
-            pm.seg_ref_base = total > 0u ? base : 0u;
-            pm.seg_ref_count = flags ? 0u : total;
-            pm.flags = flags;
-            A.page_meta[page] = pm;
-            s_base = flags;
-            s_pbase = base;
-            if (page == pages - 1u) A.counters->refs = base + total;
-        }
-        __syncthreads();
+        const uint32_t excl = page_prefix(P, A, page, pages, c, s_warp, s_base, s_pbase);
         // List the page's non-empty cells for k_sort_cells (a page that lost its
         // references lists none): up to 8 references in the small list, more in
         // the large one. One scan carries both flags (small low, large high).
@@ -920,23 +959,7 @@ __global__ void __launch_bounds__(256) k_prefix_pages(const FrameParams* __restr
             const uint32_t cb = s_pbase + excl;
             if (small) A.cells_small[s_small + (x & 0xFFFFu)] = make_uint2(cb, c);
             if (large) A.cells_large[s_large + (x >> 16)] = make_uint2(cb, c);
-        }
-        if (threadIdx.x < 16u && s_base == 0u) {
-            const uint32_t lt = threadIdx.x;
-            bool has = false;
-            for (uint32_t z = 0; z < kDepthSlices; ++z) has = has || s_counts[z * 16u + lt] > 0u;
-            if (has) {
-                fiber_fine_page_meta pm = A.page_meta[page];
-                uint32_t f = frustum_for_tile(P, pm.coarse_tile_id);
-                if (f != kInvalid) {
-                    const fiber_frustum_desc& d = P.frusta[f];
-                    uint32_t lc = pm.coarse_tile_id - d.coarse_depth_tile_base;
-                    uint32_t fx = (lc % d.coarse_tiles_x) * kCoarseExtent + lt % kCoarseExtent;
-                    uint32_t fy = (lc / d.coarse_tiles_x) * kCoarseExtent + lt / kCoarseExtent;
-                    if (fx < ceil_div(d.screen_width, d.froxel_size_x) && fy < ceil_div(d.screen_height, d.froxel_size_y))
-                        A.active_flags[(size_t)pm.coarse_tile_id * 16u + lt] = 1u;
-                }
-            }
+            page_active_tiles(P, A, page, s_counts);
         }
         __syncthreads();
     }
@@ -1181,6 +1204,22 @@ __global__ void __launch_bounds__(256) k_emit(const FrameParams* __restrict__ Pp
     }
 }
 
+// A cell longer than a warp sort: its warp writes the references in final
+// form (unsorted) and queues the cell for k_sort_big_cells.
+__device__ __forceinline__ void convert_big_cell(const PrepassArgs& A, const InstanceView* __restrict__ inst,
+                                                 uint32_t b, uint32_t n, uint32_t lane) {
+    for (uint32_t j = lane; j < n; j += 32u) {
+        unsigned long long key;
+        uint32_t mat;
+        task_entry(A, inst, A.ref_keys[b + j], key, mat);
+        store_entry(A, b + j, key, mat);
+    }
+    if (lane == 0u) {
+        const uint32_t slot = atomicAdd(&A.counters->big_cells, 1u);
+        A.big_cells[slot] = make_uint2(b, n);
+    }
+}
+
 // Canonical order inside every cell (projected depth key descending, then
 // instance, then segment), after the fill, over the cell lists k_prefix_pages
 // made: a thread per cell of up to 8 references (nearly all of them), then a
@@ -1202,17 +1241,134 @@ __global__ void __launch_bounds__(256, 4) k_sort_cells(const InstanceView* __res
         if (n <= kWarpSortMax) {
             warp_sort_any(A, inst, b, n, (int)lane);
         } else {
-            for (uint32_t j = lane; j < n; j += 32u) {
-                unsigned long long key;
-                uint32_t mat;
-                task_entry(A, inst, A.ref_keys[b + j], key, mat);
-                store_entry(A, b + j, key, mat);
-            }
-            if (lane == 0u) {
-                const uint32_t slot = atomicAdd(&A.counters->big_cells, 1u);
-                A.big_cells[slot] = make_uint2(b, n);
+            convert_big_cell(A, inst, b, n, lane);
+        }
+    }
+}
+
+// ===========================================================================
+// Page-CSR backend (FineBinningBackend::PageCsr: prefix_page_candidates,
+// scatter_page_candidates and build_fine_pages_csr, strand_prepass.wgsl:
+// 1992-2049, 2387-2507). The reference lists each page's candidate tasks and
+// traces every task again inside the page's workgroup; here the visit
+// records of k_visit already hold every (page, cell, task) visit, so they are
+// grouped by page (count, scan, scatter) and one block per page counts its
+// cells in shared memory, takes the page's reference base in page order (as
+// k_prefix_pages), fills the page's slots and sorts its cells while they are
+// in L2. The results are the canonical ones of the default backend.
+// ===========================================================================
+
+// Visits per page; each visit keeps its rank inside its page. Lanes of a warp
+// that hit the same page share one atomic.
+__global__ void __launch_bounds__(256) k_page_count(PrepassArgs A) {
+    if (visits_unused(A)) return;
+    const uint32_t n = (uint32_t)*((volatile unsigned long long*)&A.counters->visits);
+    const uint32_t lane = threadIdx.x & 31u;
+    for (uint32_t r0 = blockIdx.x * blockDim.x; r0 < n; r0 += gridDim.x * blockDim.x) {
+        const uint32_t r = r0 + threadIdx.x;
+        uint32_t page = kInvalid, cell = 0u;
+        if (r < n) {
+            const uint32_t rec = A.visit_rec[r];
+            const uint32_t h = A.page_table[rec >> 8];
+            if (h != 0u && h != kMarked) {
+                page = h - 1u;
+                cell = rec & 0xFFu;
             }
         }
+        const unsigned peers = __match_any_sync(0xFFFFFFFFu, page);
+        const uint32_t leader = (uint32_t)(__ffs(peers) - 1);
+        uint32_t base = 0u;
+        if (page != kInvalid && lane == leader) base = atomicAdd(A.page_nvis + page, (uint32_t)__popc(peers));
+        base = __shfl_sync(0xFFFFFFFFu, base, (int)leader);
+        if (r < n) {
+            A.visit_rec[r] = page == kInvalid ? kInvalid : (page << 8) | cell;
+            A.visit_rank[r] = base + (uint32_t)__popc(peers & ((1u << lane) - 1u));
+        }
+    }
+}
+
+// Exclusive scan of the per-page visit counts (one block).
+__global__ void __launch_bounds__(1024) k_page_scan(PrepassArgs A) {
+    if (visits_unused(A)) return;
+    __shared__ uint32_t s_warp[33];
+    __shared__ uint32_t s_carry;
+    const uint32_t pages = *((volatile uint32_t*)&A.counters->pages);
+    if (threadIdx.x == 0) s_carry = 0u;
+    __syncthreads();
+    for (uint32_t b = 0; b < pages; b += 1024u) {
+        const uint32_t i = b + threadIdx.x;
+        const uint32_t v = i < pages ? A.page_nvis[i] : 0u;
+        uint32_t total;
+        const uint32_t ex = block_exclusive_scan<1024>(v, s_warp, total);
+        if (i < pages) A.page_vbase[i] = s_carry + ex;
+        __syncthreads();
+        if (threadIdx.x == 0) s_carry += total;
+        __syncthreads();
+    }
+}
+
+// Visits into their page's bucket: (task, cell) at page base + rank.
+__global__ void __launch_bounds__(256) k_page_scatter(PrepassArgs A) {
+    if (visits_unused(A)) return;
+    const uint32_t n = (uint32_t)*((volatile unsigned long long*)&A.counters->visits);
+    for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+        const uint32_t rec = A.visit_rec[r];
+        if (rec == kInvalid) continue;
+        A.page_bucket[A.page_vbase[rec >> 8] + A.visit_rank[r]] = make_uint2(A.visit_task[r], rec & 0xFFu);
+    }
+}
+
+// One block per page, in page order (the look-back of the page bases).
+__global__ void __launch_bounds__(256) k_build_pages(const FrameParams* __restrict__ Pp,
+                                                     const InstanceView* __restrict__ inst, PrepassArgs A) {
+    if (visits_unused(A)) return;
+    const FrameParams& P = *Pp;
+    __shared__ uint32_t s_tile, s_flags, s_pbase, s_nlarge;
+    __shared__ uint32_t s_warp[33];
+    __shared__ uint32_t s_counts[kPageSize], s_off[kPageSize], s_cur[kPageSize];
+    __shared__ uint16_t s_large[kPageSize];
+    const uint32_t pages = *((volatile uint32_t*)&A.counters->pages);
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    for (;;) {
+        if (threadIdx.x == 0) {
+            s_tile = atomicAdd(A.tile_counter, 1u);
+            s_nlarge = 0u;
+        }
+        s_counts[threadIdx.x] = 0u;
+        s_cur[threadIdx.x] = 0u;
+        __syncthreads();
+        const uint32_t page = s_tile;
+        if (page >= pages) break;
+        const uint32_t n = A.page_nvis[page], vb = A.page_vbase[page];
+        for (uint32_t e = threadIdx.x; e < n; e += blockDim.x) atomicAdd(&s_counts[A.page_bucket[vb + e].y], 1u);
+        __syncthreads();
+        const uint32_t c = s_counts[threadIdx.x];
+        A.counts[(size_t)page * kPageSize + threadIdx.x] = c;
+        const uint32_t excl = page_prefix(P, A, page, pages, c, s_warp, s_flags, s_pbase);
+        s_off[threadIdx.x] = excl;
+        if (s_flags == 0u) {
+            __syncthreads();
+            const uint32_t pbase = s_pbase;
+            // Fill: the task index of every visit into its slot (the slots of
+            // one page are a few KB, so these writes and the sort's reads stay
+            // in L2); the order inside a cell is fixed by the sort below.
+            for (uint32_t e = threadIdx.x; e < n; e += blockDim.x) {
+                const uint2 v = A.page_bucket[vb + e];
+                A.ref_keys[pbase + s_off[v.y] + atomicAdd(&s_cur[v.y], 1u)] = v.x;
+            }
+            __syncthreads();
+            if (c >= 1u && c <= kThreadSortMax) thread_sort_cell(A, inst, pbase + excl, c);
+            else if (c > kThreadSortMax) s_large[atomicAdd(&s_nlarge, 1u)] = (uint16_t)threadIdx.x;
+            __syncthreads();
+            const uint32_t nl = s_nlarge;
+            for (uint32_t i = warp; i < nl; i += blockDim.x >> 5) {
+                const uint32_t cell = s_large[i], cb = pbase + s_off[cell], cn = s_counts[cell];
+                if (cn <= kWarpSortMax) warp_sort_any(A, inst, cb, cn, (int)lane);
+                else convert_big_cell(A, inst, cb, cn, lane);
+            }
+            page_active_tiles(P, A, page, s_counts);
+        }
+        __syncthreads();
     }
 }
 
@@ -1335,8 +1491,22 @@ void launch_count(const LaunchCtx& L, const PrepassArgs& A) {
     if (L.opaque) k_traverse<kCount, true><<<L.sm_count * 8, 256, 0, L.stream>>>(L.P, L.inst, A);
     else k_traverse<kCount, false><<<L.sm_count * 8, 256, 0, L.stream>>>(L.P, L.inst, A);
 }
-void launch_prefix(const LaunchCtx& L, const PrepassArgs& A) {
-    k_prefix_pages<<<L.sm_count * 6, 256, 0, L.stream>>>(L.P, A);
+void launch_prefix(const LaunchCtx& L, const PrepassArgs& A, bool csr) {
+    k_prefix_pages<<<L.sm_count * 6, 256, 0, L.stream>>>(L.P, A, csr);
+}
+void launch_page_csr_count(const LaunchCtx& L, const PrepassArgs& A) {
+    k_page_count<<<L.sm_count * 8, 256, 0, L.stream>>>(A);
+    if (L.opaque) k_traverse<kCount, true><<<L.sm_count * 8, 256, 0, L.stream>>>(L.P, L.inst, A);
+    else k_traverse<kCount, false><<<L.sm_count * 8, 256, 0, L.stream>>>(L.P, L.inst, A);
+    k_page_scan<<<1, 1024, 0, L.stream>>>(A);
+    k_page_scatter<<<L.sm_count * 8, 256, 0, L.stream>>>(A);
+}
+void launch_build_pages(const LaunchCtx& L, const PrepassArgs& A) {
+    k_build_pages<<<L.sm_count * 6, 256, 0, L.stream>>>(L.P, L.inst, A);
+}
+void launch_fill_walk(const LaunchCtx& L, const PrepassArgs& A) {
+    if (L.opaque) k_traverse<kFill, true><<<L.sm_count * 8, 256, 0, L.stream>>>(L.P, L.inst, A);
+    else k_traverse<kFill, false><<<L.sm_count * 8, 256, 0, L.stream>>>(L.P, L.inst, A);
 }
 void launch_fill(const LaunchCtx& L, const PrepassArgs& A) {
     k_fill_visits<<<L.sm_count * 8, 256, 0, L.stream>>>(A);

@@ -208,7 +208,7 @@ typedef struct fiber_settings {
     float min_keep_probability;         /* default 0.02                     */
     float shadow_keep_probability;      /* default 1.0                      */
     uint32_t telemetry_enabled;         /* default 0                        */
-    uint32_t fine_binning_backend;      /* 0 = SegmentScatter (only one)    */
+    uint32_t fine_binning_backend;      /* 0 = SegmentScatter, 1 = PageCsr  */
     uint32_t dom_slices;                /* deep-opacity layers K (ref 12)   */
     uint32_t shadow_map_size;           /* stampback target side; 0 = DOM   */
     float ambient_color[4];             /* Lights.ambient_color (linear)    */

@@ -86,6 +86,30 @@ def test_parity_default(name):
     assert s.binning_tasks > 0 and s.fine_refs > 0 and s.camera_runs > 0 and s.shadow_runs > 0
 
 
+@pytest.mark.parametrize("name", ["tiny", "small"])
+def test_parity_page_csr_backend(name):
+    # FineBinningBackend::PageCsr: visits grouped by page, cells built per page;
+    # the same canonical counts, offsets, refs and images as the default.
+    scene = build_scene(name, settings_overrides={"fragment_counts_enabled": 1, "fine_binning_backend": 1})
+    s = _compare(scene)
+    assert s.fine_refs > 0 and s.camera_runs > 0 and s.shadow_runs > 0
+
+
+def test_parity_page_csr_fused_and_overflow():
+    # The page CSR inside the captured frame graph, then with a reference
+    # budget too small for the visit records (the walking fallback).
+    _compare(build_scene("tiny", frame=5, settings_overrides={"fine_binning_backend": 1}), fused=True)
+    scene = build_scene("tiny", settings_overrides={"ref_capacity_factor": 1, "fine_binning_backend": 1})
+    plugin = run_gpu(scene)
+    ref = run_ref(scene)
+    s = plugin.stats(allow_overflow=True)
+    assert s.overflow_flags & 4 and ref.stats().overflow_flags & 4
+    for what in (abi.DUMP_PAGE_META, abi.DUMP_COUNTS, abi.DUMP_OFFSETS, abi.DUMP_ACTIVE_TILES, abi.DUMP_RUNS,
+                 abi.DUMP_WORK):
+        _exact(plugin.dump(what), ref.get(what), what)
+    plugin.close()
+
+
 def test_parity_fused_graph():
     scene = build_scene("tiny", settings_overrides={"fragment_counts_enabled": 1})
     _compare(scene, fused=True)
