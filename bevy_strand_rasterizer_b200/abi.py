@@ -161,6 +161,19 @@ DUMP_DTYPES = {
 }
 
 BATCH_ORDER_INDEX, BATCH_ORDER_LPT = 0, 1
+TELEMETRY_HISTOGRAM_BINS, TELEMETRY_MAX_FRUSTA = 32, 16
+
+
+class FrustumTelemetry(C.Structure):
+    _fields_ = [(n, u32) for n in ("visible_instances", "visible_strands", "retained_strands", "emitted_segments",
+                                   "allocated_pages", "page_candidates", "fine_refs", "raster_runs", "raster_load",
+                                   "max_page_candidates", "max_raster_load")]
+
+
+class Telemetry(C.Structure):
+    _fields_ = [(n, u32) for n in ("allocated_pages", "binning_tasks", "page_candidates", "fine_cell_hits",
+                                   "active_candidate_pages", "max_candidates_per_page", "frustum_count", "pad")] + [
+        ("candidate_histogram", u32 * TELEMETRY_HISTOGRAM_BINS), ("frustum", FrustumTelemetry * TELEMETRY_MAX_FRUSTA)]
 
 
 class BatchTuning(C.Structure):
@@ -172,7 +185,7 @@ EXPORTS = [
     "fiber_ctx_create", "fiber_ctx_destroy", "fiber_settings_default", "fiber_settings_set",
     "fiber_slab_alloc", "fiber_slab_upload", "fiber_slab_free", "fiber_instance_set", "fiber_frame_begin",
     "fiber_opaque_depth", "fiber_prepass", "fiber_shadows", "fiber_shading", "fiber_raster", "fiber_composite", "fiber_frame_fused",
-    "fiber_render_host", "fiber_stats_get", "fiber_dump", "fiber_output_image", "fiber_span_count", "fiber_span_name",
+    "fiber_render_host", "fiber_stats_get", "fiber_telemetry_get", "fiber_dump", "fiber_output_image", "fiber_span_count", "fiber_span_name",
     "fiber_span_times", "fiber_status_string", "fiber_server_create", "fiber_server_add_scene",
     "fiber_server_start", "fiber_server_submit", "fiber_server_wait", "fiber_server_destroy", "fiber_server_now_ns",
     "fiber_batch_create", "fiber_batch_set_tuning", "fiber_batch_get_tuning", "fiber_batch_launch",
@@ -218,6 +231,7 @@ def load_library(path: Path | str | None = None) -> C.CDLL:
         "fiber_frame_fused": (C.c_int, [vp, pp(Image), pp(Image), pp(Image), vp]),
         "fiber_render_host": (C.c_int, [vp, vp, vp, vp, vp]),
         "fiber_stats_get": (C.c_int, [vp, pp(Stats)]),
+        "fiber_telemetry_get": (C.c_int, [vp, pp(Telemetry)]),
         "fiber_dump": (C.c_int, [vp, u32, vp, C.c_uint64, pp(C.c_uint64)]),
         "fiber_output_image": (C.c_int, [vp, u32, pp(Image)]),
         "fiber_span_count": (u32, []),

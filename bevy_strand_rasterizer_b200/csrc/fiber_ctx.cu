@@ -113,6 +113,7 @@ struct fiber_ctx {
     DevBuf d_visit_rec, d_visit_task, d_visit_rank, d_task_key, d_task_mat, d_cells_small, d_cells_large;
     DevBuf d_opaque;  // (covered, farthest depth q) per camera fine tile
     DevBuf d_page_nvis, d_page_vbase, d_page_bucket;  // page-CSR backend
+    DevBuf d_tel, d_tel_slots;                         // prepass telemetry
     uint32_t camera_fine_tiles = 0;
     bool opaque_frame = false;  // fiber_opaque_depth ran since fiber_frame_begin
     // A batch graph advanced this context's epoch on the device: the next
@@ -188,6 +189,7 @@ LaunchCtx launch_ctx(fiber_ctx* c, cudaStream_t s) {
     L.total_coarse_tiles = c->P.total_coarse_tiles;
     L.sm_count = c->sm_count;
     L.opaque = c->opaque_frame;
+    L.telemetry = c->settings.telemetry_enabled != 0u;
     return L;
 }
 
@@ -222,6 +224,10 @@ PrepassArgs prepass_args(fiber_ctx* c) {
     A.cells_small = dp<uint2>(c->d_cells_small);
     A.cells_large = dp<uint2>(c->d_cells_large);
     A.opaque_tiles = dp<uint2>(c->d_opaque);
+    if (c->settings.telemetry_enabled) {
+        A.tel = dp<uint32_t>(c->d_tel);
+        A.tel_slots = dp<uint32_t>(c->d_tel_slots);
+    }
     if (c->settings.fine_binning_backend == 1u) {
         A.page_nvis = dp<uint32_t>(c->d_page_nvis);
         A.page_vbase = dp<uint32_t>(c->d_page_vbase);
@@ -293,6 +299,10 @@ fiber_status frame_resets(fiber_ctx* c, cudaStream_t s) {
         FIBER_CUDA(cudaMemsetAsync(c->d_dom_depth.p, 0, L * D * D * 4, s));
         FIBER_CUDA(cudaMemsetAsync(c->d_shadow_map.p, 0, L * S * S * 4, s));
     }
+    if (c->settings.telemetry_enabled) {
+        FIBER_CUDA(cudaMemsetAsync(c->d_tel.p, 0, sizeof(fiber_telemetry), s));
+        FIBER_CUDA(cudaMemsetAsync(c->d_tel_slots.p, 0, table * 4, s));
+    }
     return FIBER_OK;
 }
 
@@ -358,6 +368,7 @@ fiber_status run_prepass(fiber_ctx* c, cudaStream_t s, const OpaqueSource* opaqu
     launch_emit(L, A);
     launch_sort_cells(L, A);
     launch_sort_big(L, A);
+    if (L.telemetry) launch_telemetry(L, A);
     return check_launch();
 }
 
@@ -518,7 +529,7 @@ fiber_status fiber_ctx_destroy(fiber_ctx* c) {
                       &c->d_validate, &c->d_host_scene, &c->d_host_depth, &c->d_visit_rec,
                       &c->d_visit_task, &c->d_visit_rank, &c->d_task_key, &c->d_task_mat,
                       &c->d_cells_small, &c->d_cells_large, &c->d_opaque, &c->d_page_nvis, &c->d_page_vbase,
-                      &c->d_page_bucket};
+                      &c->d_page_bucket, &c->d_tel, &c->d_tel_slots};
     for (DevBuf* b : bufs) release(c, *b);
     for (int i = 0; i <= kSpanCount; ++i)
         if (c->ev[i]) cudaEventDestroy(c->ev[i]);
@@ -815,6 +826,10 @@ fiber_status fiber_frame_begin(fiber_ctx* c, const fiber_froxel_config* cam_cfg,
     ENSURE(c->d_cells_small, std::min<uint64_t>(ref_cap, page_cap * kPageSize) * sizeof(uint2), false);
     ENSURE(c->d_cells_large, (ref_cap / 9 + 1) * sizeof(uint2), false);
     ENSURE(c->d_opaque, (uint64_t)c->camera_fine_tiles * sizeof(uint2), false);
+    if (st.telemetry_enabled) {
+        ENSURE(c->d_tel, sizeof(fiber_telemetry), false);
+        ENSURE(c->d_tel_slots, table * 4, false);
+    }
     if (st.fine_binning_backend == 1u) {
         ENSURE(c->d_page_nvis, page_cap * 4, false);
         ENSURE(c->d_page_vbase, page_cap * 4, false);
@@ -1183,6 +1198,15 @@ fiber_status fiber_stats_get(fiber_ctx* c, fiber_stats* out) {
     out->total_strands = c->total_strands;
     if (h.error) return FIBER_ETIMEDOUT;
     if (h.overflow) return FIBER_EOVERFLOW;
+    return FIBER_OK;
+}
+
+fiber_status fiber_telemetry_get(fiber_ctx* c, fiber_telemetry* out) {
+    if (!c || !out) return FIBER_EINVAL;
+    if (!c->settings.telemetry_enabled || !c->d_tel.p) return FIBER_EINVAL;
+    cudaSetDevice(c->device);
+    FIBER_CUDA(cudaStreamSynchronize(c->last_stream));
+    FIBER_CUDA(cudaMemcpy(out, c->d_tel.p, sizeof(fiber_telemetry), cudaMemcpyDeviceToHost));
     return FIBER_OK;
 }
 

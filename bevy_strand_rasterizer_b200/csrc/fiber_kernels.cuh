@@ -84,7 +84,21 @@ struct PrepassArgs {
     uint32_t* page_nvis;           // [page_capacity] visits per page
     uint32_t* page_vbase;          // [page_capacity] first bucket entry of each page
     uint2* page_bucket;            // [ref_capacity] (task, cell) of each visit, grouped by page
+    // Prepass telemetry only (null otherwise): a fiber_telemetry image and the
+    // candidate tasks of every page-table slot.
+    uint32_t* tel;
+    uint32_t* tel_slots;
 };
+
+// Word offsets inside the telemetry image (the fiber_telemetry layout).
+constexpr uint32_t kTelHistogram = 8, kTelFrustum = 40, kTelFrustumStride = 11;
+enum TelFrustumField : uint32_t {
+    kTelVisibleInstances = 0, kTelVisibleStrands, kTelRetainedStrands, kTelEmittedSegments, kTelAllocatedPages,
+    kTelPageCandidates, kTelFineRefs, kTelRasterRuns, kTelRasterLoad, kTelMaxPageCandidates, kTelMaxRasterLoad
+};
+__device__ __forceinline__ uint32_t* tel_frustum(uint32_t* tel, uint32_t f, uint32_t field) {
+    return tel + kTelFrustum + f * kTelFrustumStride + field;
+}
 
 // Device buffers of the shadow, shading, raster and composite stages.
 struct RenderArgs {
@@ -122,6 +136,7 @@ struct LaunchCtx {
     uint32_t I, total_coarse_tiles;
     int sm_count;
     bool opaque;                  // K0 wrote this frame's opaque fine tiles
+    bool telemetry;               // the prepass gathers telemetry
 };
 
 void launch_opaque(const LaunchCtx& L, const PrepassArgs& A, const float* depth, uint32_t pitch, uint32_t samples,
@@ -142,6 +157,7 @@ void launch_compact_active(const LaunchCtx& L, const PrepassArgs& A);
 void launch_emit(const LaunchCtx& L, const PrepassArgs& A);
 void launch_sort_cells(const LaunchCtx& L, const PrepassArgs& A);
 void launch_sort_big(const LaunchCtx& L, const PrepassArgs& A);
+void launch_telemetry(const LaunchCtx& L, const PrepassArgs& A);
 
 void launch_shadow(const LaunchCtx& L, const RenderArgs& R, uint32_t K);
 void launch_shade(const LaunchCtx& L, const RenderArgs& R);

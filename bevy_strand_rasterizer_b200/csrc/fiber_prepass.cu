@@ -145,6 +145,10 @@ __global__ void k_broad(const FrameParams* __restrict__ Pp, const InstanceView* 
                     }
                 }
                 visible = vis || visible;
+                if (vis && A.tel) {  // FRUSTUM_TELEMETRY_VISIBLE_* (:735-738)
+                    atomicAdd(tel_frustum(A.tel, f, kTelVisibleInstances), 1u);
+                    atomicAdd(tel_frustum(A.tel, f, kTelVisibleStrands), in.strand_count);
+                }
                 if (vis) {
                     // aabb_projected_screen_area (:295-362)
                     CornerScan s = scan_corners(corners, P.clip[f], vw, vh);
@@ -341,6 +345,9 @@ __global__ void __launch_bounds__(kFineThreads) k_fine(const FrameParams* __rest
                 }
             }
         }
+        // FRUSTUM_TELEMETRY_RETAINED_STRANDS (:1085): every strand the keep
+        // tests pass (one strand per warp here).
+        if (A.tel && lane == 0 && nseg > 0u) atomicAdd(tel_frustum(A.tel, f, kTelRetainedStrands), 1u);
         // Pass A: count (results of the first 32 segments stay in registers).
         uint32_t count = 0;
         SegOut first{};
@@ -438,13 +445,18 @@ __device__ __forceinline__ void lut_slices(const fiber_coarse_depth_lut_entry* e
 }
 
 // Sinks. page_slot(pti) returns whether to walk the slot's fine cells.
+// kTel: count the task as a candidate of the slot (telemetry); a task visits
+// each slot once.
+template <bool kTel>
 struct VisitSink {
     uint32_t* page_table;
     uint32_t* buf;  // this thread's column of the block buffer (stride kVisitThreads)
     uint32_t cur, n;
     bool records;
+    uint32_t* tel_slots;
     __device__ __forceinline__ bool page_slot(uint32_t pti) {
         page_table[pti] = kMarked;
+        if (kTel) atomicAdd(tel_slots + pti, 1u);
         cur = pti << 8;
         return records;
     }
@@ -687,8 +699,8 @@ __device__ __forceinline__ bool visits_unused(const PrepassArgs& A) {
 // still marks every page and raises visit_overflow, which hands count and fill
 // to the walking kernels.
 // kOpaque: the frame has opaque fine tiles (K0 ran); the variant without them
-// carries no cull code.
-template <bool kOpaque>
+// carries no cull code. kTel: count page candidates for the telemetry.
+template <bool kOpaque, bool kTel>
 __global__ void __launch_bounds__(kVisitThreads, 4) k_visit(const FrameParams* __restrict__ Pp,
                                                             const InstanceView* __restrict__ inst, PrepassArgs A) {
     const FrameParams& P = *Pp;
@@ -704,7 +716,7 @@ __global__ void __launch_bounds__(kVisitThreads, 4) k_visit(const FrameParams* _
         const uint32_t k = k0 + threadIdx.x;
         TaskWalk w;
         const bool ok = k < n_cap && task_walk(P, A, k, w);
-        VisitSink vs{A.page_table, s_buf + threadIdx.x, 0u, 0u, records};
+        VisitSink<kTel> vs{A.page_table, s_buf + threadIdx.x, 0u, 0u, records, A.tel_slots};
         if (ok) {
             // The task's reference (make_fine_seg_ref, :1313-1327) as its sort
             // key and material, gathered later by k_sort_cells from these
@@ -1457,6 +1469,52 @@ __global__ void __launch_bounds__(256) k_sort_big_cells(PrepassArgs A) {
     }
 }
 
+// finalize_telemetry (:2145-2188): totals, per-page candidate statistics and
+// the per-frustum page, reference and raster-run sums, after the emit. The
+// candidate count of a page is the number of tasks that marked its slot.
+__global__ void __launch_bounds__(256) k_telemetry(const FrameParams* __restrict__ Pp, PrepassArgs A) {
+    const FrameParams& P = *Pp;
+    uint32_t* tel = A.tel;
+    const uint32_t pages = min(*((volatile uint32_t*)&A.counters->pages), P.page_capacity);
+    const uint32_t runs = *((volatile uint32_t*)&A.counters->active_tiles);
+    const uint32_t stride = gridDim.x * blockDim.x;
+    const uint32_t t0 = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t0 == 0) {
+        tel[0] = pages;
+        tel[1] = *((volatile uint32_t*)&A.counters->tasks);
+        tel[3] = *((volatile uint32_t*)&A.counters->refs);
+        tel[6] = P.F;
+        for (uint32_t f = 0; f < P.F && f < kMaxFrusta; ++f) {
+            const uint32_t a = A.counters->frustum_task_base[f], b = A.counters->frustum_task_base[f + 1];
+            *tel_frustum(tel, f, kTelEmittedSegments) = b - a;
+        }
+    }
+    for (uint32_t p = t0; p < pages; p += stride) {
+        const fiber_fine_page_meta pm = A.page_meta[p];
+        const uint32_t f = frustum_for_tile(P, pm.coarse_tile_id);
+        if (f != kInvalid) atomicAdd(tel_frustum(tel, f, kTelAllocatedPages), 1u);
+        const uint32_t cand = A.tel_slots[pm.coarse_tile_id * kDepthSlices + pm.coarse_z];
+        if (cand == 0u) continue;
+        atomicAdd(tel + 2, cand);
+        atomicAdd(tel + 4, 1u);
+        atomicMax(tel + 5, cand);
+        atomicAdd(tel + kTelHistogram + min(31u - (uint32_t)__clz(cand), 31u), 1u);
+        if (f != kInvalid) {
+            atomicAdd(tel_frustum(tel, f, kTelPageCandidates), cand);
+            atomicAdd(tel_frustum(tel, f, kTelFineRefs), pm.seg_ref_count);
+            atomicMax(tel_frustum(tel, f, kTelMaxPageCandidates), cand);
+        }
+    }
+    // FRUSTUM_TELEMETRY_RASTER_* (:2830-2832): every tile run with work.
+    for (uint32_t r = t0; r < runs; r += stride) {
+        const fiber_raster_tile_run run = A.runs[r];
+        if (run.work_count == 0u || run.frustum_id >= P.F) continue;
+        atomicAdd(tel_frustum(tel, run.frustum_id, kTelRasterRuns), 1u);
+        atomicAdd(tel_frustum(tel, run.frustum_id, kTelRasterLoad), run.load_score);
+        atomicMax(tel_frustum(tel, run.frustum_id, kTelMaxRasterLoad), run.load_score);
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Launch wrappers
 // ---------------------------------------------------------------------------
@@ -1477,8 +1535,14 @@ void launch_fine(const LaunchCtx& L, const PrepassArgs& A) {
     k_fine<<<L.sm_count * 6, kFineThreads, 0, L.stream>>>(L.P, L.inst, A);
 }
 void launch_visit(const LaunchCtx& L, const PrepassArgs& A) {
-    if (L.opaque) k_visit<true><<<L.sm_count * 8, kVisitThreads, 0, L.stream>>>(L.P, L.inst, A);
-    else k_visit<false><<<L.sm_count * 8, kVisitThreads, 0, L.stream>>>(L.P, L.inst, A);
+    const unsigned grid = L.sm_count * 8;
+    if (L.telemetry) {
+        if (L.opaque) k_visit<true, true><<<grid, kVisitThreads, 0, L.stream>>>(L.P, L.inst, A);
+        else k_visit<false, true><<<grid, kVisitThreads, 0, L.stream>>>(L.P, L.inst, A);
+    } else {
+        if (L.opaque) k_visit<true, false><<<grid, kVisitThreads, 0, L.stream>>>(L.P, L.inst, A);
+        else k_visit<false, false><<<grid, kVisitThreads, 0, L.stream>>>(L.P, L.inst, A);
+    }
 }
 void launch_alloc(const LaunchCtx& L, const PrepassArgs& A) {
     k_alloc_pages<<<L.sm_count * 4, kScanThreads, 0, L.stream>>>(L.P, A);
@@ -1521,6 +1585,9 @@ void launch_emit(const LaunchCtx& L, const PrepassArgs& A) {
 }
 void launch_sort_cells(const LaunchCtx& L, const PrepassArgs& A) {
     k_sort_cells<<<L.sm_count * 8, 256, 0, L.stream>>>(L.inst, A);
+}
+void launch_telemetry(const LaunchCtx& L, const PrepassArgs& A) {
+    k_telemetry<<<L.sm_count * 2, 256, 0, L.stream>>>(L.P, A);
 }
 void launch_sort_big(const LaunchCtx& L, const PrepassArgs& A) {
     static bool configured[64] = {};

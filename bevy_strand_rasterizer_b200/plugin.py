@@ -371,6 +371,13 @@ class StrandRasterizerPlugin:
         abi.check(self.lib.fiber_stats_get(self.ctx, C.byref(s)), "fiber_stats_get", allow)
         return s
 
+    def telemetry(self) -> abi.Telemetry:
+        """The last frame's prepass telemetry (the plugin must be created with
+        telemetry=PrepassTelemetrySettings(enabled=True))."""
+        t = abi.Telemetry()
+        abi.check(self.lib.fiber_telemetry_get(self.ctx, C.byref(t)), "fiber_telemetry_get")
+        return t
+
     def dump(self, what: int) -> np.ndarray:
         n = C.c_uint64()
         abi.check(self.lib.fiber_dump(self.ctx, what, None, 0, C.byref(n)), "fiber_dump(size)")

@@ -261,6 +261,38 @@ typedef struct fiber_stats {
     uint64_t total_strands;
 } fiber_stats;
 
+/* PrepassTelemetrySettings counters (src/resources.rs:77-84, collected by
+ * strand_prepass.wgsl:271-292,2145-2188, read back by
+ * src/pipelines/prepass.rs:1345-1396). Gathered only when
+ * fiber_settings.telemetry_enabled is set: they add atomics to the prepass. */
+#define FIBER_TELEMETRY_HISTOGRAM_BINS 32
+#define FIBER_TELEMETRY_MAX_FRUSTA 16
+typedef struct fiber_frustum_telemetry {
+    uint32_t visible_instances;    /* instances whose AABB reaches the frustum       */
+    uint32_t visible_strands;      /* their strand counts                            */
+    uint32_t retained_strands;     /* strands kept by the stochastic cull            */
+    uint32_t emitted_segments;     /* binning tasks                                  */
+    uint32_t allocated_pages;
+    uint32_t page_candidates;      /* (task, page) pairs over its allocated pages    */
+    uint32_t fine_refs;
+    uint32_t raster_runs;          /* tile runs with work                            */
+    uint32_t raster_load;          /* sum of the runs' load scores (references)      */
+    uint32_t max_page_candidates;
+    uint32_t max_raster_load;
+} fiber_frustum_telemetry;
+typedef struct fiber_telemetry {
+    uint32_t allocated_pages;
+    uint32_t binning_tasks;
+    uint32_t page_candidates;          /* tasks per allocated page, summed           */
+    uint32_t fine_cell_hits;           /* fine references (the reference tail)       */
+    uint32_t active_candidate_pages;   /* allocated pages with a candidate           */
+    uint32_t max_candidates_per_page;
+    uint32_t frustum_count;
+    uint32_t pad;
+    uint32_t candidate_histogram[FIBER_TELEMETRY_HISTOGRAM_BINS];  /* pages by floor(log2(candidates)) */
+    fiber_frustum_telemetry frustum[FIBER_TELEMETRY_MAX_FRUSTA];
+} fiber_telemetry;
+
 /* What fiber_dump copies back (canonical forms used by parity tests). */
 typedef enum fiber_dump_what {
     FIBER_DUMP_FRUSTA = 0,        /* fiber_frustum_desc[F]                      */
@@ -385,6 +417,8 @@ fiber_status fiber_render_host(fiber_ctx* ctx, const void* scene_rgba16f_host,
 /* Synchronises the context's last stream and returns the frame counters
  * (telemetry words, src/pipelines/prepass.rs:1345-1396). */
 fiber_status fiber_stats_get(fiber_ctx* ctx, fiber_stats* out);
+/* The last frame's prepass telemetry; EINVAL unless telemetry is enabled. */
+fiber_status fiber_telemetry_get(fiber_ctx* ctx, fiber_telemetry* out);
 /* Copies one canonical buffer to host memory. With host == NULL only
  * *written receives the byte size. */
 fiber_status fiber_dump(fiber_ctx* ctx, uint32_t what, void* host, uint64_t capacity,

@@ -281,6 +281,15 @@ struct fref_frame {
     std::vector<uint32_t> fragments;
     std::vector<float> composite;
     std::vector<uint32_t> opaque_tiles;  // (covered, farthest q) per camera fine tile
+    // Prepass telemetry (PrepassTelemetrySettings): per-frustum visibility and
+    // retention counts, candidate tasks per page, the reference tail, and the
+    // fiber_telemetry image built from them after the emit.
+    std::vector<uint32_t> tel_visible_instances = std::vector<uint32_t>(16, 0u);
+    std::vector<uint32_t> tel_visible_strands = std::vector<uint32_t>(16, 0u);
+    std::vector<uint32_t> tel_retained = std::vector<uint32_t>(16, 0u);
+    std::vector<uint32_t> page_candidates;
+    uint64_t refs_tail = 0;
+    std::vector<uint32_t> telemetry;
     bool opaque_bound = false;
     uint32_t overflow = 0;
     uint32_t n_cam_tasks = 0;
@@ -433,6 +442,10 @@ void stage_broad(Ctx& c) {
             if (d.kind <= 1u) {
                 bool vis = emit_range(c, i, f, corners);
                 visible = vis || visible;
+                if (vis && f < 16u) {  // FRUSTUM_TELEMETRY_VISIBLE_* (:735-738)
+                    fr->tel_visible_instances[f] += 1u;
+                    fr->tel_visible_strands[f] += strand_count;
+                }
                 if (vis && d.kind == 0u) {
                     k = camera_keep(c.st, strand_count, aabb_area(fr, f, corners));
                     cam_k = wmax(cam_k, k);
@@ -488,6 +501,7 @@ void fine_strand(Ctx& c, uint32_t f, uint32_t inst, uint32_t strand, std::vector
     float k = fr->keep[inst * fr->F + f];
     if (strand_random > k) return;
     if (d.kind == 1u && light_layer(fr, f) == kInvalid) return;
+    if (f < 16u) __atomic_fetch_add(&fr->tel_retained[f], 1u, __ATOMIC_RELAXED);  // :1085
     uint32_t is_shadow = d.kind == 1u ? 1u : 0u;
     uint32_t packed = 0u | (is_shadow << 2u) | (f << 3u);
     const float* clip = fr->clip[f];
@@ -677,6 +691,8 @@ struct Traverse {
             uint32_t handle = fr->page_table[pti];
             if (handle == 0u || handle == kMarked) continue;
             uint32_t page = handle - 1u;
+            // The count pass's per-page candidate counter (:1485-1490).
+            if (v.pass == Pass::Count) __atomic_fetch_add(&fr->page_candidates[page], 1u, __ATOMIC_RELAXED);
             float zspan = wmax(zmax - zmin, 1.0f / (float)kDepthQuantMax);
             float fsx = u2f(d.froxel_size_x), fsy = u2f(d.froxel_size_y);
             V3 l0 = v3((dc.p0.x - origin.x) / fsx, (dc.p0.y - origin.y) / fsy,
@@ -802,6 +818,7 @@ void stage_binning(Ctx& c) {
     const size_t pages = fr->page_meta.size();
     // K9 count
     fr->counts.assign(pages * kPageSize, 0u);
+    fr->page_candidates.assign(pages, 0u);
 #pragma omp parallel for schedule(dynamic, 1024)
     for (int64_t k = 0; k < n; ++k) tr.visit(Visit{Pass::Count, (uint32_t)k, {}, 0});
     // K10 prefix (prefix_fine_pages, :2051-2143); ref bases in page order.
@@ -839,6 +856,7 @@ void stage_binning(Ctx& c) {
             active_flags[(size_t)pm.coarse_tile_id * 16u + lt] = 1u;
         }
     }
+    fr->refs_tail = tail;
     // K11 fill; then the canonical within-cell order.
     uint64_t ref_total = 0;
     for (const auto& pm : fr->page_meta) ref_total += pm.seg_ref_count;
@@ -1465,6 +1483,52 @@ void stage_raster(Ctx& c) {
     }
 }
 
+// ---- finalize_telemetry (strand_prepass.wgsl:2145-2188) ----------------------
+// The fiber_telemetry image: totals, the candidate statistics of every
+// allocated page, and per frustum the visibility / retention counts, tasks,
+// pages, candidates, references and the load of the tile runs with work.
+void stage_telemetry(Ctx& c) {
+    fref_frame* fr = c.fr;
+    const uint32_t kHist = 8, kFr = 40, kStride = 11;
+    std::vector<uint32_t>& t = fr->telemetry;
+    t.assign(kFr + 16 * kStride, 0u);
+    auto F = [&](uint32_t f, uint32_t field) -> uint32_t& { return t[kFr + f * kStride + field]; };
+    t[0] = (uint32_t)fr->page_meta.size();
+    t[1] = (uint32_t)fr->tasks.size();
+    t[3] = (uint32_t)fr->refs_tail;
+    t[6] = fr->F;
+    for (uint32_t f = 0; f < fr->F && f < 16u; ++f) {
+        F(f, 0) = fr->tel_visible_instances[f];
+        F(f, 1) = fr->tel_visible_strands[f];
+        F(f, 2) = fr->tel_retained[f];
+        F(f, 3) = fr->frustum_task_base[f + 1] - fr->frustum_task_base[f];
+    }
+    for (size_t p = 0; p < fr->page_meta.size(); ++p) {
+        const auto& pm = fr->page_meta[p];
+        const uint32_t f = frustum_for_tile(fr, pm.coarse_tile_id);
+        if (f != kInvalid) F(f, 4) += 1u;
+        const uint32_t cand = fr->page_candidates[p];
+        if (cand == 0u) continue;
+        t[2] += cand;
+        t[4] += 1u;
+        t[5] = std::max(t[5], cand);
+        uint32_t bin = 0, rem = cand;
+        while (rem > 1u && bin + 1u < 32u) { rem >>= 1u; ++bin; }
+        t[kHist + bin] += 1u;
+        if (f != kInvalid) {
+            F(f, 5) += cand;
+            F(f, 6) += pm.seg_ref_count;
+            F(f, 9) = std::max(F(f, 9), cand);
+        }
+    }
+    for (const auto& run : fr->runs) {
+        if (run.work_count == 0u || run.frustum_id >= fr->F) continue;
+        F(run.frustum_id, 7) += 1u;
+        F(run.frustum_id, 8) += run.load_score;
+        F(run.frustum_id, 10) = std::max(F(run.frustum_id, 10), run.load_score);
+    }
+}
+
 // ---- K20 composite (strand_composite.wgsl:12-33 + ALPHA_BLENDING) -----------
 void stage_composite(Ctx& c, const float* scene_color, const float* scene_depth) {
     fref_frame* fr = c.fr;
@@ -1613,6 +1677,7 @@ fref_frame* fref_run_opaque(const fref_instance* inst, uint32_t n_inst, const fi
     stage_binning(c);
     double t3 = now_ms();
     stage_emit(c);
+    stage_telemetry(c);
     double t4 = now_ms();
     stage_shadow(c);
     double t5 = now_ms();
@@ -1667,6 +1732,7 @@ uint64_t fref_get(const fref_frame* f, uint32_t what, void* host, uint64_t cap) 
         case FIBER_DUMP_FRAGMENTS: return copy_out(f->fragments, host, cap);
         case FIBER_DUMP_OPAQUE_TILES: return copy_out(f->opaque_tiles, host, cap);
         case FREF_COMPOSITE: return copy_out(f->composite, host, cap);
+        case FREF_TELEMETRY: return copy_out(f->telemetry, host, cap);
         case FREF_REF_KEYS: return copy_out(f->ref_keys, host, cap);
         case FREF_STAGE_MS: {
             uint64_t bytes = sizeof(f->stage_ms);

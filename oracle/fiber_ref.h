@@ -77,6 +77,7 @@ void fref_free(fref_frame* f);
 #define FREF_COMPOSITE 100   /* float[W*H*4] composited output (fp16-rounded) */
 #define FREF_REF_KEYS 101    /* u32[R] sort key of each reference             */
 #define FREF_STAGE_MS 102    /* float[8] per-stage wall time                  */
+#define FREF_TELEMETRY 103   /* fiber_telemetry image (u32 words)              */
 
 /* Primitive known-answer helpers (tests/test_oracle_primitives.py). */
 uint32_t fref_wang_hash(uint32_t x);

@@ -21,6 +21,7 @@ ORACLE_LIB = ORACLE_DIR / "_build" / "libfiber_ref.so"
 FREF_COMPOSITE = 100
 FREF_REF_KEYS = 101
 FREF_STAGE_MS = 102
+FREF_TELEMETRY = 103
 
 
 class FrefInstance(C.Structure):
@@ -128,6 +129,10 @@ class OracleFrame:
         s = abi.Stats()
         oracle_lib().fref_stats(self.handle, C.byref(s))
         return s
+
+    def telemetry(self) -> abi.Telemetry:
+        w = self.get(FREF_TELEMETRY, np.dtype("<u4"))
+        return abi.Telemetry.from_buffer_copy(w.tobytes())
 
     def stage_ms(self) -> np.ndarray:
         return self.get(FREF_STAGE_MS, np.dtype("<f4"))

@@ -110,6 +110,24 @@ def test_parity_page_csr_fused_and_overflow():
     plugin.close()
 
 
+@pytest.mark.parametrize("backend", [0, 1])
+def test_telemetry_matches_oracle(backend):
+    # PrepassTelemetrySettings on: the telemetry image matches the oracle's word
+    # for word on both binning backends, and the frame itself is unchanged.
+    scene = build_scene("small", settings_overrides={"telemetry_enabled": 1, "fine_binning_backend": backend,
+                                                      "fragment_counts_enabled": 1})
+    plugin = run_gpu(scene)
+    ref = run_ref(scene)
+    got, want = bytes(plugin.telemetry()), bytes(ref.telemetry())
+    gw, rw = np.frombuffer(got, np.uint32), np.frombuffer(want, np.uint32)
+    bad = np.nonzero(gw != rw)[0]
+    assert bad.size == 0, f"telemetry words differ at {bad[:8]}: gpu {gw[bad[:8]]} oracle {rw[bad[:8]]}"
+    assert gw[2] > 0 and gw[4] > 0
+    for what in (abi.DUMP_COUNTS, abi.DUMP_REFS, abi.DUMP_RUNS, abi.DUMP_FRAGMENTS, abi.DUMP_DOM_OPACITY):
+        _exact(plugin.dump(what), ref.get(what), what)
+    plugin.close()
+
+
 def test_parity_fused_graph():
     scene = build_scene("tiny", settings_overrides={"fragment_counts_enabled": 1})
     _compare(scene, fused=True)

@@ -148,3 +148,23 @@ def test_opaque_cull(tiny, samples):
             assert cc[p, cell] == want, (p, cell)
             culled_cells += int(hidden and cb[p, cell] > 0)
     assert culled_cells > 0
+
+
+def test_telemetry_consistent(tiny):
+    """finalize_telemetry's image agrees with the frame's own counts."""
+    t = tiny.telemetry()
+    s = tiny.stats()
+    assert t.allocated_pages == s.allocated_pages and t.binning_tasks == s.binning_tasks
+    assert t.frustum_count == s.frustum_count == 2
+    assert sum(t.candidate_histogram) == t.active_candidate_pages <= t.allocated_pages
+    assert t.page_candidates >= t.active_candidate_pages and t.max_candidates_per_page > 0
+    runs = 0
+    for f in range(s.frustum_count):
+        fr = t.frustum[f]
+        assert fr.emitted_segments == s.frustum_tasks[f]
+        assert fr.allocated_pages == s.frustum_pages[f] and fr.fine_refs == s.frustum_refs[f]
+        assert 0 < fr.retained_strands <= fr.visible_strands and fr.visible_instances == 1
+        assert fr.max_page_candidates <= fr.page_candidates and fr.max_raster_load <= fr.raster_load
+        runs += fr.raster_runs
+    assert runs == s.camera_runs + s.shadow_runs
+    assert sum(t.frustum[f].page_candidates for f in range(2)) == t.page_candidates
