@@ -54,6 +54,8 @@ def parse_args():
     p.add_argument("--no-batched", action="store_true", help="skip the batched-mode measurement")
     p.add_argument("--binning-backend", default="segment", choices=["segment", "page-csr"],
                    help="FineBinningBackend: segment-owned scatter (default) or the page CSR")
+    p.add_argument("--dom-page-pool", type=int, default=0,
+                   help="sparse deep-opacity residency in this many 256^2 pages (0: dense layers)")
     p.add_argument("--batched-views", type=int, default=64, help="independent views in one batch launch")
     return p.parse_args()
 
@@ -306,7 +308,7 @@ def fiber_arm(args):
     from bevy_strand_rasterizer_b200.plugin import FineBinningBackend
     backend = FineBinningBackend.PageCsr if args.binning_backend == "page-csr" else FineBinningBackend.SegmentScatter
     plugin = StrandRasterizerPlugin(device=local, dom_slices=w.dom_layers, ref_capacity_factor=w.ref_capacity_factor,
-                                    backend=backend)
+                                    backend=backend, dom_page_pool=args.dom_page_pool)
     plugin.add_geometry(packed, material)
     stream = torch.cuda.Stream()
     H, W = w.height, w.width
@@ -426,7 +428,7 @@ def fiber_arm(args):
                        "tile_px": w.froxel, "parallelism": f"replicas x{world}",
                        "l2": "per-frame working set (tasks, refs, pages, DOM) > 126 MB L2",
                        "stochastic_cull": "on (reference default)", "ref_capacity_factor": w.ref_capacity_factor,
-                       "fine_binning_backend": args.binning_backend},
+                       "fine_binning_backend": args.binning_backend, "dom_page_pool": args.dom_page_pool},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "entry_point": "fiber_render_host", "ms_per_step": e2e_ms / args.steps},
             "roofline": {"bound": "hbm", "kernel": dom_kernel, "achieved": achieved, "peak": peak,

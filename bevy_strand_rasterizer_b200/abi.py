@@ -82,7 +82,7 @@ class Settings(C.Structure):
                 ("telemetry_enabled", u32), ("fine_binning_backend", u32), ("dom_slices", u32),
                 ("shadow_map_size", u32), ("ambient_color", f32 * 4), ("history_enabled", u32),
                 ("fragment_counts_enabled", u32), ("ref_capacity_factor", u32),
-                ("page_capacity_divisor", u32)]
+                ("page_capacity_divisor", u32), ("dom_page_pool", u32)]
 
 
 class Image(C.Structure):

@@ -114,6 +114,7 @@ struct fiber_ctx {
     DevBuf d_opaque;  // (covered, farthest depth q) per camera fine tile
     DevBuf d_page_nvis, d_page_vbase, d_page_bucket;  // page-CSR backend
     DevBuf d_tel, d_tel_slots;                         // prepass telemetry
+    DevBuf d_dom_page_table, d_dom_pool;               // sparse DOM residency
     uint32_t camera_fine_tiles = 0;
     bool opaque_frame = false;  // fiber_opaque_depth ran since fiber_frame_begin
     // A batch graph advanced this context's epoch on the device: the next
@@ -250,6 +251,8 @@ RenderArgs render_args(fiber_ctx* c) {
     R.runs = dp<fiber_raster_tile_run>(c->d_runs);
     R.dom_depth = dp<float>(c->d_dom_depth);
     R.dom_opacity = dp<float>(c->d_dom_opacity);
+    R.dom_page_table = dp<uint32_t>(c->d_dom_page_table);
+    R.dom_pool = dp<float>(c->d_dom_pool);
     R.shadow_map = dp<float>(c->d_shadow_map);
     R.atlas = dp<__half>(c->d_atlas);
     R.history[0] = dp<__half>(c->d_history[0]);
@@ -296,7 +299,12 @@ fiber_status frame_resets(fiber_ctx* c, cudaStream_t s) {
     FIBER_CUDA(cudaMemsetAsync(c->d_depth.p, 0, W * H * 4, s));
     if (P.fragment_counts) FIBER_CUDA(cudaMemsetAsync(c->d_fragments.p, 0, W * H * 4, s));
     if (L) {
-        FIBER_CUDA(cudaMemsetAsync(c->d_dom_depth.p, 0, L * D * D * 4, s));
+        if (P.dom_pool_pages) {
+            const uint64_t ppx = P.dom_pages_x;
+            FIBER_CUDA(cudaMemsetAsync(c->d_dom_page_table.p, 0, L * ppx * ppx * 4, s));
+        } else {
+            FIBER_CUDA(cudaMemsetAsync(c->d_dom_depth.p, 0, L * D * D * 4, s));
+        }
         FIBER_CUDA(cudaMemsetAsync(c->d_shadow_map.p, 0, L * S * S * 4, s));
     }
     if (c->settings.telemetry_enabled) {
@@ -374,7 +382,12 @@ fiber_status run_prepass(fiber_ctx* c, cudaStream_t s, const OpaqueSource* opaqu
 
 fiber_status run_shadows(fiber_ctx* c, cudaStream_t s) {
     record(c, 9, s);
-    if (c->P.L) launch_shadow(launch_ctx(c, s), render_args(c), c->P.K);
+    if (c->P.L) {
+        const LaunchCtx L = launch_ctx(c, s);
+        const RenderArgs R = render_args(c);
+        if (c->P.dom_pool_pages) launch_dom_paging(L, R, c->P.L * c->P.dom_pages_x * c->P.dom_pages_x);
+        launch_shadow(L, R, c->P.K);
+    }
     return check_launch();
 }
 
@@ -482,6 +495,7 @@ fiber_status fiber_settings_default(fiber_settings* s) {
     s->fragment_counts_enabled = 0u;
     s->ref_capacity_factor = 4u;              // fine refs = 4 x binning (src/plugin.rs:536-540)
     s->page_capacity_divisor = 1u;
+    s->dom_page_pool = 0u;                    // dense deep-opacity layers
     return FIBER_OK;
 }
 
@@ -529,7 +543,7 @@ fiber_status fiber_ctx_destroy(fiber_ctx* c) {
                       &c->d_validate, &c->d_host_scene, &c->d_host_depth, &c->d_visit_rec,
                       &c->d_visit_task, &c->d_visit_rank, &c->d_task_key, &c->d_task_mat,
                       &c->d_cells_small, &c->d_cells_large, &c->d_opaque, &c->d_page_nvis, &c->d_page_vbase,
-                      &c->d_page_bucket, &c->d_tel, &c->d_tel_slots};
+                      &c->d_page_bucket, &c->d_tel, &c->d_tel_slots, &c->d_dom_page_table, &c->d_dom_pool};
     for (DevBuf* b : bufs) release(c, *b);
     for (int i = 0; i <= kSpanCount; ++i)
         if (c->ev[i]) cudaEventDestroy(c->ev[i]);
@@ -737,6 +751,8 @@ fiber_status fiber_frame_begin(fiber_ctx* c, const fiber_froxel_config* cam_cfg,
     P.camera_tile_end = cam_tiles;
     P.dom_size = n_lights ? light_cfgs[0].screen_width : 0u;
     P.shadow_map_size = n_lights ? (st.shadow_map_size ? st.shadow_map_size : P.dom_size) : 0u;
+    P.dom_pool_pages = n_lights ? st.dom_page_pool : 0u;
+    P.dom_pages_x = (P.dom_size + kDomPage - 1u) / kDomPage;
     // Shading atlas dims (create_shading_target_texture, src/pipelines/shading.rs:410-438).
     uint32_t aw = std::min(std::max(c->max_texels, 1u), 8192u);
     uint32_t ah = std::min(std::max((c->max_texels + aw - 1u) / aw, 1u), 8192u);
@@ -835,8 +851,14 @@ fiber_status fiber_frame_begin(fiber_ctx* c, const fiber_froxel_config* cam_cfg,
         ENSURE(c->d_page_vbase, page_cap * 4, false);
         ENSURE(c->d_page_bucket, visit_cap * sizeof(uint2), false);
     }
-    ENSURE(c->d_dom_depth, L * D * D * 4, false);
-    ENSURE(c->d_dom_opacity, L * K * D * D * 4, true);
+    if (P.dom_pool_pages) {  // sparse residency: a page table per layer and the page pool
+        const uint64_t ppx = P.dom_pages_x;
+        ENSURE(c->d_dom_page_table, L * ppx * ppx * 4, false);
+        ENSURE(c->d_dom_pool, (uint64_t)P.dom_pool_pages * kDomPageTexels * (K + 1) * 4, false);
+    } else {
+        ENSURE(c->d_dom_depth, L * D * D * 4, false);
+        ENSURE(c->d_dom_opacity, L * K * D * D * 4, true);
+    }
     ENSURE(c->d_shadow_map, L * S * S * 4, false);
     const uint64_t atlas_texels = (uint64_t)std::max(I, 1u) * P.atlas_cap;
     bool hist_new = !c->d_history[0].p || c->d_history[0].bytes < atlas_texels * 4;
@@ -1201,6 +1223,39 @@ fiber_status fiber_stats_get(fiber_ctx* c, fiber_stats* out) {
     return FIBER_OK;
 }
 
+// The DOM as dense layers on the host: a copy, or the resident pages of the
+// sparse pool expanded through the page tables (zeros elsewhere).
+static fiber_status dom_dense(fiber_ctx* c, std::vector<float>& dep, std::vector<float>& op) {
+    const FrameParams& P = c->P;
+    const uint64_t L = P.L, D = P.dom_size, K = P.K;
+    if (!P.dom_pool_pages) {
+        FIBER_CUDA(cudaMemcpy(dep.data(), c->d_dom_depth.p, dep.size() * 4, cudaMemcpyDeviceToHost));
+        FIBER_CUDA(cudaMemcpy(op.data(), c->d_dom_opacity.p, op.size() * 4, cudaMemcpyDeviceToHost));
+        return FIBER_OK;
+    }
+    const uint64_t ppx = P.dom_pages_x, page_words = (uint64_t)kDomPageTexels * (K + 1);
+    std::vector<uint32_t> table(L * ppx * ppx);
+    FIBER_CUDA(cudaMemcpy(table.data(), c->d_dom_page_table.p, table.size() * 4, cudaMemcpyDeviceToHost));
+    std::fill(dep.begin(), dep.end(), 0.0f);
+    std::fill(op.begin(), op.end(), 0.0f);
+    std::vector<float> page(page_words);
+    for (uint64_t l = 0; l < L; ++l)
+        for (uint64_t py = 0; py < ppx; ++py)
+            for (uint64_t px = 0; px < ppx; ++px) {
+                const uint32_t h = table[(l * ppx + py) * ppx + px];
+                if (h == 0u || h == kMarked || h - 1u >= P.dom_pool_pages) continue;
+                FIBER_CUDA(cudaMemcpy(page.data(), static_cast<const float*>(c->d_dom_pool.p) + (h - 1u) * page_words,
+                                      page_words * 4, cudaMemcpyDeviceToHost));
+                for (uint64_t y = 0; y < kDomPage && py * kDomPage + y < D; ++y)
+                    for (uint64_t x = 0; x < kDomPage && px * kDomPage + x < D; ++x) {
+                        const uint64_t t = (py * kDomPage + y) * D + px * kDomPage + x, o = y * kDomPage + x;
+                        dep[l * D * D + t] = page[o];
+                        for (uint64_t k = 0; k < K; ++k) op[(l * K + k) * D * D + t] = page[(1 + k) * kDomPageTexels + o];
+                    }
+            }
+    return FIBER_OK;
+}
+
 fiber_status fiber_telemetry_get(fiber_ctx* c, fiber_telemetry* out) {
     if (!c || !out) return FIBER_EINVAL;
     if (!c->settings.telemetry_enabled || !c->d_tel.p) return FIBER_EINVAL;
@@ -1258,22 +1313,24 @@ fiber_status fiber_dump(fiber_ctx* c, uint32_t what, void* host, uint64_t capaci
         case FIBER_DUMP_ACTIVE_TILES: src = c->d_active_list.p; bytes = (uint64_t)h.active_tiles * 4; break;
         case FIBER_DUMP_WORK: src = c->d_work.p; bytes = (uint64_t)std::min(h.work_items, P.work_capacity) * 32; break;
         case FIBER_DUMP_RUNS: src = c->d_runs.p; bytes = (uint64_t)h.active_tiles * 32; break;
-        case FIBER_DUMP_DOM_DEPTH: src = c->d_dom_depth.p; bytes = L * D * D * 4; break;
+        case FIBER_DUMP_DOM_DEPTH:
         case FIBER_DUMP_DOM_OPACITY: {
-            // Canonical form: opacity of texels without a depth (never written
-            // this frame) reads as 0.
+            // Dense layers in canonical form: opacity of texels without a depth
+            // (never written this frame) reads as 0; under sparse residency
+            // the texels of pages that are not resident read as 0.
             std::vector<float> dep(L * D * D), op(L * K * D * D);
-            if (!op.empty()) {
-                FIBER_CUDA(cudaMemcpy(dep.data(), c->d_dom_depth.p, dep.size() * 4, cudaMemcpyDeviceToHost));
-                FIBER_CUDA(cudaMemcpy(op.data(), c->d_dom_opacity.p, op.size() * 4, cudaMemcpyDeviceToHost));
+            if (!dep.empty()) {
+                fiber_status e = dom_dense(c, dep, op);
+                if (e != FIBER_OK) return e;
                 for (uint64_t l = 0; l < L; ++l)
                     for (uint64_t k = 0; k < K; ++k)
                         for (uint64_t p = 0; p < D * D; ++p)
                             if (dep[l * D * D + p] == 0.0f) op[(l * K + k) * D * D + p] = 0.0f;
             }
-            if (written) *written = op.size() * 4;
-            if (host && capacity >= op.size() * 4) std::memcpy(host, op.data(), op.size() * 4);
-            return FIBER_OK;
+            const std::vector<float>& v = what == FIBER_DUMP_DOM_DEPTH ? dep : op;
+            if (written) *written = v.size() * 4;
+            if (host && capacity >= v.size() * 4) std::memcpy(host, v.data(), v.size() * 4);
+            return host && capacity < v.size() * 4 ? FIBER_EINVAL : FIBER_OK;
         }
         case FIBER_DUMP_SHADOW_MAP: src = c->d_shadow_map.p; bytes = L * S * S * 4; break;
         case FIBER_DUMP_ATLAS: src = c->d_atlas.p; bytes = (uint64_t)P.I * P.atlas_cap * 8; break;
@@ -1307,8 +1364,12 @@ fiber_status fiber_output_image(fiber_ctx* c, uint32_t what, fiber_image* out) {
     switch (what) {
         case FIBER_DUMP_COLOR: *out = fiber_image{c->d_color.p, P.width, P.height, P.width * 8u, FIBER_FMT_RGBA16F}; break;
         case FIBER_DUMP_DEPTH: *out = fiber_image{c->d_depth.p, P.width, P.height, P.width * 4u, FIBER_FMT_R32F}; break;
-        case FIBER_DUMP_DOM_DEPTH: *out = fiber_image{c->d_dom_depth.p, P.dom_size, P.dom_size * P.L, P.dom_size * 4u, FIBER_FMT_R32F}; break;
+        case FIBER_DUMP_DOM_DEPTH:
+            if (P.dom_pool_pages) return FIBER_EINVAL;  // sparse residency: no dense image (fiber_dump expands it)
+            *out = fiber_image{c->d_dom_depth.p, P.dom_size, P.dom_size * P.L, P.dom_size * 4u, FIBER_FMT_R32F};
+            break;
         case FIBER_DUMP_DOM_OPACITY:
+            if (P.dom_pool_pages) return FIBER_EINVAL;
             *out = fiber_image{c->d_dom_opacity.p, P.dom_size, P.dom_size * P.L * P.K, P.dom_size * 4u, FIBER_FMT_R32F};
             break;
         case FIBER_DUMP_SHADOW_MAP:

@@ -70,6 +70,8 @@ struct FrameParams {
     uint32_t epoch;               // look-back status epoch of this frame
     uint32_t hist_in;             // shadow-history buffer read this frame (0/1)
     uint32_t visit_records;       // page-table slots fit 24 bits: count/fill stream visit records
+    uint32_t dom_pool_pages;      // 0: dense DOM layers; else the sparse DOM's pool size in pages
+    uint32_t dom_pages_x;         // DOM pages per side (ceil(D / 256))
 };
 
 // Device counters of one frame (zeroed at frame start).
@@ -82,7 +84,7 @@ struct FrameCounters {
     uint32_t camera_active;       // active tiles that belong to camera frusta
     uint32_t work_items;
     uint32_t runs;
-    uint32_t overflow;            // bit0 tasks, bit1 pages, bit2 refs, bit3 work
+    uint32_t overflow;            // bit0 tasks, bit1 pages, bit2 refs, bit3 work, bit4 DOM pool
     uint32_t error;               // kErrTimeout when a bounded wait gave up
     uint32_t big_cells;           // cells queued for the large-cell sort
     uint32_t tile_counter[8];     // virtual block ids of the look-back stages
@@ -91,7 +93,7 @@ struct FrameCounters {
     uint32_t small_cells;         // cells of 1..8 references listed for the cell sort
     uint32_t large_cells;         // cells of more than 8 references listed for the cell sort
     uint32_t opaque_bound;        // the opaque fine-tile depths of this frame are written
-    uint32_t pad;
+    uint32_t dom_pages;           // DOM pages requested this frame (sparse residency)
 };
 static_assert(sizeof(FrameCounters) == 168, "FrameCounters layout");
 

@@ -107,8 +107,10 @@ struct RenderArgs {
     const fiber_fine_seg_ref* refs;
     const fiber_raster_work_item* work;
     const fiber_raster_tile_run* runs;
-    float* dom_depth;        // [L][D][D]
-    float* dom_opacity;      // [L][K][D][D]
+    float* dom_depth;        // [L][D][D] (dense layers)
+    float* dom_opacity;      // [L][K][D][D] (dense layers)
+    uint32_t* dom_page_table;  // [L][pages_x][pages_x] pool page + 1 (sparse residency)
+    float* dom_pool;           // [pool][K + 1][256][256]: depth plane, then the K opacity planes
     float* shadow_map;       // [L][S][S] stampback target
     __half* atlas;           // [I][cap][4]
     __half* history[2];      // [I][cap][2] ping-pong; FrameParams::hist_in is read
@@ -116,6 +118,35 @@ struct RenderArgs {
     float* depth;            // [H][W]
     uint32_t* fragments;     // [H][W]
 };
+
+// Sparse DOM pages: DOM_PAGE_XY (src/plugin.rs:68) texels a side.
+constexpr uint32_t kDomPage = 256;
+constexpr uint32_t kDomPageTexels = kDomPage * kDomPage;
+
+// The deep-opacity texel (layer, x, y): its depth word and its slice-0
+// opacity word, with the stride between opacity slices. Dense layers, or the
+// resident pool page through the page table (false when the page is not
+// resident: nothing was rasterised there this frame).
+__device__ __forceinline__ bool dom_texel(const FrameParams& P, const RenderArgs& R, uint32_t layer, uint32_t x,
+                                          uint32_t y, float*& depth, float*& opacity, size_t& stride) {
+    const uint32_t D = P.dom_size;
+    if (P.dom_pool_pages == 0u) {
+        const size_t px = (size_t)y * D + x;
+        depth = R.dom_depth + (size_t)layer * D * D + px;
+        opacity = R.dom_opacity + (size_t)layer * P.K * D * D + px;
+        stride = (size_t)D * D;
+        return true;
+    }
+    const uint32_t px_ = P.dom_pages_x;
+    const uint32_t h = R.dom_page_table[((size_t)layer * px_ + y / kDomPage) * px_ + x / kDomPage];
+    if (h == 0u || h == kMarked || h - 1u >= P.dom_pool_pages) return false;
+    float* page = R.dom_pool + (size_t)(h - 1u) * kDomPageTexels * (P.K + 1u);
+    const uint32_t off = (y % kDomPage) * kDomPage + x % kDomPage;
+    depth = page + off;
+    opacity = page + kDomPageTexels + off;
+    stride = kDomPageTexels;
+    return true;
+}
 
 struct CompositeArgs {
     const __half* strand_color;
@@ -160,6 +191,7 @@ void launch_sort_big(const LaunchCtx& L, const PrepassArgs& A);
 void launch_telemetry(const LaunchCtx& L, const PrepassArgs& A);
 
 void launch_shadow(const LaunchCtx& L, const RenderArgs& R, uint32_t K);
+void launch_dom_paging(const LaunchCtx& L, const RenderArgs& R, uint32_t table_entries);
 void launch_shade(const LaunchCtx& L, const RenderArgs& R);
 void launch_raster(const LaunchCtx& L, const RenderArgs& R);
 void launch_composite(cudaStream_t s, const CompositeArgs& C);

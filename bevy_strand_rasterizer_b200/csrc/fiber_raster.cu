@@ -209,7 +209,7 @@ __device__ __forceinline__ void candidate_word(const Band& B, bool v, float x0, 
     out[32u + lane] = warp_transpose32((uint32_t)(bits >> 32), lane);
 }
 
-__global__ void __launch_bounds__(kShadowThreads) k_shadow(const FrameParams* __restrict__ Pp,
+__global__ void __launch_bounds__(kShadowThreads, 14) k_shadow(const FrameParams* __restrict__ Pp,
                                                            const InstanceView* __restrict__ inst, RenderArgs R) {
     const FrameParams& P = *Pp;
     extern __shared__ float s_dyn[];
@@ -410,18 +410,34 @@ __global__ void __launch_bounds__(kShadowThreads) k_shadow(const FrameParams* __
         }
         // ---- Combine the 4 workers per slice, write the DOM, stamp the shadow map.
         if (active) {
+            // A texel of a page the sparse pool could not hold is not stored
+            // (counted as a DOM pool overflow); the stampback still runs.
+            // Dense layers index the texel directly; the sparse pool goes
+            // through the page table (dom_texel).
+            const bool dense = P.dom_pool_pages == 0u;
+            float* dz = nullptr;
+            float* dop = nullptr;
+            size_t ds = 0;
             const size_t dom_px = (size_t)py * D + px;
+            const bool stored = dense || dom_texel(P, R, layer, px, py, dz, dop, ds);
             if (!found) {
-                R.dom_depth[(size_t)layer * D * D + dom_px] = 0.0f;
-                for (uint32_t i = 0; i < K; ++i) R.dom_opacity[((size_t)layer * K + i) * D * D + dom_px] = 0.0f;
+                if (dense) {
+                    R.dom_depth[(size_t)layer * D * D + dom_px] = 0.0f;
+                    for (uint32_t i = 0; i < K; ++i) R.dom_opacity[((size_t)layer * K + i) * D * D + dom_px] = 0.0f;
+                } else if (stored) {
+                    *dz = 0.0f;
+                    for (uint32_t i = 0; i < K; ++i) dop[i * ds] = 0.0f;
+                }
             } else {
-                R.dom_depth[(size_t)layer * D * D + dom_px] = z0;
+                if (dense) R.dom_depth[(size_t)layer * D * D + dom_px] = z0;
+                else if (stored) *dz = z0;
                 float acc = 0.0f;
                 for (uint32_t i = 0; i < K; ++i) {
                     float a = 0.0f;
                     for (uint32_t wk = 0; wk < 4u; ++wk) a = a + (1.0f - a) * partial[(wk * K + i) * kShadowThreads];
                     acc = acc + (1.0f - acc) * a;  // opaque_terminal_slice = K without an opaque depth
-                    R.dom_opacity[((size_t)layer * K + i) * D * D + dom_px] = acc;
+                    if (dense) R.dom_opacity[((size_t)layer * K + i) * D * D + dom_px] = acc;
+                    else if (stored) dop[i * ds] = acc;
                 }
                 // Fused stampback: every target texel whose DOM footprint holds
                 // this texel takes the max depth (the target starts cleared).
@@ -443,6 +459,81 @@ __global__ void __launch_bounds__(kShadowThreads) k_shadow(const FrameParams* __
             }
         }
     }
+}
+
+// ===========================================================================
+// Sparse DOM residency (the reference's bevy_vsms demand paging, replaced by
+// a per-frame page pool). Every shadow tile run with work requests the DOM
+// pages under its tile and their neighbours (request_shadow_dom_pages,
+// strand_prepass.wgsl:2540-2579, DOM_PREFETCH_PAGE_BORDER = 1); requested
+// pages take pool pages in page-table order (layer, row, column), as many as
+// the pool holds; their depth planes are cleared (a texel without depth is
+// empty whatever its opacity words hold).
+// ===========================================================================
+constexpr uint32_t kDomBorder = 1;
+
+__global__ void __launch_bounds__(256) k_dom_request(const FrameParams* __restrict__ Pp, RenderArgs R) {
+    const FrameParams& P = *Pp;
+    const uint32_t first = *((volatile uint32_t*)&R.counters->camera_active);
+    const uint32_t last = *((volatile uint32_t*)&R.counters->active_tiles);
+    const uint32_t ppx = P.dom_pages_x;
+    for (uint32_t r = first + blockIdx.x * blockDim.x + threadIdx.x; r < last; r += gridDim.x * blockDim.x) {
+        const fiber_raster_tile_run run = R.runs[r];
+        const uint32_t layer = light_layer(P, run.frustum_id);
+        if (run.work_count == 0u || layer == kInvalid) continue;
+        const fiber_frustum_desc& d = P.frusta[run.frustum_id];
+        const uint32_t ftx = ceil_div(d.screen_width, d.froxel_size_x);
+        const uint32_t x0 = (run.screen_tile_id % ftx) * d.froxel_size_x, y0 = (run.screen_tile_id / ftx) * d.froxel_size_y;
+        const uint32_t x1 = min(x0 + d.froxel_size_x - 1u, d.screen_width - 1u);
+        const uint32_t y1 = min(y0 + d.froxel_size_y - 1u, d.screen_height - 1u);
+        const uint32_t pmx0 = x0 / kDomPage, pmy0 = y0 / kDomPage;
+        const uint32_t px0 = pmx0 - min(pmx0, kDomBorder), py0 = pmy0 - min(pmy0, kDomBorder);
+        const uint32_t px1 = min(x1 / kDomPage + kDomBorder, ppx - 1u), py1 = min(y1 / kDomPage + kDomBorder, ppx - 1u);
+        for (uint32_t py = py0; py <= py1; ++py)
+            for (uint32_t px = px0; px <= px1; ++px) R.dom_page_table[((size_t)layer * ppx + py) * ppx + px] = kMarked;
+    }
+}
+
+// One block: requested entries, in table order, get pool page index + 1.
+__global__ void __launch_bounds__(1024) k_dom_alloc(const FrameParams* __restrict__ Pp, RenderArgs R, uint32_t entries) {
+    const FrameParams& P = *Pp;
+    __shared__ uint32_t s_warp[33];
+    __shared__ uint32_t s_carry;
+    if (threadIdx.x == 0) s_carry = 0u;
+    __syncthreads();
+    for (uint32_t b = 0; b < entries; b += 1024u) {
+        const uint32_t i = b + threadIdx.x;
+        const bool req = i < entries && R.dom_page_table[i] == kMarked;
+        uint32_t total;
+        const uint32_t ex = block_exclusive_scan<1024>(req ? 1u : 0u, s_warp, total);
+        if (req) {
+            const uint32_t idx = s_carry + ex;
+            R.dom_page_table[i] = idx < P.dom_pool_pages ? idx + 1u : 0u;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) s_carry += total;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        R.counters->dom_pages = s_carry;
+        if (s_carry > P.dom_pool_pages) atomicOr(&R.counters->overflow, 16u);
+    }
+}
+
+__global__ void __launch_bounds__(256) k_dom_clear(const FrameParams* __restrict__ Pp, RenderArgs R) {
+    const FrameParams& P = *Pp;
+    const uint32_t pages = min(*((volatile uint32_t*)&R.counters->dom_pages), P.dom_pool_pages);
+    const size_t per_page = kDomPageTexels / 4u, n = (size_t)pages * per_page;
+    for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+        float* page = R.dom_pool + (k / per_page) * kDomPageTexels * (P.K + 1u);
+        reinterpret_cast<float4*>(page)[k % per_page] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    }
+}
+
+void launch_dom_paging(const LaunchCtx& L, const RenderArgs& R, uint32_t table_entries) {
+    k_dom_request<<<L.sm_count * 2, 256, 0, L.stream>>>(L.P, R);
+    k_dom_alloc<<<1, 1024, 0, L.stream>>>(L.P, R, table_entries);
+    k_dom_clear<<<L.sm_count * 4, 256, 0, L.stream>>>(L.P, R);
 }
 
 // ===========================================================================

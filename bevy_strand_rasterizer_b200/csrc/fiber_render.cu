@@ -41,14 +41,18 @@ __device__ float sample_dom(const FrameParams& P, const RenderArgs& R, F3 pw, ui
     float4 raw = world_to_screen_raw(make_float4(pw.x, pw.y, pw.z, 1.0f), P.clip[f], vw, vh);
     if (raw.x < 0.0f || raw.y < 0.0f || raw.x >= vw || raw.y >= vh || raw.z < 0.0f || raw.z > 1.0f) return 1.0f;
     uint32_t px = f2u(raw.x), py = f2u(raw.y);
-    const uint32_t D = P.dom_size, K = P.K;
-    float z0 = R.dom_depth[(size_t)layer * D * D + (size_t)py * D + px];
+    const uint32_t K = P.K;
+    float* dz;
+    float* dop;
+    size_t ds;
+    if (!dom_texel(P, R, layer, px, py, dz, dop, ds)) return 1.0f;  // page not resident: nothing there
+    float z0 = *dz;
     if (z0 <= 0.0f) return 1.0f;
     float z = normalize_depth01(raw.z);
     if (z > z0 - 1e-3f) return 1.0f;
     float u = wclamp(wmax(0.0f, z0 - z) / wmax(z0, 1e-6f), 0.0f, 1.0f);  // pow(., DOM_GAMMA = 1)
     uint32_t slice = min(f2u(floorf(u * u2f(K))), K - 1u);
-    float op = R.dom_opacity[((size_t)layer * K + slice) * D * D + (size_t)py * D + px];
+    float op = dop[slice * ds];
     return wclamp(1.0f - op, 0.08f, 1.0f);
 }
 

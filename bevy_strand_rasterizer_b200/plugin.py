@@ -198,7 +198,7 @@ class StrandRasterizerPlugin:
                  backend: FineBinningBackend = FineBinningBackend.SegmentScatter,
                  dom_slices: int = 12, shadow_map_size: int = 0, ambient=(80.0, 80.0, 80.0, 80.0),
                  history: bool = True, fragment_counts: bool = False, ref_capacity_factor: int = 4,
-                 page_capacity_divisor: int = 1):
+                 page_capacity_divisor: int = 1, dom_page_pool: int = 0):
         self.lib = abi.load_library()
         self.ctx = C.c_void_p()
         abi.check(self.lib.fiber_ctx_create(device, hbm_budget, C.byref(self.ctx)), "fiber_ctx_create")
@@ -219,6 +219,7 @@ class StrandRasterizerPlugin:
         s.fragment_counts_enabled = 1 if fragment_counts else 0
         s.ref_capacity_factor = ref_capacity_factor
         s.page_capacity_divisor = page_capacity_divisor
+        s.dom_page_pool = dom_page_pool  # 0: dense DOM layers; N: sparse residency in N pages of 256^2
         self.settings = s
         abi.check(self.lib.fiber_settings_set(self.ctx, C.byref(s)), "fiber_settings_set")
         self.camera_cfg = None

@@ -216,6 +216,11 @@ typedef struct fiber_settings {
     uint32_t fragment_counts_enabled;   /* per-pixel fragment counter (0)   */
     uint32_t ref_capacity_factor;       /* refs = factor x tasks (4)        */
     uint32_t page_capacity_divisor;     /* pages = table / divisor (1)      */
+    uint32_t dom_page_pool;             /* 0 = dense deep-opacity layers (default);
+                                           N = sparse residency: the pages of
+                                           256^2 texels that shadow tile runs
+                                           request (with a one-page border)
+                                           live in a pool of N pages          */
 } fiber_settings;
 
 /* ------------------------------------------------------------------------ */
@@ -249,7 +254,8 @@ typedef struct fiber_stats {
     uint32_t camera_runs;
     uint32_t shadow_runs;
     uint32_t work_items;
-    uint32_t overflow_flags;        /* bit0 tasks, bit1 pages, bit2 refs, bit3 work */
+    uint32_t overflow_flags;        /* bit0 tasks, bit1 pages, bit2 refs, bit3 work,
+                                       bit4 DOM page pool                     */
     uint32_t timeout_flags;         /* non-zero: a bounded device wait gave up */
     uint32_t frustum_tasks[8];      /* N_f per frustum (first 8)              */
     uint32_t frustum_pages[8];

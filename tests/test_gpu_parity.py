@@ -128,6 +128,34 @@ def test_telemetry_matches_oracle(backend):
     plugin.close()
 
 
+@pytest.mark.parametrize("name", ["tiny", "small"])
+def test_parity_sparse_dom(name):
+    # Sparse DOM residency with a pool that holds every requested page: the
+    # same DOM, shadow map and images as the dense layers.
+    scene = build_scene(name, settings_overrides={"dom_page_pool": 64, "fragment_counts_enabled": 1})
+    s = _compare(scene)
+    assert s.overflow_flags == 0 and s.shadow_runs > 0
+
+
+def test_sparse_dom_pool_overflow():
+    # A pool of half the light's 16 pages: the frame flags the DOM pool
+    # overflow (bit 4); the resident pages (the first requested ones in
+    # page-table order) match the dense DOM texel for texel, the rest is empty.
+    scene = build_scene("small", settings_overrides={"dom_page_pool": 8})
+    plugin = run_gpu(scene)
+    ref = run_ref(scene)
+    s = plugin.stats(allow_overflow=True)
+    assert s.overflow_flags & 16
+    gd, rd = plugin.dump(abi.DUMP_DOM_DEPTH), ref.get(abi.DUMP_DOM_DEPTH)
+    stored = gd != 0.0
+    assert 0 < int(stored.sum()) < int((rd != 0.0).sum())
+    assert np.array_equal(gd[stored], rd[stored])
+    go = plugin.dump(abi.DUMP_DOM_OPACITY).reshape(-1, gd.size)
+    ro = ref.get(abi.DUMP_DOM_OPACITY).reshape(-1, gd.size)
+    assert np.array_equal(go[:, stored], ro[:, stored])
+    plugin.close()
+
+
 def test_parity_fused_graph():
     scene = build_scene("tiny", settings_overrides={"fragment_counts_enabled": 1})
     _compare(scene, fused=True)
