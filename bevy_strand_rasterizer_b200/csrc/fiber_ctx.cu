@@ -115,6 +115,10 @@ struct fiber_ctx {
     DevBuf d_page_nvis, d_page_vbase, d_page_bucket;  // page-CSR backend
     DevBuf d_tel, d_tel_slots;                         // prepass telemetry
     DevBuf d_dom_page_table, d_dom_pool;               // sparse DOM residency
+    // fiber_render_host: the scene image's upload runs on its own stream
+    // beside the frame; ev_in = uploaded, ev_out = the last download queued.
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t ev_in = nullptr, ev_out = nullptr;
     uint32_t camera_fine_tiles = 0;
     bool opaque_frame = false;  // fiber_opaque_depth ran since fiber_frame_begin
     // A batch graph advanced this context's epoch on the device: the next
@@ -547,6 +551,9 @@ fiber_status fiber_ctx_destroy(fiber_ctx* c) {
     for (DevBuf* b : bufs) release(c, *b);
     for (int i = 0; i <= kSpanCount; ++i)
         if (c->ev[i]) cudaEventDestroy(c->ev[i]);
+    if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
+    if (c->ev_in) cudaEventDestroy(c->ev_in);
+    if (c->ev_out) cudaEventDestroy(c->ev_out);
     delete c;
     return FIBER_OK;
 }
@@ -1039,16 +1046,31 @@ fiber_status fiber_render_host(fiber_ctx* c, const void* scene_host, const float
     fiber_status e = ensure(c, c->d_host_scene, W * H * 8, false);
     if (e == FIBER_OK && depth_host) e = ensure(c, c->d_host_depth, W * H * 4, false);
     if (e != FIBER_OK) return e;
-    FIBER_CUDA(cudaMemcpyAsync(c->d_host_scene.p, scene_host, W * H * 8, cudaMemcpyHostToDevice, s));
+    if (!c->copy_stream) {
+        FIBER_CUDA(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+        FIBER_CUDA(cudaEventCreateWithFlags(&c->ev_in, cudaEventDisableTiming));
+        FIBER_CUDA(cudaEventCreateWithFlags(&c->ev_out, cudaEventDisableTiming));
+    }
+    // The depth feeds the opaque-tile reduce at the start of the prepass, so
+    // it is uploaded in stream order. The scene image is needed only by the
+    // composite: it is uploaded on the copy stream while the frame's nodes
+    // run, once the previous frame's download has left the buffer.
     if (depth_host) FIBER_CUDA(cudaMemcpyAsync(c->d_host_depth.p, depth_host, W * H * 4, cudaMemcpyHostToDevice, s));
+    FIBER_CUDA(cudaStreamWaitEvent(c->copy_stream, c->ev_out, 0));
+    FIBER_CUDA(cudaMemcpyAsync(c->d_host_scene.p, scene_host, W * H * 8, cudaMemcpyHostToDevice, c->copy_stream));
+    FIBER_CUDA(cudaEventRecord(c->ev_in, c->copy_stream));
     // The composite blends onto the loaded destination; compositing in place
     // over the scene image gives dst = scene colour (each pixel is read and
     // written by one thread).
     fiber_image scene{c->d_host_scene.p, (uint32_t)W, (uint32_t)H, (uint32_t)(W * 8), FIBER_FMT_RGBA16F};
     fiber_image depth{c->d_host_depth.p, (uint32_t)W, (uint32_t)H, (uint32_t)(W * 4), FIBER_FMT_R32F};
-    fiber_status st = fiber_frame_fused(c, &scene, depth_host ? &depth : nullptr, &scene, stream_);
+    fiber_status st = fiber_frame_fused(c, nullptr, depth_host ? &depth : nullptr, nullptr, stream_);
+    if (st != FIBER_OK) return st;
+    FIBER_CUDA(cudaStreamWaitEvent(s, c->ev_in, 0));
+    st = run_composite(c, &scene, depth_host ? &depth : nullptr, &scene, s);
     if (st != FIBER_OK) return st;
     FIBER_CUDA(cudaMemcpyAsync(out_host, c->d_host_scene.p, W * H * 8, cudaMemcpyDeviceToHost, s));
+    FIBER_CUDA(cudaEventRecord(c->ev_out, s));
     return FIBER_OK;
 }
 

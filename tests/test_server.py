@@ -104,3 +104,49 @@ def test_budget_limits_slots_and_rejects_oversized_requests():
     out = np.zeros((120, 160, 4), np.float16)
     srv.wait(srv.submit(sid, cfg, cam, lcfg, lights, out))
     srv.close()
+
+
+def test_render_host_back_to_back():
+    # fiber_render_host uploads the scene image on a copy stream beside the
+    # frame; two calls queued back to back with different images (and a scene
+    # depth on the second) must each equal the same frame rendered alone.
+    import torch
+    scenes = _scenes()
+    rng = np.random.default_rng(11)
+    cfg, cam, lcfg, lights = _request(scenes[0], rng, 160, 120, 1)
+    bg_a = _background(160, 120)
+    bg_b = bg_a.copy()
+    bg_b[...] = np.array([0.3, 0.2, 0.1, 1.0], np.float16)
+    depth = np.zeros((120, 160), np.float32)
+    depth[:, :80] = 1e-3  # a far opaque wall over the left half
+    want_a = _alone(scenes[0], cfg, cam, lcfg, lights, bg_a)
+    st = abi.default_settings()
+    st.history_enabled = 0
+    p = StrandRasterizerPlugin()
+    abi.check(p.lib.fiber_settings_set(p.ctx, C.byref(st)), "fiber_settings_set")
+    p.add_geometry(scenes[0], StrandMaterial())
+    stream = torch.cuda.Stream()
+    h = C.c_void_p(stream.cuda_stream)
+    pinned = [torch.from_numpy(x).pin_memory() for x in (bg_a, bg_b, depth)]
+    outs = [torch.zeros((120, 160, 4), dtype=torch.float16).pin_memory() for _ in range(2)]
+    p.frame_begin_raw(cfg, cam, lcfg, lights, stream)
+    abi.check(p.lib.fiber_render_host(p.ctx, C.c_void_p(pinned[0].data_ptr()), None, C.c_void_p(outs[0].data_ptr()), h),
+              "fiber_render_host")
+    p.frame_begin_raw(cfg, cam, lcfg, lights, stream)
+    abi.check(p.lib.fiber_render_host(p.ctx, C.c_void_p(pinned[1].data_ptr()), C.c_void_p(pinned[2].data_ptr()),
+                                      C.c_void_p(outs[1].data_ptr()), h), "fiber_render_host")
+    stream.synchronize()
+    assert np.array_equal(outs[0].numpy().view(np.uint16), want_a.view(np.uint16))
+    # the second frame alone: the same scene image and depth through fresh calls
+    q = StrandRasterizerPlugin()
+    abi.check(q.lib.fiber_settings_set(q.ctx, C.byref(st)), "fiber_settings_set")
+    q.add_geometry(scenes[0], StrandMaterial())
+    q.frame_begin_raw(cfg, cam, lcfg, lights, None)
+    want_b = np.zeros_like(bg_b)
+    abi.check(q.lib.fiber_render_host(q.ctx, C.c_void_p(bg_b.ctypes.data), C.c_void_p(depth.ctypes.data),
+                                      C.c_void_p(want_b.ctypes.data), None), "fiber_render_host")
+    q.stats()
+    assert np.array_equal(outs[1].numpy().view(np.uint16), want_b.view(np.uint16))
+    assert not np.array_equal(outs[0].numpy().view(np.uint16), outs[1].numpy().view(np.uint16))
+    p.close()
+    q.close()
