@@ -112,6 +112,7 @@ struct fiber_ctx {
     DevBuf d_refs, d_ref_keys, d_active_flags, d_active_list, d_work, d_runs, d_big_cells;
     DevBuf d_visit_rec, d_visit_task, d_visit_rank, d_task_key, d_task_mat, d_cells_small, d_cells_large;
     DevBuf d_opaque;  // (covered, farthest depth q) per camera fine tile
+    DevBuf d_task_proj, d_ref_task;  // k_fine's projected end points per task; each reference's task
     DevBuf d_page_nvis, d_page_vbase, d_page_bucket;  // page-CSR backend
     DevBuf d_tel, d_tel_slots;                         // prepass telemetry
     DevBuf d_dom_page_table, d_dom_pool;               // sparse DOM residency
@@ -229,6 +230,8 @@ PrepassArgs prepass_args(fiber_ctx* c) {
     A.cells_small = dp<uint2>(c->d_cells_small);
     A.cells_large = dp<uint2>(c->d_cells_large);
     A.opaque_tiles = dp<uint2>(c->d_opaque);
+    A.task_proj = dp<float4>(c->d_task_proj);
+    A.ref_task = dp<uint32_t>(c->d_ref_task);
     if (c->settings.telemetry_enabled) {
         A.tel = dp<uint32_t>(c->d_tel);
         A.tel_slots = dp<uint32_t>(c->d_tel_slots);
@@ -253,6 +256,8 @@ RenderArgs render_args(fiber_ctx* c) {
     R.refs = dp<fiber_fine_seg_ref>(c->d_refs);
     R.work = dp<fiber_raster_work_item>(c->d_work);
     R.runs = dp<fiber_raster_tile_run>(c->d_runs);
+    R.ref_task = dp<uint32_t>(c->d_ref_task);
+    R.task_proj = dp<float4>(c->d_task_proj);
     R.dom_depth = dp<float>(c->d_dom_depth);
     R.dom_opacity = dp<float>(c->d_dom_opacity);
     R.dom_page_table = dp<uint32_t>(c->d_dom_page_table);
@@ -547,7 +552,8 @@ fiber_status fiber_ctx_destroy(fiber_ctx* c) {
                       &c->d_validate, &c->d_host_scene, &c->d_host_depth, &c->d_visit_rec,
                       &c->d_visit_task, &c->d_visit_rank, &c->d_task_key, &c->d_task_mat,
                       &c->d_cells_small, &c->d_cells_large, &c->d_opaque, &c->d_page_nvis, &c->d_page_vbase,
-                      &c->d_page_bucket, &c->d_tel, &c->d_tel_slots, &c->d_dom_page_table, &c->d_dom_pool};
+                      &c->d_page_bucket, &c->d_tel, &c->d_tel_slots, &c->d_dom_page_table, &c->d_dom_pool,
+                      &c->d_task_proj, &c->d_ref_task};
     for (DevBuf* b : bufs) release(c, *b);
     for (int i = 0; i <= kSpanCount; ++i)
         if (c->ev[i]) cudaEventDestroy(c->ev[i]);
@@ -849,6 +855,8 @@ fiber_status fiber_frame_begin(fiber_ctx* c, const fiber_froxel_config* cam_cfg,
     ENSURE(c->d_cells_small, std::min<uint64_t>(ref_cap, page_cap * kPageSize) * sizeof(uint2), false);
     ENSURE(c->d_cells_large, (ref_cap / 9 + 1) * sizeof(uint2), false);
     ENSURE(c->d_opaque, (uint64_t)c->camera_fine_tiles * sizeof(uint2), false);
+    ENSURE(c->d_task_proj, task_cap * 2 * sizeof(float4), false);
+    ENSURE(c->d_ref_task, ref_cap * 4, false);
     if (st.telemetry_enabled) {
         ENSURE(c->d_tel, sizeof(fiber_telemetry), false);
         ENSURE(c->d_tel_slots, table * 4, false);

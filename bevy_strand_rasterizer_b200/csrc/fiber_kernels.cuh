@@ -80,6 +80,8 @@ struct PrepassArgs {
     uint2* cells_small;            // (ref base, count) of cells with 1..8 references
     uint2* cells_large;            // (ref base, count) of cells with more than 8
     uint2* opaque_tiles;           // [camera fine tiles] (fully covered, quantised farthest opaque depth)
+    float4* task_proj;             // [task_capacity][2] both end points as world_to_screen_raw gave them
+    uint32_t* ref_task;            // [ref_capacity] binning task of each reference (after the cell sort)
     // Page-CSR backend only (null otherwise).
     uint32_t* page_nvis;           // [page_capacity] visits per page
     uint32_t* page_vbase;          // [page_capacity] first bucket entry of each page
@@ -107,6 +109,8 @@ struct RenderArgs {
     const fiber_fine_seg_ref* refs;
     const fiber_raster_work_item* work;
     const fiber_raster_tile_run* runs;
+    const uint32_t* ref_task;    // [refs] binning task of each reference
+    const float4* task_proj;     // [tasks][2] the task's end points as k_fine projected them
     float* dom_depth;        // [L][D][D] (dense layers)
     float* dom_opacity;      // [L][K][D][D] (dense layers)
     uint32_t* dom_page_table;  // [L][pages_x][pages_x] pool page + 1 (sparse residency)

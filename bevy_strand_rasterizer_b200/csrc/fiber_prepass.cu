@@ -280,6 +280,7 @@ constexpr int kFineWarps = kFineThreads / 32;
 struct SegOut {
     uint32_t seg;
     uint32_t p0, p1, dz;
+    float4 r0, r1;  // world_to_screen_raw of both end points, kept for the rasters
 };
 
 __device__ __forceinline__ bool fine_segment(const FrameParams& P, const InstanceView& in, uint32_t f,
@@ -298,18 +299,21 @@ __device__ __forceinline__ bool fine_segment(const FrameParams& P, const Instanc
         return false;
     float ssx = wmax(1.0f, vw), ssy = wmax(1.0f, vh);
     o.seg = seg;
+    o.r0 = r0;
+    o.r1 = r1;
     o.p0 = pack2x16unorm(wclamp(c0.x / ssx, 0.0f, 1.0f), wclamp(c0.y / ssy, 0.0f, 1.0f));
     o.p1 = pack2x16unorm(wclamp(c1.x / ssx, 0.0f, 1.0f), wclamp(c1.y / ssy, 0.0f, 1.0f));
     o.dz = pack2x16unorm(wclamp(c0.z, 0.0f, 1.0f), wclamp(c1.z, 0.0f, 1.0f));
     return true;
 }
 
-__global__ void __launch_bounds__(kFineThreads) k_fine(const FrameParams* __restrict__ Pp,
+__global__ void __launch_bounds__(kFineThreads, 4) k_fine(const FrameParams* __restrict__ Pp,
                                                        const InstanceView* __restrict__ inst, PrepassArgs A) {
     const FrameParams& P = *Pp;
     __shared__ uint32_t s_tile;
     __shared__ uint32_t s_warp_count[kFineWarps];
     __shared__ uint32_t s_base;
+    __shared__ float4 s_proj[kFineWarps][2][32];  // pass A's first-chunk projections, until pass B stores them
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t tiles_per_f = ceil_div(P.total_strands, kFineWarps);
     const uint32_t n_tiles = tiles_per_f * P.F;
@@ -350,12 +354,20 @@ __global__ void __launch_bounds__(kFineThreads) k_fine(const FrameParams* __rest
         if (A.tel && lane == 0 && nseg > 0u) atomicAdd(tel_frustum(A.tel, f, kTelRetainedStrands), 1u);
         // Pass A: count (results of the first 32 segments stay in registers).
         uint32_t count = 0;
-        SegOut first{};
+        uint32_t first_seg = 0u, first_p0 = 0u, first_p1 = 0u, first_dz = 0u;
         bool first_ok = false;
         for (uint32_t c = 0; c < nseg; c += 32u) {
             SegOut o;
             bool ok = (c + lane < nseg) && fine_segment(P, inst[i], f, meta_offset + c + lane, o);
-            if (c == 0u) { first = o; first_ok = ok; }
+            if (c == 0u) {
+                first_seg = o.seg;
+                first_p0 = o.p0;
+                first_p1 = o.p1;
+                first_dz = o.dz;
+                first_ok = ok;
+                s_proj[warp][0][lane] = o.r0;
+                s_proj[warp][1][lane] = o.r1;
+            }
             count += __popc(__ballot_sync(0xFFFFFFFFu, ok));
         }
         if (lane == 0) s_warp_count[warp] = count;
@@ -378,9 +390,18 @@ __global__ void __launch_bounds__(kFineThreads) k_fine(const FrameParams* __rest
         for (int w = 0; w < warp; ++w) out += s_warp_count[w];
         // Pass B: write in segment order.
         for (uint32_t c = 0; c < nseg; c += 32u) {
-            SegOut o = first;
+            SegOut o;
             bool ok = first_ok;
-            if (c != 0u) ok = (c + lane < nseg) && fine_segment(P, inst[i], f, meta_offset + c + lane, o);
+            if (c == 0u) {
+                o.seg = first_seg;
+                o.p0 = first_p0;
+                o.p1 = first_p1;
+                o.dz = first_dz;
+                o.r0 = s_proj[warp][0][lane];
+                o.r1 = s_proj[warp][1][lane];
+            } else {
+                ok = (c + lane < nseg) && fine_segment(P, inst[i], f, meta_offset + c + lane, o);
+            }
             uint32_t mask = __ballot_sync(0xFFFFFFFFu, ok);
             if (ok) {
                 uint32_t dst = out + __popc(mask & ((1u << lane) - 1u));
@@ -388,6 +409,8 @@ __global__ void __launch_bounds__(kFineThreads) k_fine(const FrameParams* __rest
                     reinterpret_cast<uint4*>(A.tasks)[dst] = make_uint4(i, s, o.seg, packed);
                     fiber_projected_segment ps{o.p0, o.p1, o.dz};
                     A.projected[dst] = ps;
+                    A.task_proj[2u * (size_t)dst] = o.r0;
+                    A.task_proj[2u * (size_t)dst + 1u] = o.r1;
                 } else {
                     atomicOr(&A.counters->overflow, 1u);
                 }
@@ -1035,28 +1058,32 @@ __global__ void __launch_bounds__(kScanThreads) k_compact_active(const FramePara
 // The reference of binning task k (make_fine_seg_ref, :1313-1327) as a sort
 // key (depth key, instance, segment) and its material, as k_visit stored them
 // (12 B per task, which a frame's L2 mostly holds).
+// A cell entry: the task's canonical-order key and the task index; the sort
+// moves the pair, and the store writes the reference (with the task's
+// material), its depth key and its task.
 __device__ __forceinline__ void task_entry(const PrepassArgs& A, const InstanceView* __restrict__ /*inst*/,
-                                           uint32_t k, unsigned long long& key, uint32_t& mat) {
+                                           uint32_t k, unsigned long long& key, uint32_t& task) {
     key = A.task_key[k];
-    mat = A.task_mat[k];
+    task = k;
 }
 
-__device__ __forceinline__ void store_entry(const PrepassArgs& A, uint32_t dst, unsigned long long key, uint32_t mat) {
-    A.refs[dst] = fiber_fine_seg_ref{(uint32_t)(key >> 32) & 0x7FFFu, (uint32_t)key, mat};
+__device__ __forceinline__ void store_entry(const PrepassArgs& A, uint32_t dst, unsigned long long key, uint32_t task) {
+    A.refs[dst] = fiber_fine_seg_ref{(uint32_t)(key >> 32) & 0x7FFFu, (uint32_t)key, A.task_mat[task]};
     A.ref_keys[dst] = 0x1FFFFu - (uint32_t)(key >> 47);
+    A.ref_task[dst] = task;
 }
 
 template <int R>
 __device__ __forceinline__ void warp_sort_cell(const PrepassArgs& A, const InstanceView* __restrict__ inst,
                                                uint32_t base, uint32_t n, int lane) {
     unsigned long long k[R];
-    uint32_t mat[R];
+    uint32_t task[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) {
         const uint32_t e = (uint32_t)lane * R + r;
         k[r] = ~0ull;
-        mat[r] = 0u;
-        if (e < n) task_entry(A, inst, A.ref_keys[base + e], k[r], mat[r]);
+        task[r] = 0u;
+        if (e < n) task_entry(A, inst, A.ref_keys[base + e], k[r], task[r]);
     }
 #pragma unroll
     for (int size = 2; size <= 32 * R; size <<= 1) {
@@ -1067,11 +1094,11 @@ __device__ __forceinline__ void warp_sort_cell(const PrepassArgs& A, const Insta
                 for (int r = 0; r < R; ++r) {
                     const int e = lane * R + r;
                     unsigned long long ok = __shfl_xor_sync(0xFFFFFFFFu, k[r], stride / R);
-                    uint32_t om = __shfl_xor_sync(0xFFFFFFFFu, mat[r], stride / R);
+                    uint32_t om = __shfl_xor_sync(0xFFFFFFFFu, task[r], stride / R);
                     const bool up = (e & size) == 0;
                     const bool lower = (e & stride) == 0;
                     const bool take_other = lower == up ? (ok < k[r]) : (ok > k[r]);
-                    if (take_other) { k[r] = ok; mat[r] = om; }
+                    if (take_other) { k[r] = ok; task[r] = om; }
                 }
             } else {
 #pragma unroll
@@ -1082,7 +1109,7 @@ __device__ __forceinline__ void warp_sort_cell(const PrepassArgs& A, const Insta
                         const bool up = (e & size) == 0;
                         if (up ? (k[r] > k[r2]) : (k[r] < k[r2])) {
                             unsigned long long tk = k[r]; k[r] = k[r2]; k[r2] = tk;
-                            uint32_t tm = mat[r]; mat[r] = mat[r2]; mat[r2] = tm;
+                            uint32_t tt = task[r]; task[r] = task[r2]; task[r2] = tt;
                         }
                     }
                 }
@@ -1092,7 +1119,7 @@ __device__ __forceinline__ void warp_sort_cell(const PrepassArgs& A, const Insta
 #pragma unroll
     for (int r = 0; r < R; ++r) {
         const uint32_t e = (uint32_t)lane * R + r;
-        if (e < n) store_entry(A, base + e, k[r], mat[r]);
+        if (e < n) store_entry(A, base + e, k[r], task[r]);
     }
 }
 
@@ -1110,17 +1137,17 @@ __device__ __forceinline__ void warp_sort_any(const PrepassArgs& A, const Instan
 __device__ __forceinline__ void thread_sort_cell(const PrepassArgs& A, const InstanceView* __restrict__ inst,
                                                  uint32_t base, uint32_t n) {
     unsigned long long k[8];
-    uint32_t mat[8];
+    uint32_t task[8];
 #pragma unroll
     for (int e = 0; e < 8; ++e) {
         k[e] = ~0ull;
-        mat[e] = 0u;
-        if ((uint32_t)e < n) task_entry(A, inst, A.ref_keys[base + e], k[e], mat[e]);
+        task[e] = 0u;
+        if ((uint32_t)e < n) task_entry(A, inst, A.ref_keys[base + e], k[e], task[e]);
     }
     auto cas = [&](int a, int b) {
         if (k[a] > k[b]) {
             const unsigned long long tk = k[a]; k[a] = k[b]; k[b] = tk;
-            const uint32_t tm = mat[a]; mat[a] = mat[b]; mat[b] = tm;
+            const uint32_t tt = task[a]; task[a] = task[b]; task[b] = tt;
         }
     };
     cas(0, 1); cas(2, 3); cas(4, 5); cas(6, 7);
@@ -1131,7 +1158,7 @@ __device__ __forceinline__ void thread_sort_cell(const PrepassArgs& A, const Ins
     cas(1, 2); cas(3, 4); cas(5, 6);
 #pragma unroll
     for (int e = 0; e < 8; ++e)
-        if ((uint32_t)e < n) store_entry(A, base + e, k[e], mat[e]);
+        if ((uint32_t)e < n) store_entry(A, base + e, k[e], task[e]);
 }
 
 // One warp per active tile: the tile's 256 depth slots (16 coarse z x 16 fine
@@ -1222,9 +1249,9 @@ __device__ __forceinline__ void convert_big_cell(const PrepassArgs& A, const Ins
                                                  uint32_t b, uint32_t n, uint32_t lane) {
     for (uint32_t j = lane; j < n; j += 32u) {
         unsigned long long key;
-        uint32_t mat;
-        task_entry(A, inst, A.ref_keys[b + j], key, mat);
-        store_entry(A, b + j, key, mat);
+        uint32_t task;
+        task_entry(A, inst, A.ref_keys[b + j], key, task);
+        store_entry(A, b + j, key, task);
     }
     if (lane == 0u) {
         const uint32_t slot = atomicAdd(&A.counters->big_cells, 1u);
@@ -1397,7 +1424,7 @@ __device__ __forceinline__ void big_load(const PrepassArgs& A, uint32_t base, ui
     if (i < n) {
         fiber_fine_seg_ref r = A.refs[base + i];
         k = ref_sort_key(A.ref_keys[base + i], r.inst_id, r.seg_id);
-        m = r.material_idx;
+        m = A.ref_task[base + i];
     } else {
         k = ~0ull;
         m = 0u;
@@ -1405,8 +1432,9 @@ __device__ __forceinline__ void big_load(const PrepassArgs& A, uint32_t base, ui
 }
 __device__ __forceinline__ void big_store(const PrepassArgs& A, uint32_t base, uint32_t i, unsigned long long k,
                                           uint32_t m) {
-    A.refs[base + i] = fiber_fine_seg_ref{(uint32_t)(k >> 32) & 0x7FFFu, (uint32_t)k, m};
+    A.refs[base + i] = fiber_fine_seg_ref{(uint32_t)(k >> 32) & 0x7FFFu, (uint32_t)k, A.task_mat[m]};
     A.ref_keys[base + i] = 0x1FFFFu - (uint32_t)(k >> 47);
+    A.ref_task[base + i] = m;
 }
 // Pair t of a stage: (i, j) with i < j.
 __device__ __forceinline__ void bitonic_pair(uint32_t t, uint32_t size, uint32_t stride, bool flip, uint32_t& i,

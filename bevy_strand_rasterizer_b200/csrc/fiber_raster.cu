@@ -274,11 +274,13 @@ __global__ void __launch_bounds__(kShadowThreads, 14) k_shadow(const FrameParams
             for (uint32_t s = threadIdx.x; s < rp.n; s += blockDim.x) {
                 uint32_t item, j;
                 slot_source(s_prefix, rp, s, item, j);
-                const fiber_fine_seg_ref ref = R.refs[s_wbase[item] + j];
+                const uint32_t slot = s_wbase[item] + j;
+                const fiber_fine_seg_ref ref = R.refs[slot];
                 const InstanceView& in = inst[ref.inst_id];
-                float4 w0, w1;
-                segment_world(in, ref.seg_id, w0, w1);
-                float4 a = world_to_screen_raw(w0, clip, vw, vh), b = world_to_screen_raw(w1, clip, vw, vh);
+                // The end points as k_fine projected them for this frustum
+                // (world_to_screen_raw of the segment's vertices).
+                const uint32_t t = __ldg(R.ref_task + slot);
+                const float4 a = __ldg(R.task_proj + 2u * (size_t)t), b = __ldg(R.task_proj + 2u * (size_t)t + 1u);
                 const fiber_strand_material& m = in.materials[ref.material_idx];
                 sp0x[s] = a.x; sp0y[s] = a.y; sp0z[s] = normalize_depth01(a.z);
                 sp1x[s] = b.x; sp1y[s] = b.y; sp1z[s] = normalize_depth01(b.z);
@@ -625,11 +627,12 @@ __global__ void __launch_bounds__(kCamThreads) k_raster(const FrameParams* __res
             for (uint32_t s = threadIdx.x; s < rp.n; s += blockDim.x) {
                 uint32_t item, j;
                 slot_source(s_prefix, rp, s, item, j);
-                const fiber_fine_seg_ref ref = R.refs[s_wbase[item] + j];
+                const uint32_t slot = s_wbase[item] + j;
+                const fiber_fine_seg_ref ref = R.refs[slot];
                 const InstanceView& in = inst[ref.inst_id];
-                float4 w0, w1;
-                segment_world(in, ref.seg_id, w0, w1);
-                float4 a = world_to_screen_raw(w0, clip, vw, vh), b = world_to_screen_raw(w1, clip, vw, vh);
+                // The end points as k_fine projected them for this frustum.
+                const uint32_t t = __ldg(R.ref_task + slot);
+                const float4 a = __ldg(R.task_proj + 2u * (size_t)t), b = __ldg(R.task_proj + 2u * (size_t)t + 1u);
                 uint16_t tag = (uint16_t)((item << 2) | (j & 3u));
                 if (!(a.x < 0.0f && b.x < 0.0f)) {
                     const fiber_strand_material& m = in.materials[ref.material_idx];
