@@ -120,6 +120,9 @@ struct fiber_ctx {
     // beside the frame; ev_in = uploaded, ev_out = the last download queued.
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+    // The prepass's cell sort runs on this stream beside the emit.
+    cudaStream_t side_stream = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     uint32_t camera_fine_tiles = 0;
     bool opaque_frame = false;  // fiber_opaque_depth ran since fiber_frame_begin
     // A batch graph advanced this context's epoch on the device: the next
@@ -378,13 +381,23 @@ fiber_status run_prepass(fiber_ctx* c, cudaStream_t s, const OpaqueSource* opaqu
     if (csr) launch_fill_walk(L, A);
     else launch_fill(L, A);
     record(c, 7, s);
+    // The cell sort needs only the fill; the active-tile compaction and the
+    // emit need only the counts. The sort runs on the side stream beside
+    // them (a branch of the frame graph when captured) and joins before the
+    // rasters.
+    FIBER_CUDA(cudaEventRecord(c->ev_fork, s));
+    FIBER_CUDA(cudaStreamWaitEvent(c->side_stream, c->ev_fork, 0));
+    LaunchCtx Ls = L;
+    Ls.stream = c->side_stream;
+    launch_sort_cells(Ls, A);
+    launch_sort_big(Ls, A);
+    FIBER_CUDA(cudaEventRecord(c->ev_join, c->side_stream));
     set_stage(c, A, kStageActive);
     launch_compact_active(L, A);
     record(c, 8, s);
     set_stage(c, A, kStageEmit);
     launch_emit(L, A);
-    launch_sort_cells(L, A);
-    launch_sort_big(L, A);
+    FIBER_CUDA(cudaStreamWaitEvent(s, c->ev_join, 0));
     if (L.telemetry) launch_telemetry(L, A);
     return check_launch();
 }
@@ -525,7 +538,14 @@ fiber_status fiber_ctx_create(int device, uint64_t hbm_budget, fiber_ctx** out) 
     c->events_ok = true;
     for (int i = 0; i <= kSpanCount; ++i)
         if (cudaEventCreate(&c->ev[i]) != cudaSuccess) c->events_ok = false;
-    fiber_status st = ensure(c, c->d_counters, sizeof(FrameCounters), true);
+    fiber_status st = FIBER_OK;
+    if (cudaStreamCreateWithFlags(&c->side_stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming) != cudaSuccess) {
+        cudaGetLastError();
+        st = FIBER_ECUDA;
+    }
+    if (st == FIBER_OK) st = ensure(c, c->d_counters, sizeof(FrameCounters), true);
     if (st == FIBER_OK) st = ensure(c, c->d_validate, 64, true);
     if (st != FIBER_OK) {
         fiber_ctx_destroy(c);
@@ -558,6 +578,9 @@ fiber_status fiber_ctx_destroy(fiber_ctx* c) {
     for (int i = 0; i <= kSpanCount; ++i)
         if (c->ev[i]) cudaEventDestroy(c->ev[i]);
     if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
+    if (c->side_stream) cudaStreamDestroy(c->side_stream);
+    if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+    if (c->ev_join) cudaEventDestroy(c->ev_join);
     if (c->ev_in) cudaEventDestroy(c->ev_in);
     if (c->ev_out) cudaEventDestroy(c->ev_out);
     delete c;
