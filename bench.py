@@ -168,15 +168,17 @@ def algorithmic_bytes(st, w, n_lights: int, K: int, D: int) -> dict:
     WH = w.width * w.height
     dom = n_lights * 4 * (K + 1) * D * D
     per = {
-        "k_fine": 20 * P + 16 * S + sum(28 * n for n in tasks),
+        "k_fine": 20 * P + 16 * S + sum(60 * n for n in tasks),  # + 32 B projected end points per task
         "k_visit": sum(40 * n for n in tasks) + sum(8 * r for r in refs),
         "k_count_visits": sum(16 * r for r in refs),
         "k_fill_visits": sum(20 * r for r in refs),
         "k_prefix_pages": sum(8 * 256 * p for p in pages),
-        "k_emit+k_sort_cells": sum(32 * (wk + t) + 32 * r for wk, t, r in zip(work, runs, refs)),
-        "k_shadow": sum(52 * refs[f] + 32 * (work[f] + runs[f]) for f in range(1, F)) + dom,
+        "k_emit+k_sort_cells": sum(32 * (wk + t) + 36 * r for wk, t, r in zip(work, runs, refs)),
+        # the rasters stage a reference from its 12 B record, its task index
+        # and the task's 32 B of projected end points
+        "k_shadow": sum(48 * refs[f] + 32 * (work[f] + runs[f]) for f in range(1, F)) + dom,
         "k_shade": st.camera_tasks * (40 + 8 * n_lights),
-        "k_raster": 52 * refs[0] + 32 * (work[0] + runs[0]) + 12 * WH,
+        "k_raster": 48 * refs[0] + 32 * (work[0] + runs[0]) + 12 * WH,
     }
     # The frame's B_alg is the path's own formula (fixed before any kernel was
     # written); the per-kernel figures above add this implementation's records.
