@@ -1264,7 +1264,7 @@ __device__ __forceinline__ void convert_big_cell(const PrepassArgs& A, const Ins
 // made: a thread per cell of up to 8 references (nearly all of them), then a
 // warp per larger cell. A cell longer than a warp sort is converted in place
 // by its warp and queued for k_sort_big_cells.
-__global__ void __launch_bounds__(256, 4) k_sort_cells(const InstanceView* __restrict__ inst, PrepassArgs A) {
+__global__ void __launch_bounds__(256, 5) k_sort_cells(const InstanceView* __restrict__ inst, PrepassArgs A) {
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t n_small = *((volatile uint32_t*)&A.counters->small_cells);
     const uint32_t n_large = *((volatile uint32_t*)&A.counters->large_cells);
