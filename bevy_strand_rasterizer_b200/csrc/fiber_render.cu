@@ -224,7 +224,7 @@ __device__ F3 marschner(F3 L, F3 V, F3 U, const fiber_strand_material& m, float 
     return f3(tot[0], tot[1], tot[2]);
 }
 
-__global__ void __launch_bounds__(128, 6) k_shade(const FrameParams* __restrict__ Pp,
+__global__ void __launch_bounds__(128, 8) k_shade(const FrameParams* __restrict__ Pp,
                                                const InstanceView* __restrict__ inst, RenderArgs R) {
     const FrameParams& P = *Pp;
     __shared__ QuadTable s_quad;
