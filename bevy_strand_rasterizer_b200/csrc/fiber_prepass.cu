@@ -715,8 +715,8 @@ __device__ __forceinline__ bool visits_unused(const PrepassArgs& A) {
     return *((volatile uint32_t*)&A.counters->visit_overflow) != 0u;
 }
 
-// K7: page marks + visit records. Blocks walk 256 tasks at a time; each task's
-// first kVisitSlots visits go to shared memory, the block reserves room for all
+// K7: page marks + visit records. Warps walk 32 tasks at a time; each task's
+// first kVisitSlots visits go to shared memory, the warp reserves room for all
 // its visits with one atomic, and a task with more visits walks again to write
 // the rest. When the records do not fit (or slots exceed 24 bits) the pass
 // still marks every page and raises visit_overflow, which hands count and fill
@@ -728,15 +728,18 @@ __global__ void __launch_bounds__(kVisitThreads, 4) k_visit(const FrameParams* _
                                                             const InstanceView* __restrict__ inst, PrepassArgs A) {
     const FrameParams& P = *Pp;
     __shared__ uint32_t s_buf[kVisitSlots * kVisitThreads];
-    __shared__ uint32_t s_warp[33];
-    __shared__ uint32_t s_base;
     const uint32_t n = *((volatile uint32_t*)&A.counters->tasks);
     const uint32_t n_cap = min(n, P.task_capacity);
     const bool records = P.visit_records != 0u;
     const uint2* opq = kOpaque ? A.opaque_tiles : nullptr;
     if (!records && blockIdx.x == 0 && threadIdx.x == 0) atomicOr(&A.counters->visit_overflow, 1u);
-    for (uint32_t k0 = blockIdx.x * kVisitThreads; k0 < n_cap; k0 += gridDim.x * kVisitThreads) {
-        const uint32_t k = k0 + threadIdx.x;
+    // Warps take 32 tasks at a time and reserve their records on their own,
+    // so a warp never waits for the slowest walk of its block.
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t warp_id = (blockIdx.x * kVisitThreads + threadIdx.x) >> 5;
+    const uint32_t warps = gridDim.x * (kVisitThreads / 32u);
+    for (uint32_t k0 = warp_id * 32u; k0 < n_cap; k0 += warps * 32u) {
+        const uint32_t k = k0 + lane;
         TaskWalk w;
         const bool ok = k < n_cap && task_walk(P, A, k, w);
         VisitSink<kTel> vs{A.page_table, s_buf + threadIdx.x, 0u, 0u, records, A.tel_slots};
@@ -750,21 +753,24 @@ __global__ void __launch_bounds__(kVisitThreads, 4) k_visit(const FrameParams* _
             walk_task(P, A, w, opq, vs);
         }
         if (!records) continue;
-        uint32_t total;
-        const uint32_t excl = block_exclusive_scan<kVisitThreads>(vs.n, s_warp, total);
-        if (threadIdx.x == 0) {
-            uint32_t base = kInvalid;
-            if (total > 0u && !visits_unused(A)) {
-                const unsigned long long b = atomicAdd(&A.counters->visits, (unsigned long long)total);
-                if (b + total <= (unsigned long long)P.ref_capacity) base = (uint32_t)b;
-                else atomicOr(&A.counters->visit_overflow, 1u);
-            }
-            s_base = base;
+        uint32_t incl = vs.n;
+#pragma unroll
+        for (uint32_t o = 1; o < 32u; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+            if (lane >= o) incl += y;
         }
-        __syncthreads();
-        const uint32_t base = s_base;
+        const uint32_t total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+        uint32_t base = kInvalid;
+        if (lane == 31u && total > 0u && !visits_unused(A)) {
+            const unsigned long long b = atomicAdd(&A.counters->visits, (unsigned long long)total);
+            if (b + total <= (unsigned long long)P.ref_capacity) base = (uint32_t)b;
+            else atomicOr(&A.counters->visit_overflow, 1u);
+        }
+        base = __shfl_sync(0xFFFFFFFFu, base, 31);
         if (base != kInvalid && vs.n > 0u) {
-            const uint32_t at = base + excl;
+            // Visit records are placed in reservation order; the count and fill
+            // passes and the cell sort make the references independent of it.
+            const uint32_t at = base + incl - vs.n;
             const uint32_t nb = min(vs.n, kVisitSlots);
             for (uint32_t j = 0; j < nb; ++j) {
                 A.visit_rec[at + j] = s_buf[j * kVisitThreads + threadIdx.x];
@@ -775,7 +781,6 @@ __global__ void __launch_bounds__(kVisitThreads, 4) k_visit(const FrameParams* _
                 walk_task(P, A, w, opq, sp);
             }
         }
-        __syncthreads();  // s_buf and s_base are rewritten by the next round
     }
 }
 
