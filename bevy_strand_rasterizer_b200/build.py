@@ -2,7 +2,8 @@
 
 The library is compiled with --fmad=false and IEEE division / square root so
 that the integer-deciding stages (projection, clipping, depth quantisation,
-DDA traversal) reproduce binary32 results operation by operation.
+DDA traversal) reproduce binary32 results operation by operation; the shading
+file alone (compared within a tolerance) is compiled with contraction.
 """
 from __future__ import annotations
 
@@ -31,6 +32,22 @@ NVCC_FLAGS = [
 ]
 
 
+# Shading and composite are compared within a tolerance (they end in binary16),
+# so their file is compiled with contraction and approximate division and
+# square root. What selects a DOM texel and slice there (projection, depth
+# normalisation, the slice quotient) is written with correctly rounded
+# intrinsics and stays exact.
+FAST_FP_SOURCES = {"fiber_render.cu"}
+FAST_FP = {"--fmad=false": "--fmad=true", "-prec-div=true": "-prec-div=false", "-prec-sqrt=true": "-prec-sqrt=false"}
+
+
+def flags_for(src: str) -> list[str]:
+    """nvcc flags of one source file."""
+    if src in FAST_FP_SOURCES:
+        return [FAST_FP.get(f, f) for f in NVCC_FLAGS]
+    return list(NVCC_FLAGS)
+
+
 def _nvcc() -> str:
     cuda_home = os.environ.get("CUDA_HOME", "/usr/local/cuda")
     cand = Path(cuda_home) / "bin" / "nvcc"
@@ -56,7 +73,7 @@ def build(verbose: bool = False, force: bool = False, ptxas_info: bool = False) 
     extra = ["-Xptxas", "-v"] if ptxas_info else []
     for src in SOURCES:
         obj = obj_dir / (Path(src).stem + ".o")
-        cmd = [_nvcc(), *NVCC_FLAGS, *extra, "-I", str(include), "-c", str(CSRC / src), "-o", str(obj)]
+        cmd = [_nvcc(), *flags_for(src), *extra, "-I", str(include), "-c", str(CSRC / src), "-o", str(obj)]
         if verbose:
             print(" ".join(cmd), file=sys.stderr)
         subprocess.run(cmd, check=True)

@@ -118,27 +118,33 @@ __device__ __forceinline__ uint32_t ceil_div(uint32_t x, uint32_t y) { return (x
 struct F3 { float x, y, z; };
 __device__ __forceinline__ F3 f3(float x, float y, float z) { return F3{x, y, z}; }
 
+// The projection helpers below spell every operation as a correctly rounded
+// intrinsic, so they give the same binary32 results in a translation unit
+// compiled with contraction and approximate division (the shading's).
+__device__ __forceinline__ float row4(float a, float x, float b, float y, float c, float z, float d, float w) {
+    return __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(a, x), __fmul_rn(b, y)), __fmul_rn(c, z)), __fmul_rn(d, w));
+}
 __device__ __forceinline__ float4 matvec(const float* m, float x, float y, float z, float w) {
     float4 r;
-    r.x = ((m[0] * x + m[4] * y) + m[8] * z) + m[12] * w;
-    r.y = ((m[1] * x + m[5] * y) + m[9] * z) + m[13] * w;
-    r.z = ((m[2] * x + m[6] * y) + m[10] * z) + m[14] * w;
-    r.w = ((m[3] * x + m[7] * y) + m[11] * z) + m[15] * w;
+    r.x = row4(m[0], x, m[4], y, m[8], z, m[12], w);
+    r.y = row4(m[1], x, m[5], y, m[9], z, m[13], w);
+    r.z = row4(m[2], x, m[6], y, m[10], z, m[14], w);
+    r.w = row4(m[3], x, m[7], y, m[11], z, m[15], w);
     return r;
 }
 
 // common.wgsl:206-212
 __device__ __forceinline__ float normalize_depth01(float z) {
     if (z >= 0.0f && z <= 1.0f) return z;
-    return wclamp(z * 0.5f + 0.5f, 0.0f, 1.0f);
+    return wclamp(__fadd_rn(__fmul_rn(z, 0.5f), 0.5f), 0.0f, 1.0f);
 }
 // common.wgsl:93-107 -> (sx, sy, ndc z, clip w)
 __device__ __forceinline__ float4 world_to_screen_raw(float4 p, const float* clip, float vw, float vh) {
     float4 c = matvec(clip, p.x, p.y, p.z, p.w);
     if (c.w <= 0.0f) return make_float4(-1.0f, -1.0f, -1.0f, -1.0f);
-    float nx = c.x / c.w, ny = c.y / c.w, nz = c.z / c.w;
-    float sx = 0.0f + (nx * 0.5f + 0.5f) * vw;
-    float sy = 0.0f + (ny * -0.5f + 0.5f) * vh;
+    float nx = __fdiv_rn(c.x, c.w), ny = __fdiv_rn(c.y, c.w), nz = __fdiv_rn(c.z, c.w);
+    float sx = __fadd_rn(0.0f, __fmul_rn(__fadd_rn(__fmul_rn(nx, 0.5f), 0.5f), vw));
+    float sy = __fadd_rn(0.0f, __fmul_rn(__fadd_rn(__fmul_rn(ny, -0.5f), 0.5f), vh));
     return make_float4(sx, sy, nz, c.w);
 }
 // common.wgsl:229-242

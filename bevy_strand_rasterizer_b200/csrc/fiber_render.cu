@@ -19,13 +19,26 @@ __constant__ float c_mp_den[5] = {1.0f, 4.0f, 64.0f, 2304.0f, 147456.0f};  // 4^
 constexpr float kPi = 3.14159265359f;
 constexpr float kPiHalf = kPi / 2.0f;
 
-__device__ __forceinline__ F3 nrm3(F3 v) {
-    float l = sqrtf(v.x * v.x + v.y * v.y + v.z * v.z);
-    return f3(v.x / l, v.y / l, v.z / l);
+// This file is compiled with contraction and approximate division. The
+// shading frame (tangent, view and light directions, their projections and
+// the angles between them) is spelt with correctly rounded intrinsics, so an
+// acos argument lands on the same side of +-1 as the reference's and an
+// antiparallel or degenerate frame gives the same NaN; the smooth terms after
+// it (the Mp series, the quadrature, the detectors) run on the fast path.
+__device__ __forceinline__ float dot3(F3 a, F3 b) {
+    return __fadd_rn(__fadd_rn(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y)), __fmul_rn(a.z, b.z));
 }
-__device__ __forceinline__ float dot3(F3 a, F3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ F3 nrm3(F3 v) {
+    const float l = __fsqrt_rn(dot3(v, v));
+    return f3(__fdiv_rn(v.x, l), __fdiv_rn(v.y, l), __fdiv_rn(v.z, l));
+}
 __device__ __forceinline__ F3 cross3(F3 a, F3 b) {
-    return f3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+    return f3(__fsub_rn(__fmul_rn(a.y, b.z), __fmul_rn(a.z, b.y)), __fsub_rn(__fmul_rn(a.z, b.x), __fmul_rn(a.x, b.z)),
+              __fsub_rn(__fmul_rn(a.x, b.y), __fmul_rn(a.y, b.x)));
+}
+// v - w * s, per component.
+__device__ __forceinline__ F3 sub_scaled3(F3 v, F3 w, float s) {
+    return f3(__fsub_rn(v.x, __fmul_rn(w.x, s)), __fsub_rn(v.y, __fmul_rn(w.y, s)), __fsub_rn(v.z, __fmul_rn(w.z, s)));
 }
 
 __device__ float sample_dom(const FrameParams& P, const RenderArgs& R, F3 pw, uint32_t layer) {
@@ -50,7 +63,7 @@ __device__ float sample_dom(const FrameParams& P, const RenderArgs& R, F3 pw, ui
     if (z0 <= 0.0f) return 1.0f;
     float z = normalize_depth01(raw.z);
     if (z > z0 - 1e-3f) return 1.0f;
-    float u = wclamp(wmax(0.0f, z0 - z) / wmax(z0, 1e-6f), 0.0f, 1.0f);  // pow(., DOM_GAMMA = 1)
+    float u = wclamp(__fdiv_rn(wmax(0.0f, z0 - z), wmax(z0, 1e-6f)), 0.0f, 1.0f);  // pow(., DOM_GAMMA = 1)
     uint32_t slice = min(f2u(floorf(u * u2f(K))), K - 1u);
     float op = dop[slice * ds];
     return wclamp(1.0f - op, 0.08f, 1.0f);
@@ -137,8 +150,8 @@ __device__ F3 marschner(F3 L, F3 V, F3 U, const fiber_strand_material& m, float 
     float theta_i = acosf(dot3(L, U));
     float theta_r = acosf(dot3(L, V));
     float dUL = dot3(U, L), dVL = dot3(V, L);
-    F3 lp = nrm3(f3(U.x - L.x * dUL, U.y - L.y * dUL, U.z - L.z * dUL));
-    F3 vp = nrm3(f3(V.x - L.x * dVL, V.y - L.y * dVL, V.z - L.z * dVL));
+    F3 lp = nrm3(sub_scaled3(U, L, dUL));
+    F3 vp = nrm3(sub_scaled3(V, L, dVL));
     float ang = acosf(dot3(nrm3(lp), nrm3(vp)));
     float sd = dot3(cross3(lp, vp), L);
     float phi = ang * (sd > 0.0f ? 1.0f : (sd < 0.0f ? -1.0f : 0.0f));
@@ -240,8 +253,9 @@ __global__ void __launch_bounds__(128, 8) k_shade(const FrameParams* __restrict_
         const fiber_strand_meta sm = in.meta[t.y];
         float4 v0, v1;
         segment_world(in, seg, v0, v1);
-        F3 U = nrm3(f3(v1.x - v0.x, v1.y - v0.y, v1.z - v0.z));
-        F3 cam = nrm3(f3(P.camera_pos[0] - v0.x, P.camera_pos[1] - v0.y, P.camera_pos[2] - v0.z));
+        F3 U = nrm3(f3(__fsub_rn(v1.x, v0.x), __fsub_rn(v1.y, v0.y), __fsub_rn(v1.z, v0.z)));
+        F3 cam = nrm3(f3(__fsub_rn(P.camera_pos[0], v0.x), __fsub_rn(P.camera_pos[1], v0.y),
+                         __fsub_rn(P.camera_pos[2], v0.z)));
         F3 B = nrm3(cross3(U, cam));
         F3 V = nrm3(cross3(B, U));
         const fiber_strand_material mat = in.materials[sm.material_idx];
