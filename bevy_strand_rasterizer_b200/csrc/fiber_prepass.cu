@@ -809,14 +809,16 @@ __global__ void __launch_bounds__(256) k_count_visits(PrepassArgs A) {
 __global__ void __launch_bounds__(256) k_fill_visits(PrepassArgs A) {
     if (visits_unused(A)) return;
     const uint32_t n = (uint32_t)*((volatile unsigned long long*)&A.counters->visits);
+    // The visit records stream through once (evict-first loads), so L2 keeps
+    // the scattered task-index lines until their sectors are complete.
     for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
-        const uint32_t g = A.visit_rec[r];
+        const uint32_t g = __ldcs(A.visit_rec + r);
         if (g == kInvalid) continue;
         const fiber_fine_page_meta pm = A.page_meta[g / kPageSize];
         if (pm.seg_ref_count == 0u) continue;
-        const uint64_t dst = (uint64_t)pm.seg_ref_base + A.offsets[g] + A.visit_rank[r];
+        const uint64_t dst = (uint64_t)pm.seg_ref_base + A.offsets[g] + __ldcs(A.visit_rank + r);
         if (dst >= (uint64_t)pm.seg_ref_base + pm.seg_ref_count) continue;
-        A.ref_keys[dst] = A.visit_task[r];
+        A.ref_keys[dst] = __ldcs(A.visit_task + r);
     }
 }
 
