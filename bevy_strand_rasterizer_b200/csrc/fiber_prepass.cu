@@ -772,9 +772,10 @@ __global__ void __launch_bounds__(kVisitThreads, 4) k_visit(const FrameParams* _
             // passes and the cell sort make the references independent of it.
             const uint32_t at = base + incl - vs.n;
             const uint32_t nb = min(vs.n, kVisitSlots);
+            // Streaming stores: the records are read once, by the count pass.
             for (uint32_t j = 0; j < nb; ++j) {
-                A.visit_rec[at + j] = s_buf[j * kVisitThreads + threadIdx.x];
-                A.visit_task[at + j] = k;
+                __stcs(A.visit_rec + at + j, s_buf[j * kVisitThreads + threadIdx.x]);
+                __stcs(A.visit_task + at + j, k);
             }
             if (vs.n > kVisitSlots) {
                 SpillSink sp{A.visit_rec, A.visit_task, at, k, vs.n, 0u, 0u};
