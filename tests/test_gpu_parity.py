@@ -168,6 +168,44 @@ def test_parity_unsaturated_shading():
     _compare(scene)
 
 
+def _materials():
+    from bevy_strand_rasterizer_b200.plugin import StrandMaterial
+    return {
+        # Narrow lobes: a sharp longitudinal term and a tight azimuthal detector.
+        "narrow": StrandMaterial(absorption_color=(0.2, 0.5, 0.9, 0.6), specular_color=(0.9, 0.8, 0.7, 0.5),
+                                 ambient_factor=0.2, ao_factor=0.3, eta=1.3, beta=0.15, alpha=0.12, shift=-0.05),
+        # Wide lobes, a dense medium and thicker strands.
+        "wide": StrandMaterial(absorption_color=(0.95, 0.1, 0.3, 0.25), specular_color=(0.4, 1.0, 0.6, 1.0),
+                               ambient_factor=0.02, ao_factor=0.05, eta=2.1, beta=1.0, alpha=0.6, shift=0.12,
+                               min_radius_pixels=0.8, max_radius_pixels=3.0),
+    }
+
+
+@pytest.mark.parametrize("name,illuminance", [("narrow", 100.0), ("wide", 400.0)])
+def test_parity_materials(name, illuminance):
+    # Non-default BCSDF parameters and radii, lit so that the shaded texels
+    # spread over (0, 1) with the narrow highlight reaching 1: the shading's
+    # lobes and the rasters' coverage on other inputs.
+    scene = build_scene("tiny", illuminance=illuminance, material=_materials()[name])
+    _compare(scene)
+
+
+def test_parity_two_instances():
+    # A second instance of the same strands, rotated 30 degrees about y, scaled
+    # by 0.8 and moved, with its own material: per-instance transforms,
+    # materials and keep probabilities.
+    scene = build_scene("tiny", illuminance=100.0)
+    packed, _, _ = scene.assets[0]
+    a, s = np.radians(30.0), 0.8
+    m = np.zeros(16, np.float32)  # column-major world_from_local
+    m[0], m[2], m[8], m[10] = s * np.cos(a), -s * np.sin(a), s * np.sin(a), s * np.cos(a)
+    m[5], m[15] = s, 1.0
+    m[12], m[13], m[14] = 0.04, 0.02, -0.03
+    scene.assets.append((packed, _materials()["narrow"], m))
+    s_ = _compare(scene)
+    assert s_.binning_tasks > 0
+
+
 def test_parity_no_cull_two_lights_orbit():
     scene = build_scene("tiny", frame=37, cull=False, lights=[(1.0, 1.0, 1.0), (-1.0, 1.0, 0.5)])
     _compare(scene)
