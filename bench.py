@@ -372,6 +372,15 @@ def fiber_arm(args):
             for name, ms in plugin.span_times().items():
                 spans.setdefault(name, []).append(ms)
     span_med = {k: statistics.median(v) for k, v in spans.items()}
+    # Per-frame device times of the same frames (each synchronised on its own):
+    # median / p95 / p99, as the reference's bench summarises its frames.
+    per_frame = sorted(spans.get("frame/total", []))
+    frame_pct = None
+    if per_frame:
+        def pct(q):
+            return per_frame[min(len(per_frame) - 1, int(round(q * (len(per_frame) - 1))))]
+        frame_pct = {"frames": len(per_frame), "median": statistics.median(per_frame), "p95": pct(0.95),
+                     "p99": pct(0.99)}
 
     # End to end through fiber_render_host: pinned host scene in, composited frame out.
     host_in = torch.empty((H, W, 4), dtype=torch.float16, pin_memory=True)
@@ -443,6 +452,7 @@ def fiber_arm(args):
             "clocks": clk,
             "gpu_launches": KERNELS_PER_FRAME * args.steps,
             "spans_ms": span_med,
+            "frame_ms": frame_pct,
             "counts": {"binning_tasks": st.binning_tasks, "camera_tasks": st.camera_tasks,
                        "pages": st.allocated_pages, "fine_refs": st.fine_refs, "work_items": st.work_items,
                        "camera_runs": st.camera_runs, "shadow_runs": st.shadow_runs},
