@@ -1571,7 +1571,7 @@ void launch_fine(const LaunchCtx& L, const PrepassArgs& A) {
     k_fine<<<L.sm_count * 6, kFineThreads, 0, L.stream>>>(L.P, L.inst, A);
 }
 void launch_visit(const LaunchCtx& L, const PrepassArgs& A) {
-    const unsigned grid = L.sm_count * 8;
+    const unsigned grid = L.sm_count * 4;  // the resident blocks (4 per SM), each looping over warps of tasks
     if (L.telemetry) {
         if (L.opaque) k_visit<true, true><<<grid, kVisitThreads, 0, L.stream>>>(L.P, L.inst, A);
         else k_visit<false, true><<<grid, kVisitThreads, 0, L.stream>>>(L.P, L.inst, A);
@@ -1620,7 +1620,7 @@ void launch_emit(const LaunchCtx& L, const PrepassArgs& A) {
     k_emit<<<L.sm_count * 6, 256, 0, L.stream>>>(L.P, A);
 }
 void launch_sort_cells(const LaunchCtx& L, const PrepassArgs& A) {
-    k_sort_cells<<<L.sm_count * 8, 256, 0, L.stream>>>(L.inst, A);
+    k_sort_cells<<<L.sm_count * 5, 256, 0, L.stream>>>(L.inst, A);  // the resident blocks (5 per SM)
 }
 void launch_telemetry(const LaunchCtx& L, const PrepassArgs& A) {
     k_telemetry<<<L.sm_count * 2, 256, 0, L.stream>>>(L.P, A);
