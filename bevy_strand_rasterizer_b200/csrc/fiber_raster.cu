@@ -321,12 +321,17 @@ __global__ void __launch_bounds__(kShadowThreads, 14) k_shadow(const FrameParams
         float z0 = -1.0f;          // its max covered depth
         bool complete = !active;   // the best item is fully processed
         uint32_t cur_item = 0u, cur_off = 0u;
+        uint32_t rounds1 = 0u, item0 = 0u, off0 = 0u;  // pass 1's staged rounds; thread 0: the state after round 0
         bool single_round = false, staged_all = false;
         for (bool first_round = true;; first_round = false) {
             if (threadIdx.x == 0) {
                 s_more = cur_item < n_items ? 1u : 0u;
                 if (s_more) s_plan = plan_round(s_wcount, n_items, kShadowCap, cur_item, cur_off, s_prefix);
-                if (first_round) s_more |= (cur_item >= n_items ? 2u : 0u);
+                if (first_round) {
+                    s_more |= (cur_item >= n_items ? 2u : 0u);
+                    item0 = cur_item;
+                    off0 = cur_off;
+                }
             }
             __syncthreads();
             const uint32_t more = s_more;
@@ -335,6 +340,7 @@ __global__ void __launch_bounds__(kShadowThreads, 14) k_shadow(const FrameParams
             const RoundPlan rp = s_plan;
             stage(rp);
             __syncthreads();
+            ++rounds1;
             staged_all = single_round;
             if (!complete) {
                 const uint32_t nq = (rp.n + 31u) >> 5;
@@ -367,8 +373,15 @@ __global__ void __launch_bounds__(kShadowThreads, 14) k_shadow(const FrameParams
         if (__syncthreads_or(found)) {
             cur_item = 0u;
             cur_off = 0u;
+            // Pass 1 that stopped after the first round leaves that round
+            // staged: pass 2 starts on it and plans from the state after it.
+            bool reuse = !staged_all && rounds1 == 1u;
+            if (reuse) {
+                cur_item = item0;
+                cur_off = off0;
+            }
             for (;;) {
-                if (!staged_all) {
+                if (!staged_all && !reuse) {
                     if (threadIdx.x == 0) {
                         s_more = cur_item < n_items ? 1u : 0u;
                         if (s_more) s_plan = plan_round(s_wcount, n_items, kShadowCap, cur_item, cur_off, s_prefix);
@@ -378,6 +391,7 @@ __global__ void __launch_bounds__(kShadowThreads, 14) k_shadow(const FrameParams
                     stage(s_plan);
                     __syncthreads();
                 }
+                reuse = false;
                 const RoundPlan rp = s_plan;
                 if (found) {
                     const uint32_t nq = (rp.n + 31u) >> 5;
