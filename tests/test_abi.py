@@ -58,3 +58,22 @@ def test_status_strings_and_bad_arguments():
     assert lib.fiber_ctx_destroy(None) == abi.EINVAL
     assert lib.fiber_span_count() == 14
     assert lib.fiber_span_name(1) == b"strand_prepass/fine"
+
+
+def test_exact_op_flags_per_source():
+    # The integer-deciding stages need one correctly rounded binary32 op per
+    # source operation; only the shading file (compared within a tolerance)
+    # is compiled with contraction and approximate division and square root.
+    import importlib.util
+    spec = importlib.util.spec_from_file_location(
+        "fiber_build", Path(abi.__file__).resolve().parent / "build.py")
+    b = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(b)
+    exact = {"--fmad=false", "-prec-div=true", "-prec-sqrt=true"}
+    fast = {"--fmad=true", "-prec-div=false", "-prec-sqrt=false"}
+    assert b.FAST_FP_SOURCES == {"fiber_render.cu"}
+    for src in b.SOURCES:
+        flags = set(b.flags_for(src))
+        want, other = (fast, exact) if src in b.FAST_FP_SOURCES else (exact, fast)
+        assert want <= flags and not (other & flags), (src, sorted(flags))
+        assert "arch=compute_100a,code=sm_100a" in b.flags_for(src)
