@@ -968,43 +968,102 @@ __device__ __forceinline__ void page_active_tiles(const FrameParams& P, const Pr
 }
 
 // csr: a page-CSR frame, where k_build_pages does this work unless the visit
-// records went unused.
+// records went unused. One warp per page, claimed in page order: lane l holds
+// cells 8 l .. 8 l + 7 (one fine depth slice, fine tiles 8 (l & 1) .. + 7), so
+// a warp scan gives the cell offsets and the look-back the page base, with no
+// block barrier.
 __global__ void __launch_bounds__(256) k_prefix_pages(const FrameParams* __restrict__ Pp, PrepassArgs A, bool csr) {
     if (csr && !visits_unused(A)) return;
     const FrameParams& P = *Pp;
-    __shared__ uint32_t s_tile, s_base, s_pbase, s_small, s_large;
-    __shared__ uint32_t s_warp[33];
-    __shared__ uint32_t s_counts[kPageSize];
+    const uint32_t lane = threadIdx.x & 31u;
     const uint32_t pages = *((volatile uint32_t*)&A.counters->pages);
     for (;;) {
-        if (threadIdx.x == 0) s_tile = atomicAdd(A.tile_counter, 1u);
-        __syncthreads();
-        const uint32_t page = s_tile;
+        uint32_t page = 0u;
+        if (lane == 0u) page = atomicAdd(A.tile_counter, 1u);
+        page = __shfl_sync(0xFFFFFFFFu, page, 0);
         if (page >= pages) break;
-        const size_t g = (size_t)page * kPageSize + threadIdx.x;
-        uint32_t c = A.counts[g];
-        s_counts[threadIdx.x] = c;
-        const uint32_t excl = page_prefix(P, A, page, pages, c, s_warp, s_base, s_pbase);
-        // List the page's non-empty cells for k_sort_cells (a page that lost its
-        // references lists none): up to 8 references in the small list, more in
-        // the large one. One scan carries both flags (small low, large high).
-        if (s_base == 0u) {
-            const uint32_t small = (c >= 1u && c <= kThreadSortMax) ? 1u : 0u;
-            const uint32_t large = c > kThreadSortMax ? 1u : 0u;
-            uint32_t both;
-            const uint32_t x = block_exclusive_scan<256>(small | (large << 16), s_warp, both);
-            if (threadIdx.x == 0) {
-                const uint32_t ns = both & 0xFFFFu, nl = both >> 16;
-                s_small = ns ? atomicAdd(&A.counters->small_cells, ns) : 0u;
-                s_large = nl ? atomicAdd(&A.counters->large_cells, nl) : 0u;
-            }
-            __syncthreads();
-            const uint32_t cb = s_pbase + excl;
-            if (small) A.cells_small[s_small + (x & 0xFFFFu)] = make_uint2(cb, c);
-            if (large) A.cells_large[s_large + (x >> 16)] = make_uint2(cb, c);
-            page_active_tiles(P, A, page, s_counts);
+        const size_t g0 = (size_t)page * kPageSize + lane * 8u;
+        const uint4 ca = *reinterpret_cast<const uint4*>(A.counts + g0);
+        const uint4 cb = *reinterpret_cast<const uint4*>(A.counts + g0 + 4u);
+        const uint32_t c[8] = {ca.x, ca.y, ca.z, ca.w, cb.x, cb.y, cb.z, cb.w};
+        uint32_t e[8], sum = 0u, nsmall = 0u, nlarge = 0u, nz = 0u;
+#pragma unroll
+        for (uint32_t k = 0; k < 8u; ++k) {
+            e[k] = sum;
+            sum += c[k];
+            nsmall += (c[k] >= 1u && c[k] <= kThreadSortMax) ? 1u : 0u;
+            nlarge += c[k] > kThreadSortMax ? 1u : 0u;
+            nz |= (c[k] > 0u ? 1u : 0u) << k;
         }
-        __syncthreads();
+        // One scan carries the reference count (exclusive per cell) and, packed,
+        // the small / large cell counts for the lists.
+        uint32_t x = sum, y = nsmall | (nlarge << 16);
+#pragma unroll
+        for (uint32_t o = 1; o < 32u; o <<= 1) {
+            const uint32_t xa = __shfl_up_sync(0xFFFFFFFFu, x, o), ya = __shfl_up_sync(0xFFFFFFFFu, y, o);
+            if (lane >= o) { x += xa; y += ya; }
+        }
+        const uint32_t total = __shfl_sync(0xFFFFFFFFu, x, 31), both = __shfl_sync(0xFFFFFFFFu, y, 31);
+        const uint32_t lane_base = x - sum, list_base = y - (nsmall | (nlarge << 16));
+#pragma unroll
+        for (uint32_t k = 0; k < 8u; ++k) e[k] += lane_base;
+        *reinterpret_cast<uint4*>(A.offsets + g0) = make_uint4(e[0], e[1], e[2], e[3]);
+        *reinterpret_cast<uint4*>(A.offsets + g0 + 4u) = make_uint4(e[4], e[5], e[6], e[7]);
+        *reinterpret_cast<uint4*>(A.cursors + g0) = make_uint4(0u, 0u, 0u, 0u);
+        *reinterpret_cast<uint4*>(A.cursors + g0 + 4u) = make_uint4(0u, 0u, 0u, 0u);
+        const uint32_t base = lb_exclusive_warp(A.lb_status, page, P.epoch, total, &A.counters->error);
+        uint32_t flags = 0u, tile = 0u;
+        if (lane == 0u) {
+            fiber_fine_page_meta pm = A.page_meta[page];
+            if (total > 0u && (uint64_t)base + total > (uint64_t)P.ref_capacity) {
+                flags = 1u;
+                atomicOr(&A.counters->overflow, 4u);
+            }
+            pm.seg_ref_base = total > 0u ? base : 0u;
+            pm.seg_ref_count = flags ? 0u : total;
+            pm.flags = flags;
+            A.page_meta[page] = pm;
+            tile = pm.coarse_tile_id;
+            if (page == pages - 1u) A.counters->refs = base + total;
+        }
+        flags = __shfl_sync(0xFFFFFFFFu, flags, 0);
+        // A page that lost its references lists no cells and no active tiles.
+        if (flags != 0u) continue;
+        // The page's non-empty cells for k_sort_cells: up to 8 references in the
+        // small list, more in the large one, in cell order.
+        uint32_t s_small = 0u, s_large = 0u;
+        if (lane == 0u) {
+            const uint32_t ns = both & 0xFFFFu, nl = both >> 16;
+            s_small = ns ? atomicAdd(&A.counters->small_cells, ns) : 0u;
+            s_large = nl ? atomicAdd(&A.counters->large_cells, nl) : 0u;
+        }
+        uint32_t ks = __shfl_sync(0xFFFFFFFFu, s_small, 0) + (list_base & 0xFFFFu);
+        uint32_t kl = __shfl_sync(0xFFFFFFFFu, s_large, 0) + (list_base >> 16);
+#pragma unroll
+        for (uint32_t k = 0; k < 8u; ++k) {
+            if (c[k] >= 1u && c[k] <= kThreadSortMax) A.cells_small[ks++] = make_uint2(base + e[k], c[k]);
+            else if (c[k] > kThreadSortMax) A.cells_large[kl++] = make_uint2(base + e[k], c[k]);
+        }
+        // append_active_fine_tile (:2207-2238): each of the page's 16 fine tiles
+        // with a non-empty cell that lies on screen. Lanes of one parity hold
+        // the same 8 fine tiles at the 16 depth slices.
+        uint32_t m = nz;
+#pragma unroll
+        for (uint32_t o = 2; o < 32u; o <<= 1) m |= __shfl_xor_sync(0xFFFFFFFFu, m, o);
+        tile = __shfl_sync(0xFFFFFFFFu, tile, 0);
+        const uint32_t lt = lane;
+        const uint32_t has = __shfl_sync(0xFFFFFFFFu, m, (int)(lane >> 3) & 1);
+        if (lt < 16u && ((has >> (lt & 7u)) & 1u)) {
+            const uint32_t f = frustum_for_tile(P, tile);
+            if (f != kInvalid) {
+                const fiber_frustum_desc& d = P.frusta[f];
+                const uint32_t lc = tile - d.coarse_depth_tile_base;
+                const uint32_t fx = (lc % d.coarse_tiles_x) * kCoarseExtent + lt % kCoarseExtent;
+                const uint32_t fy = (lc / d.coarse_tiles_x) * kCoarseExtent + lt / kCoarseExtent;
+                if (fx < ceil_div(d.screen_width, d.froxel_size_x) && fy < ceil_div(d.screen_height, d.froxel_size_y))
+                    A.active_flags[(size_t)tile * 16u + lt] = 1u;
+            }
+        }
     }
 }
 
