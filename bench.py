@@ -229,6 +229,17 @@ def load_traffic() -> dict:
     return {}
 
 
+def bench_config(w, segs: int, n_lights: int, args, world: int) -> dict:
+    """The workload both arms run (the same text, so the lines compare)."""
+    return {"workload": f"{w.name}: {w.strands} strands x {w.points} points ({segs} segments), {w.width}x{w.height} "
+                        f"camera orbiting over {w.orbit_frames} frames, {n_lights} light(s) with {w.dom_size}^2 x "
+                        f"{w.dom_layers} deep-opacity maps",
+            "tile_px": w.froxel, "parallelism": f"replicas x{world}",
+            "l2": "per-frame working set (tasks, refs, pages, DOM) > 126 MB L2",
+            "stochastic_cull": "on (reference default)", "ref_capacity_factor": w.ref_capacity_factor,
+            "fine_binning_backend": args.binning_backend, "dom_page_pool": args.dom_page_pool}
+
+
 # ---------------------------------------------------------------------------
 # CPU arm (oracle restatement on the host cores)
 # ---------------------------------------------------------------------------
@@ -249,6 +260,7 @@ def cpu_frame_time(w, packed, material, cam_cfg, lights, frame=0, max_strands=No
     cam, lc = frame_structs(w, packed, frame, lights)
     st = abi.default_settings()
     st.dom_slices = w.dom_layers
+    st.ref_capacity_factor = w.ref_capacity_factor
     segs = int(np.maximum(sample.meta["count"].astype(np.int64) - 1, 0).sum())
     t0 = time.perf_counter()
     fr = run_oracle([(sample, material, np.eye(4, dtype=np.float32).reshape(16))], cam_cfg, cam,
@@ -263,14 +275,13 @@ def reference_arm(args):
     if rank != 0:
         return
     w, packed, material, cam_cfg, lights = make_scene(args.workload)
-    # A bounded sample keeps each step to a few seconds of host work.
-    max_strands = 25_000 if w.strands > 25_000 else None
+    # Each step is one whole frame of the workload (the same strands, camera
+    # orbit and light as the GPU arm), a few seconds of host work.
     for i in range(args.warmup):
-        cpu_frame_time(w, packed, material, cam_cfg, lights, frame=i, max_strands=max_strands)
+        cpu_frame_time(w, packed, material, cam_cfg, lights, frame=i)
     times, segs, note = [], 0, ""
     for k in range(args.steps):
-        dt, segs, note = cpu_frame_time(w, packed, material, cam_cfg, lights, frame=args.warmup + k,
-                                        max_strands=max_strands)
+        dt, segs, note = cpu_frame_time(w, packed, material, cam_cfg, lights, frame=args.warmup + k)
         times.append(dt)
     total = sum(times)
     value = segs * args.steps / total
@@ -279,8 +290,7 @@ def reference_arm(args):
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * total / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"{w.name}: {w.strands} strands x {w.points} points, {w.width}x{w.height}, "
-                               f"DOM {w.dom_size}^2 x {w.dom_layers}", "sample": note},
+        "config": dict(bench_config(w, segs, len(lights), args, args.gpus), sample=note),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": note},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "note": "the reference is Rust + WGSL over wgpu/Vulkan with no CPU implementation; its CPU arm is the "
@@ -410,6 +420,19 @@ def fiber_arm(args):
     e2e_value = replicas.job_rate(segs * args.steps, world, e2e_ms / 1000.0)
     assert np.isfinite(host_out.float().numpy()).all()
 
+    # PrepassTelemetrySettings counters over a few more orbit frames (telemetry
+    # adds atomics to the prepass, so it is switched on only after the timing).
+    tel_samples = {}
+    if not args.profile:
+        plugin.settings.telemetry_enabled = 1
+        abi.check(plugin.lib.fiber_settings_set(plugin.ctx, C.byref(plugin.settings)), "fiber_settings_set")
+        with torch.cuda.stream(stream):
+            for k in range(min(args.steps, 10)):
+                step(k)
+                stream.synchronize()
+                for name, v in telemetry_words(plugin.telemetry()).items():
+                    tel_samples.setdefault(name, []).append(float(v))
+
     # Roofline of the dominant kernel (HBM-bound dataflow; no dense contraction).
     ab = algorithmic_bytes(st, w, len(lights), w.dom_layers, w.dom_size)
     kernel_ms = {SPAN_TO_KERNEL[k]: v for k, v in span_med.items() if k in SPAN_TO_KERNEL}
@@ -424,22 +447,19 @@ def fiber_arm(args):
     if rank == 0:
         cpu = None
         if not args.no_cpu_baseline and world == 1:
-            max_strands = 25_000 if w.strands > 25_000 else None
-            dt, csegs, note = cpu_frame_time(w, packed, material, cam_cfg, lights, frame=0, max_strands=max_strands)
-            cpu = {"value": csegs / dt, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "port",
-                   "sample": note}
+            cpu_frame_time(w, packed, material, cam_cfg, lights, frame=0)
+            dts = []
+            for k in range(2):
+                dt, csegs, note = cpu_frame_time(w, packed, material, cam_cfg, lights, frame=1 + k)
+                dts.append(dt)
+            cpu = {"value": csegs * len(dts) / sum(dts), "unit": UNIT, "cores": os.cpu_count() or 1,
+                   "kind": "port", "sample": f"{note}: two orbit frames after one warm-up frame"}
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "frames_per_s": 1000.0 * world / ms_per_step,
-            "config": {"workload": f"{w.name}: {w.strands} strands x {w.points} points ({segs} segments), "
-                                   f"{w.width}x{w.height} camera orbiting over {w.orbit_frames} frames, "
-                                   f"{len(lights)} light(s) with {w.dom_size}^2 x {w.dom_layers} deep-opacity maps",
-                       "tile_px": w.froxel, "parallelism": f"replicas x{world}",
-                       "l2": "per-frame working set (tasks, refs, pages, DOM) > 126 MB L2",
-                       "stochastic_cull": "on (reference default)", "ref_capacity_factor": w.ref_capacity_factor,
-                       "fine_binning_backend": args.binning_backend, "dom_page_pool": args.dom_page_pool},
+            "config": bench_config(w, segs, len(lights), args, world),
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "entry_point": "fiber_render_host", "ms_per_step": e2e_ms / args.steps},
             "roofline": {"bound": "hbm", "kernel": dom_kernel, "achieved": achieved, "peak": peak,
@@ -453,6 +473,7 @@ def fiber_arm(args):
             "gpu_launches": KERNELS_PER_FRAME * args.steps,
             "spans_ms": span_med,
             "frame_ms": frame_pct,
+            "report": bench_report(args, w, packed, spans, tel_samples),
             "counts": {"binning_tasks": st.binning_tasks, "camera_tasks": st.camera_tasks,
                        "pages": st.allocated_pages, "fine_refs": st.fine_refs, "work_items": st.work_items,
                        "camera_runs": st.camera_runs, "shadow_runs": st.shadow_runs},
@@ -467,6 +488,53 @@ def fiber_arm(args):
         dist.destroy_process_group()
     if line is not None:
         print(json.dumps(line), flush=True)
+
+
+def summarize(values) -> dict:
+    """min / mean / median / p90 / p95 / p99 / max of samples, nearest-rank on
+    (n - 1) * q as the reference's strand_bench summarises them
+    (examples/strand_bench.rs:931-947)."""
+    v = sorted(values)
+    def pct(q):
+        return v[int(round((len(v) - 1) * q))]
+    return {"samples": len(v), "min": v[0], "mean": sum(v) / len(v), "median": pct(0.5), "p90": pct(0.9),
+            "p95": pct(0.95), "p99": pct(0.99), "max": v[-1]}
+
+
+def telemetry_words(t) -> dict:
+    """The telemetry image as the reference names its diagnostics
+    (src/pipelines/prepass.rs:1345-1396)."""
+    out = {}
+    for name in ("allocated_pages", "binning_tasks", "page_candidates", "fine_cell_hits", "active_candidate_pages",
+                 "max_candidates_per_page"):
+        out[name] = getattr(t, name)
+    for b in range(len(t.candidate_histogram)):
+        out[f"candidate_histogram/{b}"] = t.candidate_histogram[b]
+    for f in range(min(t.frustum_count, len(t.frustum))):
+        for name, _ in t.frustum[f]._fields_:
+            out[f"frustum/{f}/{name}"] = getattr(t.frustum[f], name)
+    return out
+
+
+def bench_report(args, w, packed, spans: dict, tel_samples: dict) -> dict:
+    """The reference benchmark's report (examples/strand_bench.rs:859-913):
+    schema version, case, shape, per-span GPU time summaries and the prepass
+    telemetry summaries."""
+    import torch
+    props = torch.cuda.get_device_properties(torch.cuda.current_device())
+    return {
+        "schema_version": 1, "case": w.name, "mode": "headless",
+        "resolution": {"width": w.width, "height": w.height},
+        "warmup_frames": args.warmup, "sample_frames": len(spans.get("frame/total", [])),
+        "telemetry_enabled": bool(tel_samples),
+        "fine_binning_backend": args.binning_backend, "seed": w.seed,
+        "workload": {"geometry_count": 1, "strand_count": int(packed.strand_count),
+                     "vertex_count": int(packed.vertices.shape[0]), "points_per_strand": w.points,
+                     "asset": "synthetic scalp hair"},
+        "adapter": {"name": props.name, "backend": "cuda", "driver": torch.version.cuda},
+        "timings_ms": {f"render/{k}/elapsed_gpu": summarize(v) for k, v in sorted(spans.items()) if v},
+        "telemetry": {k: summarize(v) for k, v in sorted(tel_samples.items())},
+    }
 
 
 SERVED_BUDGET = 150 * 10**9  # bytes of HBM the served configuration may hold

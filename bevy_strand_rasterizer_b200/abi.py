@@ -30,6 +30,7 @@ STATUS_NAMES = {OK: "ok", EINVAL: "EINVAL", ENOMEM: "ENOMEM", EOVERFLOW: "EOVERF
 
 SLAB_VERT, SLAB_INDEX, SLAB_MATERIAL, SLAB_GEO, SLAB_META = 0, 1, 5, 6, 7
 FMT_RGBA16F, FMT_R32F, FMT_RGBA32F = 0, 1, 2
+MAX_FRUSTA = 16  # FIBER_MAX_FRUSTA: the camera plus up to 15 lights
 
 (DUMP_FRUSTA, DUMP_RANGES, DUMP_KEEP, DUMP_LUT, DUMP_TASKS, DUMP_PROJECTED, DUMP_PAGE_TABLE,
  DUMP_PAGE_META, DUMP_COUNTS, DUMP_OFFSETS, DUMP_REFS, DUMP_ACTIVE_TILES, DUMP_WORK, DUMP_RUNS,
@@ -93,10 +94,11 @@ class Stats(C.Structure):
     _fields_ = [("frustum_count", u32), ("instance_count", u32), ("binning_tasks", u32),
                 ("camera_tasks", u32), ("allocated_pages", u32), ("fine_refs", u32),
                 ("active_tiles", u32), ("camera_runs", u32), ("shadow_runs", u32), ("work_items", u32),
-                ("overflow_flags", u32), ("timeout_flags", u32), ("frustum_tasks", u32 * 8),
-                ("frustum_pages", u32 * 8), ("frustum_refs", u32 * 8), ("frustum_work", u32 * 8),
-                ("frustum_runs", u32 * 8), ("total_segments", C.c_uint64), ("total_points", C.c_uint64),
-                ("total_strands", C.c_uint64)]
+                ("overflow_flags", u32), ("timeout_flags", u32), ("frustum_tasks", u32 * MAX_FRUSTA),
+                ("frustum_pages", u32 * MAX_FRUSTA), ("frustum_refs", u32 * MAX_FRUSTA),
+                ("frustum_work", u32 * MAX_FRUSTA), ("frustum_runs", u32 * MAX_FRUSTA),
+                ("total_segments", C.c_uint64), ("total_points", C.c_uint64), ("total_strands", C.c_uint64),
+                ("fine_refs_total", C.c_uint64), ("refs_requested", C.c_uint64)]
 
     def as_dict(self) -> dict:
         out = {}
@@ -129,7 +131,7 @@ class ServerRequest(C.Structure):
 
 class ServerResult(C.Structure):
     _fields_ = [("status", C.c_int), ("slot", u32), ("arrival_ns", C.c_uint64), ("admit_ns", C.c_uint64),
-                ("done_ns", C.c_uint64)]
+                ("done_ns", C.c_uint64), ("renders", u32), ("pad", u32)]
 
 
 # numpy views of the task-contract structs (src/pipelines/task_contract.rs:45-135)
@@ -190,7 +192,7 @@ EXPORTS = [
     "fiber_server_start", "fiber_server_submit", "fiber_server_wait", "fiber_server_destroy", "fiber_server_now_ns",
     "fiber_batch_create", "fiber_batch_set_tuning", "fiber_batch_get_tuning", "fiber_batch_launch",
     "fiber_batch_tune", "fiber_batch_destroy", "fiber_batch_plan",
-    "fiber_prefix_pages_noalloc",
+    "fiber_prefix_pages_noalloc", "fiber_debug_stall_lookback",
 ]
 
 _LIB = None
@@ -231,6 +233,7 @@ def load_library(path: Path | str | None = None) -> C.CDLL:
         "fiber_frame_fused": (C.c_int, [vp, pp(Image), pp(Image), pp(Image), vp]),
         "fiber_render_host": (C.c_int, [vp, vp, vp, vp, vp]),
         "fiber_stats_get": (C.c_int, [vp, pp(Stats)]),
+        "fiber_debug_stall_lookback": (C.c_int, [vp, u32, u32, u32]),
         "fiber_telemetry_get": (C.c_int, [vp, pp(Telemetry)]),
         "fiber_dump": (C.c_int, [vp, u32, vp, C.c_uint64, pp(C.c_uint64)]),
         "fiber_output_image": (C.c_int, [vp, u32, pp(Image)]),

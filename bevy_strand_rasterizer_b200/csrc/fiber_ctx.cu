@@ -128,6 +128,11 @@ struct fiber_ctx {
     // A batch graph advanced this context's epoch on the device: the next
     // fiber_frame_begin clears the look-back words and restarts the epoch.
     bool epoch_dirty = false;
+    // fiber_debug_stall_lookback: the next frame's look-back test hook.
+    uint32_t stall_stage = 0, stall_tile = 0, stall_limit = 0;
+    // Smallest reference capacity of the next frames (the request server
+    // raises it after a frame whose references overflowed).
+    uint64_t ref_floor = 0;
     DevBuf d_dom_depth, d_dom_opacity, d_shadow_map, d_atlas, d_history[2];
     DevBuf d_color, d_depth, d_fragments, d_validate, d_host_scene, d_host_depth;
     int hist_cur = 0;
@@ -735,6 +740,10 @@ fiber_status fiber_frame_begin(fiber_ctx* c, const fiber_froxel_config* cam_cfg,
     const fiber_settings& st = c->settings;
     FrameParams& P = c->P;
     std::memset(&P, 0, sizeof(P));
+    P.lb_spin_limit = c->stall_limit;
+    P.lb_stall_stage = c->stall_stage;
+    P.lb_stall_tile = c->stall_tile;
+    c->stall_stage = c->stall_tile = c->stall_limit = 0;
     // Frustum table (src/plugin.rs:386-482): camera first, then lights.
     c->frusta.clear();
     uint32_t bucket = 0, coarse = 0, fine = 0, cam_tiles = 0;
@@ -807,7 +816,9 @@ fiber_status fiber_frame_begin(fiber_ctx* c, const fiber_froxel_config* cam_cfg,
     const uint64_t base_binning = std::max<uint64_t>(next_pow2(c->total_segments), prepass_cap);
     const uint64_t task_cap = std::max<uint64_t>(next_pow2(base_binning * P.F), base_binning);
     const uint64_t page_cap = std::max<uint64_t>(1, table / st.page_capacity_divisor);
-    const uint64_t ref_cap = std::max<uint64_t>(next_pow2(task_cap * st.ref_capacity_factor), std::max<uint64_t>(task_cap, 1024));
+    const uint64_t ref_cap = std::max<uint64_t>(
+        std::max<uint64_t>(next_pow2(task_cap * st.ref_capacity_factor), std::max<uint64_t>(task_cap, 1024)),
+        next_pow2(c->ref_floor));
     const uint64_t fine_tiles = table;  // coarse tiles x 16 fine tiles
     const uint64_t work_cap = std::max<uint64_t>(1, std::min<uint64_t>(ref_cap, 256ull * fine_tiles));
     if (ref_cap >= 0xFFFFFFFFull || work_cap >= 0xFFFFFFFFull) return FIBER_ENOMEM;
@@ -1132,7 +1143,8 @@ fiber_scene_state* fiber_ctx_save_scene(const fiber_ctx* c) {
     return s;
 }
 
-void fiber_ctx_load_scene(fiber_ctx* c, const fiber_scene_state* s) {
+fiber_status fiber_ctx_load_scene(fiber_ctx* c, const fiber_scene_state* s) {
+    if (!c || !s) return FIBER_EINVAL;
     c->rows = s->rows;
     c->views = s->views;
     c->inst_segments = s->inst_segments;
@@ -1143,6 +1155,7 @@ void fiber_ctx_load_scene(fiber_ctx* c, const fiber_scene_state* s) {
     c->total_strand_count = s->total_strand_count;
     c->max_strand_count = s->max_strand_count;
     c->frame_ready = false;
+    return FIBER_OK;
 }
 
 void fiber_scene_state_free(fiber_scene_state* s) { delete s; }
@@ -1150,6 +1163,22 @@ void fiber_scene_state_free(fiber_scene_state* s) { delete s; }
 uint64_t fiber_scene_segments(const fiber_scene_state* s) { return s ? s->total_segments : 0u; }
 
 uint64_t fiber_ctx_allocated(const fiber_ctx* c) { return c ? c->allocated : 0u; }
+
+bool fiber_ctx_grow_refs(fiber_ctx* c, cudaStream_t s) {
+    if (!c) return false;
+    uint32_t overflow = 0u, refs = 0u;
+    if (cudaMemcpyAsync(&overflow, reinterpret_cast<const char*>(c->d_counters.p) + offsetof(FrameCounters, overflow),
+                        4, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaMemcpyAsync(&refs, reinterpret_cast<const char*>(c->d_counters.p) + offsetof(FrameCounters, refs), 4,
+                        cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    if (!(overflow & 4u) || refs <= c->P.ref_capacity) return false;
+    c->ref_floor = std::max<uint64_t>(c->ref_floor, refs);
+    return true;
+}
 
 fiber_status fiber_ctx_frame_status(fiber_ctx* c, cudaStream_t s) {
     if (!c) return FIBER_EINVAL;
@@ -1224,6 +1253,14 @@ fiber_status fiber_ctx_render_host_nodes(fiber_ctx* c, const void* scene_host, v
 
 extern "C" {
 
+fiber_status fiber_debug_stall_lookback(fiber_ctx* c, uint32_t stage, uint32_t tile, uint32_t spin_limit) {
+    if (!c || stage >= kStageCount) return FIBER_EINVAL;
+    c->stall_stage = stage + 1u;
+    c->stall_tile = tile;
+    c->stall_limit = spin_limit;
+    return FIBER_OK;
+}
+
 fiber_status fiber_stats_get(fiber_ctx* c, fiber_stats* out) {
     if (!c || !out) return FIBER_EINVAL;
     cudaSetDevice(c->device);
@@ -1247,24 +1284,27 @@ fiber_status fiber_stats_get(fiber_ctx* c, fiber_stats* out) {
             if (m.coarse_tile_id >= c->P.frusta[f].coarse_depth_tile_base &&
                 m.coarse_tile_id < c->P.frusta[f].coarse_depth_tile_base + c->P.frusta[f].coarse_depth_tile_count)
                 break;
-        if (f < 8) {
+        if (f < FIBER_MAX_FRUSTA) {
             out->frustum_pages[f]++;
             out->frustum_refs[f] += m.seg_ref_count;
         }
     }
-    out->fine_refs = (uint32_t)refs;
+    out->fine_refs = (uint32_t)std::min<uint64_t>(refs, 0xFFFFFFFFull);
+    out->fine_refs_total = refs;
+    out->refs_requested = h.refs;
     out->active_tiles = h.active_tiles;
     out->camera_runs = h.camera_active;
     out->shadow_runs = h.active_tiles - h.camera_active;
     out->work_items = h.work_items;
     out->overflow_flags = h.overflow;
     out->timeout_flags = h.error;
-    for (uint32_t f = 0; f < c->P.F && f < 8; ++f) out->frustum_tasks[f] = h.frustum_task_base[f + 1] - h.frustum_task_base[f];
+    for (uint32_t f = 0; f < c->P.F && f < FIBER_MAX_FRUSTA; ++f)
+        out->frustum_tasks[f] = h.frustum_task_base[f + 1] - h.frustum_task_base[f];
     std::vector<fiber_raster_tile_run> runs(h.active_tiles);
     if (h.active_tiles)
         FIBER_CUDA(cudaMemcpy(runs.data(), c->d_runs.p, h.active_tiles * sizeof(fiber_raster_tile_run), cudaMemcpyDeviceToHost));
     for (const auto& r : runs)
-        if (r.frustum_id < 8) {
+        if (r.frustum_id < FIBER_MAX_FRUSTA) {
             out->frustum_work[r.frustum_id] += r.work_count;
             out->frustum_runs[r.frustum_id]++;
         }

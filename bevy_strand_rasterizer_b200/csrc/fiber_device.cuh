@@ -72,6 +72,9 @@ struct FrameParams {
     uint32_t visit_records;       // page-table slots fit 24 bits: count/fill stream visit records
     uint32_t dom_pool_pages;      // 0: dense DOM layers; else the sparse DOM's pool size in pages
     uint32_t dom_pages_x;         // DOM pages per side (ceil(D / 256))
+    uint32_t lb_spin_limit;       // polls before a look-back wait gives up
+    uint32_t lb_stall_stage;      // 1 + look-back stage with a tile that never publishes (0: none)
+    uint32_t lb_stall_tile;       // that tile (fiber_debug_stall_lookback; one frame only)
 };
 
 // Device counters of one frame (zeroed at frame start).
@@ -279,7 +282,8 @@ __device__ __forceinline__ void lb_publish(unsigned long long* status, uint32_t 
 
 // Called by one thread. Returns the exclusive prefix of `tile`.
 __device__ __forceinline__ uint32_t lb_exclusive(unsigned long long* status, uint32_t tile, uint32_t epoch,
-                                                 uint32_t aggregate, uint32_t* error) {
+                                                 uint32_t aggregate, uint32_t* error,
+                                                 uint32_t spin_limit = kSpinLimit) {
     if (tile == 0) {
         lb_publish(status, 0, epoch, 2u, aggregate);
         return 0u;
@@ -296,7 +300,7 @@ __device__ __forceinline__ uint32_t lb_exclusive(unsigned long long* status, uin
         if (flag == 0u) {
             // Give up after kSpinLimit polls, or at once when another block of
             // this frame already gave up, so a broken chain costs one limit.
-            if (++spins > kSpinLimit || ((spins & 255u) == 0u && *((volatile uint32_t*)error) != 0u)) {
+            if (++spins > spin_limit || ((spins & 255u) == 0u && *((volatile uint32_t*)error) != 0u)) {
                 atomicOr(error, kErrTimeout);
                 break;
             }
@@ -316,15 +320,20 @@ __device__ __forceinline__ uint32_t lb_exclusive(unsigned long long* status, uin
 // reads a window of 32 predecessors at once (lane i reads tile - 1 - i) and
 // adds the values up to the nearest inclusive one, so a block walks back
 // through 32 published aggregates per L2 round trip. Waiting is bounded as in
-// lb_exclusive.
+// lb_exclusive, after `spin_limit` polls. A tile equal to `withheld` publishes
+// nothing: the frame-level test hook that makes its successors' waits run out
+// (fiber_debug_stall_lookback).
 __device__ __forceinline__ uint32_t lb_exclusive_warp(unsigned long long* status, uint32_t tile, uint32_t epoch,
-                                                      uint32_t aggregate, uint32_t* error) {
+                                                      uint32_t aggregate, uint32_t* error,
+                                                      uint32_t spin_limit = kSpinLimit,
+                                                      uint32_t withheld = kInvalid) {
     const uint32_t lane = threadIdx.x & 31u;
+    const bool publish = tile != withheld;
     if (tile == 0) {
-        if (lane == 0) lb_publish(status, 0, epoch, 2u, aggregate);
+        if (lane == 0 && publish) lb_publish(status, 0, epoch, 2u, aggregate);
         return 0u;
     }
-    if (lane == 0) lb_publish(status, tile, epoch, 1u, aggregate);
+    if (lane == 0 && publish) lb_publish(status, tile, epoch, 1u, aggregate);
     uint32_t excl = 0;
     int64_t end = (int64_t)tile;  // window: predecessors end - 1 - lane
     uint32_t spins = 0;
@@ -343,7 +352,7 @@ __device__ __forceinline__ uint32_t lb_exclusive_warp(unsigned long long* status
         const uint32_t first = incl ? (uint32_t)(__ffs(incl) - 1) : 32u;
         const unsigned needed = first >= 31u ? 0xFFFFFFFFu : ((2u << first) - 1u);
         if (waiting & needed) {
-            bool give_up = ++spins > kSpinLimit;
+            bool give_up = ++spins > spin_limit;
             if ((spins & 255u) == 0u) {
                 const uint32_t err = lane == 0 ? *((volatile uint32_t*)error) : 0u;
                 give_up = give_up || __shfl_sync(0xFFFFFFFFu, err, 0) != 0u;
@@ -362,8 +371,25 @@ __device__ __forceinline__ uint32_t lb_exclusive_warp(unsigned long long* status
         if (first < 32u) break;
         end -= 32;
     }
-    if (lane == 0) lb_publish(status, tile, epoch, 2u, excl + aggregate);
+    if (lane == 0 && publish) lb_publish(status, tile, epoch, 2u, excl + aggregate);
     return excl;
+}
+
+// The look-back wait settings of one stage of this frame.
+__device__ __forceinline__ uint32_t lb_limit(const FrameParams& P) {
+    return P.lb_spin_limit ? P.lb_spin_limit : kSpinLimit;
+}
+__device__ __forceinline__ uint32_t lb_withheld(const FrameParams& P, uint32_t stage) {
+    return P.lb_stall_stage == stage + 1u ? P.lb_stall_tile : kInvalid;
+}
+
+// After a look-back wait gave up, the bases it produced are partial sums (no
+// larger than the true ones, so every write stays in bounds) and the arrays
+// they index may hold records of earlier frames. Every kernel that consumes
+// them starts with this check and does nothing in such a frame, which then
+// reports FIBER_ETIMEDOUT.
+__device__ __forceinline__ bool frame_failed(const FrameCounters* c) {
+    return *((const volatile uint32_t*)&c->error) != 0u;
 }
 
 // Block-wide exclusive scan of one value per thread (blockDim multiple of 32).

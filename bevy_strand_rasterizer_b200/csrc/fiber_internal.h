@@ -15,7 +15,7 @@
 struct fiber_scene_state;
 
 fiber_scene_state* fiber_ctx_save_scene(const fiber_ctx* c);
-void fiber_ctx_load_scene(fiber_ctx* c, const fiber_scene_state* s);
+fiber_status fiber_ctx_load_scene(fiber_ctx* c, const fiber_scene_state* s);
 void fiber_scene_state_free(fiber_scene_state* s);
 uint64_t fiber_scene_segments(const fiber_scene_state* s);
 
@@ -25,6 +25,11 @@ fiber_status fiber_ctx_render_host_nodes(fiber_ctx* c, const void* scene_host, v
 
 // Device bytes the context holds.
 uint64_t fiber_ctx_allocated(const fiber_ctx* c);
+
+// After a frame on `s` whose references overflowed: raises the context's
+// reference capacity to what the frame's cells asked for, for the next
+// fiber_frame_begin; returns true when it did (re-render the frame).
+bool fiber_ctx_grow_refs(fiber_ctx* c, cudaStream_t s);
 
 // After the frame on `s` completed: ETIMEDOUT if a bounded device wait gave
 // up, EOVERFLOW if a queue dropped work, else OK. Reads two counter words.

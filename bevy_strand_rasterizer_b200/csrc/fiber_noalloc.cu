@@ -18,13 +18,17 @@ namespace fiber {
 
 // Largest page count one call accepts; the scratch is 8 B per page (512 KiB).
 constexpr uint32_t kNoAllocMaxPages = 65536;
-// [0] block counter, [1] error word, [2 .. 2 + pages] look-back status words.
-static __device__ __align__(256) unsigned long long g_noalloc_scratch[kNoAllocMaxPages + 2];
+// Scratch words ahead of the look-back status words: [0] page claim counter,
+// [1] error word, [2] finished-block counter, [3] reference total.
+constexpr uint32_t kNoAllocHeadWords = 4;
+static __device__ __align__(256) unsigned long long g_noalloc_scratch[kNoAllocMaxPages + kNoAllocHeadWords];
 
 // One block per page, in page order: exclusive scan of the page's 256 cell
 // counts -> offsets; the page's reference base from a decoupled look-back over
 // pages (prefix_fine_pages, strand_prepass.wgsl:2051-2143, with the ordered
-// base the CUDA path uses instead of the reference's atomic tail).
+// base the CUDA path uses instead of the reference's atomic tail). The block
+// that finishes last writes totals: by then every block has set the error
+// word if one of its waits gave up.
 __global__ void __launch_bounds__(256) k_prefix_pages_noalloc(const uint32_t* __restrict__ counts, uint32_t pages,
                                                               uint32_t* __restrict__ offsets,
                                                               uint32_t* __restrict__ page_base,
@@ -34,7 +38,9 @@ __global__ void __launch_bounds__(256) k_prefix_pages_noalloc(const uint32_t* __
     __shared__ uint32_t s_warp[33];
     uint32_t* counter = reinterpret_cast<uint32_t*>(scratch);
     uint32_t* error = reinterpret_cast<uint32_t*>(scratch + 1);
-    unsigned long long* status = scratch + 2;
+    uint32_t* done = reinterpret_cast<uint32_t*>(scratch + 2);
+    uint32_t* ref_total = reinterpret_cast<uint32_t*>(scratch + 3);
+    unsigned long long* status = scratch + kNoAllocHeadWords;
     for (;;) {
         if (threadIdx.x == 0) s_page = atomicAdd(counter, 1u);
         __syncthreads();
@@ -48,12 +54,17 @@ __global__ void __launch_bounds__(256) k_prefix_pages_noalloc(const uint32_t* __
         if (threadIdx.x == 0) {
             const uint32_t base = lb_exclusive(status, page, 1u, total, error);
             page_base[page] = total > 0u ? base : 0u;
-            if (page == pages - 1u) {
-                totals[0] = base + total;
-                totals[1] = *((volatile uint32_t*)error);
-            }
+            if (page == pages - 1u) *((volatile uint32_t*)ref_total) = base + total;
         }
         __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(done, 1u) == gridDim.x - 1u) {
+            __threadfence();
+            totals[0] = *((volatile uint32_t*)ref_total);
+            totals[1] = *((volatile uint32_t*)error);
+        }
     }
 }
 
@@ -91,9 +102,10 @@ extern "C" fiber_status fiber_prefix_pages_noalloc(const uint32_t* counts, uint3
         }
         scratch = g_scratch_ptr[dev];
     }
-    // The counter, the error word and this call's status words must start at
+    // The counters, the error word and this call's status words must start at
     // zero; the array keeps the previous call's contents.
-    if (cudaMemsetAsync(scratch, 0, ((size_t)pages + 2) * sizeof(unsigned long long), s) != cudaSuccess) {
+    if (cudaMemsetAsync(scratch, 0, ((size_t)pages + kNoAllocHeadWords) * sizeof(unsigned long long), s) !=
+        cudaSuccess) {
         cudaGetLastError();
         return FIBER_ECUDA;
     }

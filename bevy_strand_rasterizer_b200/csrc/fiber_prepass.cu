@@ -375,7 +375,8 @@ __global__ void __launch_bounds__(kFineThreads, 4) k_fine(const FrameParams* __r
         if (threadIdx.x < 32u) {
             uint32_t agg = 0;
             for (int w = 0; w < kFineWarps; ++w) agg += s_warp_count[w];
-            uint32_t base = lb_exclusive_warp(A.lb_status, tile, P.epoch, agg, &A.counters->error);
+            uint32_t base = lb_exclusive_warp(A.lb_status, tile, P.epoch, agg, &A.counters->error, lb_limit(P),
+                                              lb_withheld(P, kStageFine));
             if (threadIdx.x == 0) {
                 s_base = base;
                 if (tile % tiles_per_f == 0u) A.counters->frustum_task_base[f] = base;
@@ -726,6 +727,7 @@ __device__ __forceinline__ bool visits_unused(const PrepassArgs& A) {
 template <bool kOpaque, bool kTel>
 __global__ void __launch_bounds__(kVisitThreads, 4) k_visit(const FrameParams* __restrict__ Pp,
                                                             const InstanceView* __restrict__ inst, PrepassArgs A) {
+    if (frame_failed(A.counters)) return;
     const FrameParams& P = *Pp;
     __shared__ uint32_t s_buf[kVisitSlots * kVisitThreads];
     const uint32_t n = *((volatile uint32_t*)&A.counters->tasks);
@@ -787,6 +789,7 @@ __global__ void __launch_bounds__(kVisitThreads, 4) k_visit(const FrameParams* _
 
 // K9 over visit records: cell counts by atomics; each visit keeps its rank.
 __global__ void __launch_bounds__(256) k_count_visits(PrepassArgs A) {
+    if (frame_failed(A.counters)) return;
     if (visits_unused(A)) return;
     const uint32_t n = (uint32_t)*((volatile unsigned long long*)&A.counters->visits);
     for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
@@ -808,6 +811,7 @@ __global__ void __launch_bounds__(256) k_count_visits(PrepassArgs A) {
 // references (make_fine_seg_ref, :1313-1327) and writes them in canonical
 // order, contiguously.
 __global__ void __launch_bounds__(256) k_fill_visits(PrepassArgs A) {
+    if (frame_failed(A.counters)) return;
     if (visits_unused(A)) return;
     const uint32_t n = (uint32_t)*((volatile unsigned long long*)&A.counters->visits);
     // The visit records stream through once (evict-first loads), so L2 keeps
@@ -827,6 +831,7 @@ __global__ void __launch_bounds__(256) k_fill_visits(PrepassArgs A) {
 template <int PASS, bool kOpaque>
 __global__ void __launch_bounds__(256) k_traverse(const FrameParams* __restrict__ Pp,
                                                   const InstanceView* __restrict__ inst, PrepassArgs A) {
+    if (frame_failed(A.counters)) return;
     if (!visits_unused(A)) return;
     const FrameParams& P = *Pp;
     const uint32_t n = *((volatile uint32_t*)&A.counters->tasks);
@@ -852,6 +857,7 @@ constexpr int kScanThreads = 256;
 constexpr int kScanItems = 4;
 
 __global__ void __launch_bounds__(kScanThreads) k_alloc_pages(const FrameParams* __restrict__ Pp, PrepassArgs A) {
+    if (frame_failed(A.counters)) return;
     const FrameParams& P = *Pp;
     __shared__ uint32_t s_tile, s_base;
     __shared__ uint32_t s_warp[33];
@@ -873,7 +879,8 @@ __global__ void __launch_bounds__(kScanThreads) k_alloc_pages(const FrameParams*
         uint32_t total;
         uint32_t excl = block_exclusive_scan<kScanThreads>(cnt, s_warp, total);
         if (threadIdx.x < 32u) {
-            uint32_t base = lb_exclusive_warp(A.lb_status, tile, P.epoch, total, &A.counters->error);
+            uint32_t base = lb_exclusive_warp(A.lb_status, tile, P.epoch, total, &A.counters->error, lb_limit(P),
+                                              lb_withheld(P, kStageAlloc));
             if (threadIdx.x == 0) {
                 s_base = base;
                 if (tile == n_tiles - 1u) A.counters->pages = min(base + total, P.page_capacity);
@@ -927,7 +934,8 @@ __device__ __forceinline__ uint32_t page_prefix(const FrameParams& P, const Prep
     A.offsets[g] = excl;
     A.cursors[g] = 0u;
     uint32_t base = 0u;
-    if (threadIdx.x < 32u) base = lb_exclusive_warp(A.lb_status, page, P.epoch, total, &A.counters->error);
+    if (threadIdx.x < 32u) base = lb_exclusive_warp(A.lb_status, page, P.epoch, total, &A.counters->error, lb_limit(P),
+                                              lb_withheld(P, kStagePrefix));
     if (threadIdx.x == 0) {
         fiber_fine_page_meta pm = A.page_meta[page];
         uint32_t flags = 0u;
@@ -973,6 +981,7 @@ __device__ __forceinline__ void page_active_tiles(const FrameParams& P, const Pr
 // a warp scan gives the cell offsets and the look-back the page base, with no
 // block barrier.
 __global__ void __launch_bounds__(256) k_prefix_pages(const FrameParams* __restrict__ Pp, PrepassArgs A, bool csr) {
+    if (frame_failed(A.counters)) return;
     if (csr && !visits_unused(A)) return;
     const FrameParams& P = *Pp;
     const uint32_t lane = threadIdx.x & 31u;
@@ -1011,7 +1020,8 @@ __global__ void __launch_bounds__(256) k_prefix_pages(const FrameParams* __restr
         *reinterpret_cast<uint4*>(A.offsets + g0 + 4u) = make_uint4(e[4], e[5], e[6], e[7]);
         *reinterpret_cast<uint4*>(A.cursors + g0) = make_uint4(0u, 0u, 0u, 0u);
         *reinterpret_cast<uint4*>(A.cursors + g0 + 4u) = make_uint4(0u, 0u, 0u, 0u);
-        const uint32_t base = lb_exclusive_warp(A.lb_status, page, P.epoch, total, &A.counters->error);
+        const uint32_t base = lb_exclusive_warp(A.lb_status, page, P.epoch, total, &A.counters->error, lb_limit(P),
+                                              lb_withheld(P, kStagePrefix));
         uint32_t flags = 0u, tile = 0u;
         if (lane == 0u) {
             fiber_fine_page_meta pm = A.page_meta[page];
@@ -1071,6 +1081,7 @@ __global__ void __launch_bounds__(256) k_prefix_pages(const FrameParams* __restr
 // K13: ordered compaction of the active fine-tile flags.
 // ===========================================================================
 __global__ void __launch_bounds__(kScanThreads) k_compact_active(const FrameParams* __restrict__ Pp, PrepassArgs A) {
+    if (frame_failed(A.counters)) return;
     const FrameParams& P = *Pp;
     __shared__ uint32_t s_tile, s_base;
     __shared__ uint32_t s_warp[33];
@@ -1096,7 +1107,8 @@ __global__ void __launch_bounds__(kScanThreads) k_compact_active(const FramePara
         for (int o = 16; o > 0; o >>= 1) cam += __shfl_xor_sync(0xFFFFFFFFu, cam, o);
         if ((threadIdx.x & 31) == 0 && cam) atomicAdd(&A.counters->camera_active, cam);
         if (threadIdx.x < 32u) {
-            uint32_t base = lb_exclusive_warp(A.lb_status, tile, P.epoch, total, &A.counters->error);
+            uint32_t base = lb_exclusive_warp(A.lb_status, tile, P.epoch, total, &A.counters->error, lb_limit(P),
+                                              lb_withheld(P, kStageActive));
             if (threadIdx.x == 0) {
                 s_base = base;
                 if (tile == n_tiles - 1u) A.counters->active_tiles = base + total;
@@ -1233,6 +1245,7 @@ __device__ __forceinline__ void thread_sort_cell(const PrepassArgs& A, const Ins
 // share one coarse z (one page) and the warp scan keeps the slot order. Warps
 // claim tiles and look back on their own; no block barrier is involved.
 __global__ void __launch_bounds__(256) k_emit(const FrameParams* __restrict__ Pp, PrepassArgs A) {
+    if (frame_failed(A.counters)) return;
     const FrameParams& P = *Pp;
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t n_active = *((volatile uint32_t*)&A.counters->active_tiles);
@@ -1284,7 +1297,8 @@ __global__ void __launch_bounds__(256) k_emit(const FrameParams* __restrict__ Pp
         const uint32_t n_work = __shfl_sync(0xFFFFFFFFu, x, 31);
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) load += __shfl_xor_sync(0xFFFFFFFFu, load, o);
-        const uint32_t wb = lb_exclusive_warp(A.lb_status, a, P.epoch, n_work, &A.counters->error);
+        const uint32_t wb = lb_exclusive_warp(A.lb_status, a, P.epoch, n_work, &A.counters->error, lb_limit(P),
+                                              lb_withheld(P, kStageEmit));
         if (lane == 0) {
             A.runs[a] = fiber_raster_tile_run{wb, n_work, f, screen_tile, load, 0u, 0u, 0u};
             if (a == n_active - 1u) A.counters->work_items = wb + n_work;
@@ -1332,6 +1346,7 @@ __device__ __forceinline__ void convert_big_cell(const PrepassArgs& A, const Ins
 // warp per larger cell. A cell longer than a warp sort is converted in place
 // by its warp and queued for k_sort_big_cells.
 __global__ void __launch_bounds__(256, 5) k_sort_cells(const InstanceView* __restrict__ inst, PrepassArgs A) {
+    if (frame_failed(A.counters)) return;
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t n_small = *((volatile uint32_t*)&A.counters->small_cells);
     const uint32_t n_large = *((volatile uint32_t*)&A.counters->large_cells);
@@ -1367,6 +1382,7 @@ __global__ void __launch_bounds__(256, 5) k_sort_cells(const InstanceView* __res
 // Visits per page; each visit keeps its rank inside its page. Lanes of a warp
 // that hit the same page share one atomic.
 __global__ void __launch_bounds__(256) k_page_count(PrepassArgs A) {
+    if (frame_failed(A.counters)) return;
     if (visits_unused(A)) return;
     const uint32_t n = (uint32_t)*((volatile unsigned long long*)&A.counters->visits);
     const uint32_t lane = threadIdx.x & 31u;
@@ -1395,6 +1411,7 @@ __global__ void __launch_bounds__(256) k_page_count(PrepassArgs A) {
 
 // Exclusive scan of the per-page visit counts (one block).
 __global__ void __launch_bounds__(1024) k_page_scan(PrepassArgs A) {
+    if (frame_failed(A.counters)) return;
     if (visits_unused(A)) return;
     __shared__ uint32_t s_warp[33];
     __shared__ uint32_t s_carry;
@@ -1415,6 +1432,7 @@ __global__ void __launch_bounds__(1024) k_page_scan(PrepassArgs A) {
 
 // Visits into their page's bucket: (task, cell) at page base + rank.
 __global__ void __launch_bounds__(256) k_page_scatter(PrepassArgs A) {
+    if (frame_failed(A.counters)) return;
     if (visits_unused(A)) return;
     const uint32_t n = (uint32_t)*((volatile unsigned long long*)&A.counters->visits);
     for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
@@ -1427,6 +1445,7 @@ __global__ void __launch_bounds__(256) k_page_scatter(PrepassArgs A) {
 // One block per page, in page order (the look-back of the page bases).
 __global__ void __launch_bounds__(256) k_build_pages(const FrameParams* __restrict__ Pp,
                                                      const InstanceView* __restrict__ inst, PrepassArgs A) {
+    if (frame_failed(A.counters)) return;
     if (visits_unused(A)) return;
     const FrameParams& P = *Pp;
     __shared__ uint32_t s_tile, s_flags, s_pbase, s_nlarge;
@@ -1517,6 +1536,7 @@ __device__ __forceinline__ void bitonic_pair(uint32_t t, uint32_t size, uint32_t
 }
 
 __global__ void __launch_bounds__(256) k_sort_big_cells(PrepassArgs A) {
+    if (frame_failed(A.counters)) return;
     extern __shared__ unsigned char s_raw[];
     unsigned long long* s_k = reinterpret_cast<unsigned long long*>(s_raw);
     uint32_t* s_m = reinterpret_cast<uint32_t*>(s_raw + kBigSmem * sizeof(unsigned long long));

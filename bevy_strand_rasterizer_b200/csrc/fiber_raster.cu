@@ -211,6 +211,7 @@ __device__ __forceinline__ void candidate_word(const Band& B, bool v, float x0, 
 
 __global__ void __launch_bounds__(kShadowThreads, 14) k_shadow(const FrameParams* __restrict__ Pp,
                                                            const InstanceView* __restrict__ inst, RenderArgs R) {
+    if (frame_failed(R.counters)) return;
     const FrameParams& P = *Pp;
     extern __shared__ float s_dyn[];
     float* sp0x = s_dyn;
@@ -489,6 +490,7 @@ __global__ void __launch_bounds__(kShadowThreads, 14) k_shadow(const FrameParams
 constexpr uint32_t kDomBorder = 1;
 
 __global__ void __launch_bounds__(256) k_dom_request(const FrameParams* __restrict__ Pp, RenderArgs R) {
+    if (frame_failed(R.counters)) return;
     const FrameParams& P = *Pp;
     const uint32_t first = *((volatile uint32_t*)&R.counters->camera_active);
     const uint32_t last = *((volatile uint32_t*)&R.counters->active_tiles);
@@ -512,6 +514,7 @@ __global__ void __launch_bounds__(256) k_dom_request(const FrameParams* __restri
 
 // One block: requested entries, in table order, get pool page index + 1.
 __global__ void __launch_bounds__(1024) k_dom_alloc(const FrameParams* __restrict__ Pp, RenderArgs R, uint32_t entries) {
+    if (frame_failed(R.counters)) return;
     const FrameParams& P = *Pp;
     __shared__ uint32_t s_warp[33];
     __shared__ uint32_t s_carry;
@@ -570,6 +573,7 @@ constexpr uint16_t kEntryInvalid = 0x8000u;
 
 __global__ void __launch_bounds__(kCamThreads) k_raster(const FrameParams* __restrict__ Pp,
                                                         const InstanceView* __restrict__ inst, RenderArgs R) {
+    if (frame_failed(R.counters)) return;
     const FrameParams& P = *Pp;
     // Per staged entry: 64 B of projection, radii and shading texels, the run
     // item and position in it (bit 15: behind the camera, never a candidate).

@@ -239,6 +239,7 @@ __device__ F3 marschner(F3 L, F3 V, F3 U, const fiber_strand_material& m, float 
 
 __global__ void __launch_bounds__(128, 8) k_shade(const FrameParams* __restrict__ Pp,
                                                const InstanceView* __restrict__ inst, RenderArgs R) {
+    if (frame_failed(R.counters)) return;
     const FrameParams& P = *Pp;
     __shared__ QuadTable s_quad;
     fill_quad_table(s_quad);

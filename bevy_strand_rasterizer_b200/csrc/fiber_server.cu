@@ -17,6 +17,7 @@
 // history is off on every slot, so a request's image is the same whichever
 // requests ran before it or next to it.
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
@@ -106,6 +107,7 @@ struct fiber_server {
     std::unordered_set<uint64_t> outstanding;  // submitted, not yet collected by fiber_server_wait
     uint64_t next_ticket = 1;
     bool started = false, stopping = false;
+    std::atomic<uint32_t> rerenders{0};  // frames rendered again after a reference overflow
 };
 
 uint64_t fiber_server_now_ns(void) {
@@ -125,15 +127,24 @@ void release_slot(Slot& s) {
     s.stream = nullptr;
 }
 
-// One request on one slot; returns when its image is in host memory.
-fiber_status render(fiber_server* srv, Slot& slot, const fiber_server_request& r) {
-    fiber_ctx_load_scene(slot.ctx, slot.scenes[r.scene]);
-    fiber_status st = fiber_frame_begin(slot.ctx, &r.camera_cfg, &r.camera, r.light_cfgs, r.lights, r.n_lights,
-                                        slot.stream);
+// One request on one slot; returns when its image is in host memory. A frame
+// whose references overflowed the slot's capacity (sized from the segment
+// count, src/plugin.rs:483-576) raises the slot's reference capacity to what
+// the frame asked for and renders again, so no request returns a truncated
+// image; the slot keeps the larger capacity for later requests.
+fiber_status render(fiber_server* srv, Slot& slot, const fiber_server_request& r, uint32_t* renders) {
+    fiber_status st = fiber_ctx_load_scene(slot.ctx, slot.scenes[r.scene]);
     const void* bg = r.scene_rgba16f ? r.scene_rgba16f : srv->zero_scene;
-    if (st == FIBER_OK) st = fiber_ctx_render_host_nodes(slot.ctx, bg, r.out_rgba16f, slot.stream);
-    if (cudaStreamSynchronize(slot.stream) != cudaSuccess && st == FIBER_OK) st = FIBER_ECUDA;
-    if (st == FIBER_OK) st = fiber_ctx_frame_status(slot.ctx, slot.stream);
+    for (int attempt = 0; st == FIBER_OK && attempt < 3; ++attempt) {
+        if (renders) *renders = (uint32_t)attempt + 1u;
+        st = fiber_frame_begin(slot.ctx, &r.camera_cfg, &r.camera, r.light_cfgs, r.lights, r.n_lights, slot.stream);
+        if (st == FIBER_OK) st = fiber_ctx_render_host_nodes(slot.ctx, bg, r.out_rgba16f, slot.stream);
+        if (cudaStreamSynchronize(slot.stream) != cudaSuccess && st == FIBER_OK) st = FIBER_ECUDA;
+        if (st == FIBER_OK) st = fiber_ctx_frame_status(slot.ctx, slot.stream);
+        if (st != FIBER_EOVERFLOW || !fiber_ctx_grow_refs(slot.ctx, slot.stream)) break;
+        st = FIBER_OK;
+        srv->rerenders.fetch_add(1u);
+    }
     return st;
 }
 
@@ -153,7 +164,7 @@ void worker_main(fiber_server* srv, uint32_t si) {
         res.slot = si;
         res.arrival_ns = p.req.arrival_ns;
         res.admit_ns = fiber_server_now_ns();
-        res.status = render(srv, slot, p.req);
+        res.status = render(srv, slot, p.req, &res.renders);
         res.done_ns = fiber_server_now_ns();
         {
             std::lock_guard<std::mutex> lk(srv->mu);
@@ -258,7 +269,7 @@ fiber_status size_slot(fiber_server* srv, Slot& s) {
         r.lights[l].direction_to_light[1] = 1.0f;
     }
     r.out_rgba16f = srv->warm_out;
-    const fiber_status st = render(srv, s, r);
+    const fiber_status st = render(srv, s, r, nullptr);
     return st == FIBER_EOVERFLOW ? FIBER_OK : st;  // the sizing frame's image is not used
 }
 

@@ -114,9 +114,15 @@ def replay(server, scene_ids, arrivals, requests, outputs) -> dict:
         th.join()
     if errors:
         raise errors[0]
-    lat = np.array([(res.done_ns - res.arrival_ns) / 1e6 for res in results])
+    # A request whose status is not OK (e.g. EOVERFLOW: work dropped, the image
+    # truncated) counts as failed: it is not a frame, and its latency is kept
+    # out of the percentiles.
+    ok = [res for res in results if res.status == abi.OK]
+    lat = np.array([(res.done_ns - res.arrival_ns) / 1e6 for res in ok]) if ok else np.array([np.nan])
     span = (max(res.done_ns for res in results) - min(res.arrival_ns for res in results)) / 1e9
     return {"requests": n, "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
-            "mean_ms": float(lat.mean()), "frames_per_s": n / span, "span_s": span,
+            "mean_ms": float(lat.mean()), "frames_per_s": len(ok) / span, "span_s": span,
             "slots_used": len({res.slot for res in results}),
-            "overflowed": sum(1 for res in results if res.status == abi.EOVERFLOW)}
+            "failed": n - len(ok),
+            "overflowed": sum(1 for res in results if res.status == abi.EOVERFLOW),
+            "rerendered": sum(1 for res in results if res.renders > 1)}

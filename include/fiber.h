@@ -27,6 +27,9 @@
 extern "C" {
 #endif
 
+/* Frusta of one frame: the camera plus up to 15 directional lights. */
+#define FIBER_MAX_FRUSTA 16
+
 /* ------------------------------------------------------------------------ */
 /* Status codes                                                              */
 /* ------------------------------------------------------------------------ */
@@ -249,7 +252,8 @@ typedef struct fiber_stats {
     uint32_t binning_tasks;         /* N = sum_f N_f                          */
     uint32_t camera_tasks;          /* shading queue length                   */
     uint32_t allocated_pages;
-    uint32_t fine_refs;
+    uint32_t fine_refs;             /* references kept (saturates at 2^32-1;
+                                       fine_refs_total holds the full count)  */
     uint32_t active_tiles;
     uint32_t camera_runs;
     uint32_t shadow_runs;
@@ -257,14 +261,17 @@ typedef struct fiber_stats {
     uint32_t overflow_flags;        /* bit0 tasks, bit1 pages, bit2 refs, bit3 work,
                                        bit4 DOM page pool                     */
     uint32_t timeout_flags;         /* non-zero: a bounded device wait gave up */
-    uint32_t frustum_tasks[8];      /* N_f per frustum (first 8)              */
-    uint32_t frustum_pages[8];
-    uint32_t frustum_refs[8];
-    uint32_t frustum_work[8];
-    uint32_t frustum_runs[8];
+    uint32_t frustum_tasks[FIBER_MAX_FRUSTA];  /* N_f per frustum (camera, then lights) */
+    uint32_t frustum_pages[FIBER_MAX_FRUSTA];
+    uint32_t frustum_refs[FIBER_MAX_FRUSTA];
+    uint32_t frustum_work[FIBER_MAX_FRUSTA];
+    uint32_t frustum_runs[FIBER_MAX_FRUSTA];
     uint64_t total_segments;        /* segments of all registered instances   */
     uint64_t total_points;
     uint64_t total_strands;
+    uint64_t fine_refs_total;       /* references kept, 64-bit                */
+    uint64_t refs_requested;        /* references the frame's cells asked for;
+                                       above the kept count when refs overflowed */
 } fiber_stats;
 
 /* PrepassTelemetrySettings counters (src/resources.rs:77-84, collected by
@@ -423,6 +430,21 @@ fiber_status fiber_render_host(fiber_ctx* ctx, const void* scene_rgba16f_host,
 /* Synchronises the context's last stream and returns the frame counters
  * (telemetry words, src/pipelines/prepass.rs:1345-1396). */
 fiber_status fiber_stats_get(fiber_ctx* ctx, fiber_stats* out);
+
+/* ------------------------------------------------------------------------ */
+/* Test hook (no counterpart in the reference)                               */
+/* ------------------------------------------------------------------------ */
+/* Makes the next frame's bounded device waits run out, to exercise the
+ * FIBER_ETIMEDOUT path without faulting or hanging anything. In the frame of
+ * the next fiber_frame_begin, look-back stage `stage` (0 fine prepass, 1 page
+ * allocation, 2 page prefix, 3 active-tile compaction, 4 raster work emit)
+ * has a tile `tile` that never publishes its prefix, and every look-back wait
+ * of that frame gives up after `spin_limit` polls (0: the default 2^21). The
+ * waits behind that tile give up and set the frame's error word; the kernels
+ * after the stage then do nothing, and fiber_stats_get returns
+ * FIBER_ETIMEDOUT with timeout_flags set. The frame after it is normal. */
+fiber_status fiber_debug_stall_lookback(fiber_ctx* ctx, uint32_t stage, uint32_t tile, uint32_t spin_limit);
+
 /* The last frame's prepass telemetry; EINVAL unless telemetry is enabled. */
 fiber_status fiber_telemetry_get(fiber_ctx* ctx, fiber_telemetry* out);
 /* Copies one canonical buffer to host memory. With host == NULL only
@@ -490,6 +512,10 @@ typedef struct fiber_server_result {
     fiber_status status;
     uint32_t slot;                   /* slot that rendered it             */
     uint64_t arrival_ns, admit_ns, done_ns;  /* fiber_server_now_ns clock  */
+    uint32_t renders;                /* frames rendered: 1, or 2-3 when the
+                                        slot's reference capacity had to grow
+                                        (the image is never truncated)     */
+    uint32_t pad;
 } fiber_server_result;
 
 /* Creates a server on `device`; `settings` apply to every slot except that the
@@ -573,12 +599,15 @@ fiber_status fiber_batch_plan(const float* costs, uint32_t n, uint32_t branches,
  * memory: counts[pages * 256] (froxel counts, cell = (z * 4 + y) * 4 + x),
  * offsets[pages * 256] (exclusive prefix within each page), page_base[pages]
  * (first reference of each page, pages in order; 0 for an empty page) and
- * totals[2] (total references; non-zero if a bounded device wait gave up).
+ * totals[2] (total references; non-zero if a bounded device wait gave up,
+ * written by the last block to finish).
  * The only scratch is a fixed file-scope device array (8 B per page, for at
  * most 65536 pages = 512 KiB) that every GPU loading the library keeps until
  * exit; more pages return FIBER_EINVAL. Nothing is allocated or freed. The
  * first call on a device looks up the array's address with that device
- * current, so make it before any stream capture. Every call shares the array
+ * current, so make it before any stream capture; the address is kept for the
+ * life of the process, so after cudaDeviceReset (which may move the array)
+ * reload the library before calling again. Every call shares the array
  * and clears the part it uses: calls that overlap on the GPU (two streams, or
  * two host threads on one device) race. Work is queued on `stream`. */
 fiber_status fiber_prefix_pages_noalloc(const uint32_t* counts, uint32_t pages, uint32_t* offsets,

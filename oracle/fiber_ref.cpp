@@ -1530,31 +1530,51 @@ void stage_telemetry(Ctx& c) {
 }
 
 // ---- K20 composite (strand_composite.wgsl:12-33 + ALPHA_BLENDING) -----------
+// One pixel. The fragment shader's output is `scene` where the scene depth is
+// in front of the strand depth, else mix(scene.rgb, strand.rgb, strand.a) with
+// the scene's alpha (strand_composite.wgsl:23-32). The colour target blends it
+// with BlendState::ALPHA_BLENDING (src/pipelines/composite.rs:115-124) onto
+// the destination loaded with LoadOp::Load (src/nodes/composite.rs:102-118):
+// rgb = src.rgb * src.a + dst.rgb * (1 - src.a), a = src.a * 1 + dst.a * (1 - src.a).
+// The destination is post_process_write().destination, an image of its own;
+// it equals the scene colour only when the pass composites in place.
+void composite_pixel(const float* sc, float sd, const float* st, float strand_depth, const float* dst, float* out) {
+    float frag[4];
+    if (sd > strand_depth) {
+        for (int q = 0; q < 4; ++q) frag[q] = sc[q];
+    } else {
+        for (int q = 0; q < 3; ++q) frag[q] = wmix(sc[q], st[q], st[3]);
+        frag[3] = sc[3];
+    }
+    const float oma = 1.0f - frag[3];
+    for (int q = 0; q < 3; ++q) out[q] = frag[q] * frag[3] + dst[q] * oma;
+    out[3] = frag[3] * 1.0f + dst[3] * oma;
+}
+
+// The frame's composite over one scene image. dest: the destination's
+// contents before the pass (NULL = the scene colour, compositing in place);
+// half_out rounds every channel to binary16 (an RGBA16F target).
+void composite_image(const fref_frame* fr, const float* scene_color, const float* scene_depth, const float* dest,
+                     bool half_out, float* out) {
+    const size_t n = (size_t)fr->W * fr->H;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < (int64_t)n; ++i) {
+        const float* sc = scene_color + 4 * i;
+        const float sd = scene_depth ? scene_depth[i] : 0.0f;
+        float st[4];
+        for (int q = 0; q < 4; ++q) st[q] = from_half_bits(fr->color[i * 4 + q]);
+        float o[4];
+        composite_pixel(sc, sd, st, fr->depth[i], dest ? dest + 4 * i : sc, o);
+        for (int q = 0; q < 4; ++q) out[i * 4 + q] = half_out ? from_half_bits(to_half_bits(o[q])) : o[q];
+    }
+}
+
 void stage_composite(Ctx& c, const float* scene_color, const float* scene_depth) {
     fref_frame* fr = c.fr;
     const size_t n = (size_t)fr->W * fr->H;
     fr->composite.assign(n * 4, 0.0f);
     if (!scene_color) return;
-#pragma omp parallel for schedule(static)
-    for (int64_t i = 0; i < (int64_t)n; ++i) {
-        const float* sc = scene_color + 4 * i;
-        float sd = scene_depth ? scene_depth[i] : 0.0f;
-        float st[4];
-        for (int q = 0; q < 4; ++q) st[q] = from_half_bits(fr->color[i * 4 + q]);
-        float frag[4];
-        if (sd > fr->depth[i]) {
-            for (int q = 0; q < 4; ++q) frag[q] = sc[q];
-        } else {
-            for (int q = 0; q < 3; ++q) frag[q] = wmix(sc[q], st[q], st[3]);
-            frag[3] = sc[3];
-        }
-        // BlendState::ALPHA_BLENDING onto the loaded destination (= scene colour).
-        float oma = 1.0f - frag[3];
-        float out[4];
-        for (int q = 0; q < 3; ++q) out[q] = frag[q] * frag[3] + sc[q] * oma;
-        out[3] = frag[3] * 1.0f + sc[3] * oma;
-        for (int q = 0; q < 4; ++q) fr->composite[i * 4 + q] = from_half_bits(to_half_bits(out[q]));
-    }
+    composite_image(fr, scene_color, scene_depth, nullptr, true, fr->composite.data());
 }
 
 // Frustum table (use_prepass_buffers, src/plugin.rs:386-482): camera first,
@@ -1752,25 +1772,34 @@ void fref_stats(const fref_frame* f, fiber_stats* s) {
     s->allocated_pages = (uint32_t)f->page_meta.size();
     uint64_t refs = 0;
     for (const auto& pm : f->page_meta) refs += pm.seg_ref_count;
-    s->fine_refs = (uint32_t)refs;
+    s->fine_refs = (uint32_t)std::min<uint64_t>(refs, 0xFFFFFFFFull);
+    s->fine_refs_total = refs;
+    s->refs_requested = f->refs_tail;
     s->active_tiles = (uint32_t)f->active_tiles.size();
     s->camera_runs = f->camera_runs;
     s->shadow_runs = f->shadow_runs;
     s->work_items = (uint32_t)f->work.size();
     s->overflow_flags = f->overflow;
-    for (uint32_t i = 0; i < f->F && i < 8; ++i) s->frustum_tasks[i] = f->frustum_task_base[i + 1] - f->frustum_task_base[i];
+    for (uint32_t i = 0; i < f->F && i < FIBER_MAX_FRUSTA; ++i)
+        s->frustum_tasks[i] = f->frustum_task_base[i + 1] - f->frustum_task_base[i];
     for (const auto& pm : f->page_meta) {
         uint32_t fr = frustum_for_tile(f, pm.coarse_tile_id);
-        if (fr < 8) { s->frustum_pages[fr]++; s->frustum_refs[fr] += pm.seg_ref_count; }
+        if (fr < FIBER_MAX_FRUSTA) { s->frustum_pages[fr]++; s->frustum_refs[fr] += pm.seg_ref_count; }
     }
     for (const auto& r : f->runs)
-        if (r.frustum_id < 8) { s->frustum_work[r.frustum_id] += r.work_count; s->frustum_runs[r.frustum_id]++; }
+        if (r.frustum_id < FIBER_MAX_FRUSTA) { s->frustum_work[r.frustum_id] += r.work_count; s->frustum_runs[r.frustum_id]++; }
     s->total_segments = f->total_segments;
     s->total_points = f->total_points;
     s->total_strands = f->total_strands;
 }
 
 void fref_free(fref_frame* f) { delete f; }
+
+void fref_composite(const fref_frame* f, const float* scene_color, const float* scene_depth, const float* dest,
+                    int half_out, float* out) {
+    if (!f || !scene_color || !out) return;
+    composite_image(f, scene_color, scene_depth, dest, half_out != 0, out);
+}
 
 uint32_t fref_wang_hash(uint32_t x) { return wang_hash(x); }
 float fref_hash_to_unit_float(uint32_t x) { return hash_to_unit_float(x); }

@@ -73,6 +73,15 @@ uint64_t fref_get(const fref_frame* f, uint32_t what, void* host, uint64_t capac
 void fref_stats(const fref_frame* f, fiber_stats* out);
 void fref_free(fref_frame* f);
 
+/* The composite of a finished frame's strand image over one scene image
+ * (strand_composite.wgsl:12-33 with ALPHA_BLENDING onto the loaded
+ * destination). scene_color and dest are float RGBA [H][W][4], scene_depth
+ * float [H][W] (NULL: no opaque scene). dest holds the destination's contents
+ * before the pass; NULL composites in place (dest = scene_color). half_out
+ * rounds each output channel to binary16. out: float [H][W][4]. */
+void fref_composite(const fref_frame* f, const float* scene_color, const float* scene_depth, const float* dest,
+                    int half_out, float* out);
+
 /* Extra oracle outputs beyond the fiber_dump_what set. */
 #define FREF_COMPOSITE 100   /* float[W*H*4] composited output (fp16-rounded) */
 #define FREF_REF_KEYS 101    /* u32[R] sort key of each reference             */

@@ -77,6 +77,8 @@ def oracle_lib():
         lib.fref_clip_segment.argtypes = [C.POINTER(C.c_float)] * 5
         lib.fref_build_lut.restype = None
         lib.fref_build_lut.argtypes = [C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.c_uint32, C.c_void_p]
+        lib.fref_composite.restype = None
+        lib.fref_composite.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]
         _LIB = lib
     return _LIB
 
@@ -133,6 +135,20 @@ class OracleFrame:
     def telemetry(self) -> abi.Telemetry:
         w = self.get(FREF_TELEMETRY, np.dtype("<u4"))
         return abi.Telemetry.from_buffer_copy(w.tobytes())
+
+    def composite(self, scene_color: np.ndarray, scene_depth: np.ndarray | None = None,
+                  dest: np.ndarray | None = None, half_out: bool = True) -> np.ndarray:
+        """The frame's composite over scene_color (H, W, 4) float32, blended
+        onto dest (the destination's contents before the pass; None = in
+        place over the scene colour). Returns (H, W, 4) float32."""
+        sc = np.ascontiguousarray(scene_color, np.float32)
+        sd = None if scene_depth is None else np.ascontiguousarray(scene_depth, np.float32)
+        dd = None if dest is None else np.ascontiguousarray(dest, np.float32)
+        out = np.empty_like(sc)
+        oracle_lib().fref_composite(self.handle, sc.ctypes.data, sd.ctypes.data if sd is not None else None,
+                                    dd.ctypes.data if dd is not None else None, 1 if half_out else 0,
+                                    out.ctypes.data)
+        return out
 
     def stage_ms(self) -> np.ndarray:
         return self.get(FREF_STAGE_MS, np.dtype("<f4"))

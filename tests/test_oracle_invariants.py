@@ -168,3 +168,40 @@ def test_telemetry_consistent(tiny):
         runs += fr.raster_runs
     assert runs == s.camera_runs + s.shadow_runs
     assert sum(t.frustum[f].page_candidates for f in range(2)) == t.page_candidates
+
+
+def _composite_numpy(strand_rgba, strand_depth, scene, scene_depth, dest):
+    """strand_composite.wgsl:12-33 + ALPHA_BLENDING onto the loaded destination,
+    restated in numpy (binary32, one rounding per operation)."""
+    f32 = np.float32
+    a = strand_rgba[..., 3:4]
+    mixed = scene[..., :3] * (f32(1) - a) + strand_rgba[..., :3] * a
+    frag = np.concatenate([mixed, scene[..., 3:4]], axis=-1)
+    front = (scene_depth > strand_depth)[..., None]
+    frag = np.where(front, scene, frag).astype(f32)
+    oma = f32(1) - frag[..., 3:4]
+    rgb = frag[..., :3] * frag[..., 3:4] + dest[..., :3] * oma
+    alpha = frag[..., 3:4] * f32(1) + dest[..., 3:4] * oma
+    return np.concatenate([rgb, alpha], axis=-1).astype(f32)
+
+
+def test_composite_against_numpy(tiny):
+    # The oracle's composite over a distinct destination, in place, and with
+    # no scene depth, against the numpy statement of the same rule.
+    scene = build_scene("tiny")
+    h, w = scene.camera_cfg.screen_height, scene.camera_cfg.screen_width
+    strand = tiny.get(abi.DUMP_COLOR).astype(np.float32).reshape(h, w, 4)
+    sdepth = tiny.get(abi.DUMP_DEPTH).reshape(h, w)
+    rng = np.random.default_rng(4)
+    color = rng.uniform(0, 1, (h, w, 4)).astype(np.float16).astype(np.float32)
+    color[..., 3] = rng.uniform(0.2, 1.0, (h, w)).astype(np.float16)
+    depth = np.where(rng.random((h, w)) < 0.5, sdepth * np.float32(0.5), sdepth * np.float32(1.5)).astype(np.float32)
+    dest = rng.uniform(0, 1, (h, w, 4)).astype(np.float32)
+    assert (sdepth > 0).sum() > 100
+    for d, dst in ((depth, dest), (depth, None), (None, dest)):
+        got = tiny.composite(color, d, dst, half_out=False)
+        want = _composite_numpy(strand, sdepth, color, np.zeros_like(sdepth) if d is None else d,
+                                color if dst is None else dst)
+        assert np.array_equal(got, want)
+    half = tiny.composite(color, depth, dest, half_out=True)
+    assert np.array_equal(half, tiny.composite(color, depth, dest, half_out=False).astype(np.float16).astype(np.float32))
