@@ -114,7 +114,7 @@ SERVER_MAX_LIGHTS = 4
 
 class ServerConfig(C.Structure):
     _fields_ = [("slots", u32), ("max_width", u32), ("max_height", u32), ("max_lights", u32), ("max_dom", u32),
-                ("pad", u32), ("hbm_budget", C.c_uint64)]
+                ("priority_levels", u32), ("hbm_budget", C.c_uint64)]
 
 
 class ServerScene(C.Structure):
@@ -131,7 +131,7 @@ class ServerRequest(C.Structure):
 
 class ServerResult(C.Structure):
     _fields_ = [("status", C.c_int), ("slot", u32), ("arrival_ns", C.c_uint64), ("admit_ns", C.c_uint64),
-                ("done_ns", C.c_uint64), ("renders", u32), ("pad", u32)]
+                ("done_ns", C.c_uint64), ("renders", u32), ("priority", u32)]
 
 
 # numpy views of the task-contract structs (src/pipelines/task_contract.rs:45-135)

@@ -122,6 +122,7 @@ struct fiber_ctx {
     cudaEvent_t ev_in = nullptr, ev_out = nullptr;
     // The prepass's cell sort runs on this stream beside the emit.
     cudaStream_t side_stream = nullptr;
+    cudaStream_t side_override = nullptr;  // fiber_ctx_set_side_stream (request server priorities)
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     uint32_t camera_fine_tiles = 0;
     bool opaque_frame = false;  // fiber_opaque_depth ran since fiber_frame_begin
@@ -390,13 +391,14 @@ fiber_status run_prepass(fiber_ctx* c, cudaStream_t s, const OpaqueSource* opaqu
     // emit need only the counts. The sort runs on the side stream beside
     // them (a branch of the frame graph when captured) and joins before the
     // rasters.
+    cudaStream_t side = c->side_override ? c->side_override : c->side_stream;
     FIBER_CUDA(cudaEventRecord(c->ev_fork, s));
-    FIBER_CUDA(cudaStreamWaitEvent(c->side_stream, c->ev_fork, 0));
+    FIBER_CUDA(cudaStreamWaitEvent(side, c->ev_fork, 0));
     LaunchCtx Ls = L;
-    Ls.stream = c->side_stream;
+    Ls.stream = side;
     launch_sort_cells(Ls, A);
     launch_sort_big(Ls, A);
-    FIBER_CUDA(cudaEventRecord(c->ev_join, c->side_stream));
+    FIBER_CUDA(cudaEventRecord(c->ev_join, side));
     set_stage(c, A, kStageActive);
     launch_compact_active(L, A);
     record(c, 8, s);
@@ -835,7 +837,7 @@ fiber_status fiber_frame_begin(fiber_ctx* c, const fiber_froxel_config* cam_cfg,
     P.width = cam_cfg->screen_width;
     P.height = cam_cfg->screen_height;
     // Look-back status regions.
-    uint64_t fine_tiles_lb = (uint64_t)P.F * ((P.total_strands + 7u) / 8u);
+    uint64_t fine_tiles_lb = (uint64_t)P.F * ((P.total_strands + kFineStrandsPerTile - 1u) / kFineStrandsPerTile);
     uint64_t lb_sizes[kStageCount] = {fine_tiles_lb + 1, table / 1024 + 2, page_cap + 1, table / 1024 + 2,
                                       fine_tiles + 1};
     uint64_t lb_total = 0;
@@ -1230,6 +1232,10 @@ uint64_t fiber_ctx_frame_cost(const fiber_ctx* c) {
 }
 
 int fiber_ctx_device(const fiber_ctx* c) { return c->device; }
+
+void fiber_ctx_set_side_stream(fiber_ctx* c, cudaStream_t side) {
+    if (c) c->side_override = side;
+}
 
 fiber_status fiber_ctx_render_host_nodes(fiber_ctx* c, const void* scene_host, void* out_host, cudaStream_t s) {
     if (!c || !scene_host || !out_host) return FIBER_EINVAL;

@@ -23,6 +23,8 @@ constexpr uint32_t kInvalid = 0xFFFFFFFFu;
 constexpr uint32_t kMarked = 0xFFFFFFFEu;  // MARKED_COUNT_PAGE (strand_prepass.wgsl:69)
 constexpr uint32_t kMaxFrusta = 16;
 constexpr uint32_t kPixelSlots = 64;       // strand_rasterizer.wgsl:309,839
+// Strands per look-back tile of the fine prepass (k_fine).
+constexpr uint32_t kFineStrandsPerTile = 64;
 
 // Error words written by device code (never trap).
 constexpr uint32_t kErrTimeout = 1u;

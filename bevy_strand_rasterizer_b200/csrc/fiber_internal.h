@@ -52,3 +52,7 @@ void fiber_ctx_mark_replayed(fiber_ctx* c, cudaStream_t s);
 // Predicted frame cost: segments x frusta + camera pixels + DOM texels.
 uint64_t fiber_ctx_frame_cost(const fiber_ctx* c);
 int fiber_ctx_device(const fiber_ctx* c);
+// The stream the prepass's cell sort forks onto beside the frame's own stream
+// (nullptr: the context's). The request server passes one of the frame's
+// priority, so both branches of a frame run at the same stream priority.
+void fiber_ctx_set_side_stream(fiber_ctx* c, cudaStream_t side);

@@ -268,14 +268,19 @@ __global__ void k_lut(const FrameParams* __restrict__ Pp, PrepassArgs A) {
 }
 
 // ===========================================================================
-// K2 + K6 fine prepass: one warp per strand, eight strands per block, one
-// block per (frustum, strand chunk) in frustum-major order. Each block counts
-// its clipped segments, takes its output offset from a decoupled look-back
-// and writes BinningTask + ProjectedSegment in (frustum, inst, strand, seg)
-// order — the binning queue's canonical order, produced without a sort.
+// K2 + K6 fine prepass: a warp per strand (a lane per segment), each warp
+// taking kFineStrandsPerWarp consecutive strands, one block per (frustum,
+// kFineStrandsPerTile-strand chunk) in frustum-major order. Pass A counts
+// every strand's clipped segments; the block takes its output offset from a
+// decoupled look-back; pass B projects again and writes BinningTask +
+// ProjectedSegment in (frustum, inst, strand, seg) order — the binning
+// queue's canonical order, produced without a sort. A tile of 64 strands
+// spends one look-back (and two block barriers) on 64 strands' work.
 // ===========================================================================
 constexpr int kFineThreads = 256;
 constexpr int kFineWarps = kFineThreads / 32;
+constexpr uint32_t kFineStrandsPerWarp = kFineStrandsPerTile / kFineWarps;
+static_assert(kFineStrandsPerWarp * kFineWarps == kFineStrandsPerTile, "fine tile shape");
 
 struct SegOut {
     uint32_t seg;
@@ -283,16 +288,21 @@ struct SegOut {
     float4 r0, r1;  // world_to_screen_raw of both end points, kept for the rasters
 };
 
-__device__ __forceinline__ bool fine_segment(const FrameParams& P, const InstanceView& in, uint32_t f,
-                                             uint32_t seg, SegOut& o) {
+// world_to_screen_raw (common.wgsl:93-107) of the strand point at index
+// position `pos` after the instance transform.
+__device__ __forceinline__ float4 fine_vertex(const FrameParams& P, const InstanceView& in, uint32_t f, uint32_t pos) {
     const fiber_frustum_desc& d = P.frusta[f];
-    if (seg + 1u >= in.n_indices) return false;
-    uint32_t vi0 = __ldg(in.indices + seg), vi1 = __ldg(in.indices + seg + 1u);
-    float4 a = __ldg(in.vertices + vi0), b = __ldg(in.vertices + vi1);
-    const float* W = in.world_from_local;
-    float4 w0 = matvec(W, a.x, a.y, a.z, 1.0f), w1 = matvec(W, b.x, b.y, b.z, 1.0f);
-    float vw = u2f(d.screen_width), vh = u2f(d.screen_height);
-    float4 r0 = world_to_screen_raw(w0, P.clip[f], vw, vh), r1 = world_to_screen_raw(w1, P.clip[f], vw, vh);
+    const float4 a = __ldg(in.vertices + __ldg(in.indices + pos));
+    const float4 w = matvec(in.world_from_local, a.x, a.y, a.z, 1.0f);
+    return world_to_screen_raw(w, P.clip[f], u2f(d.screen_width), u2f(d.screen_height));
+}
+
+// A segment from its two projected end points: normalised depth, clip to the
+// screen box, quantise (fine_prepass, strand_prepass.wgsl:1016-1140).
+__device__ __forceinline__ bool fine_segment(const FrameParams& P, uint32_t f, uint32_t seg, float4 r0, float4 r1,
+                                             SegOut& o) {
+    const fiber_frustum_desc& d = P.frusta[f];
+    const float vw = u2f(d.screen_width), vh = u2f(d.screen_height);
     F3 p0 = f3(r0.x, r0.y, normalize_depth01(r0.z)), p1 = f3(r1.x, r1.y, normalize_depth01(r1.z));
     F3 c0, c1;
     if (!clip_segment(p0, p1, f3(0.0f, 0.0f, 0.0f), f3(wmax(0.0f, vw - 1e-3f), wmax(0.0f, vh - 1e-3f), 1.0f), c0, c1))
@@ -307,15 +317,67 @@ __device__ __forceinline__ bool fine_segment(const FrameParams& P, const Instanc
     return true;
 }
 
+// Segments c .. c + 30 of a strand, one per lane 0..30: lane l projects point
+// c + l once and takes its segment's far end point from lane l + 1 (a point
+// shared by two segments is projected once, by the same operations).
+constexpr uint32_t kFineChunk = 31;
+__device__ __forceinline__ bool fine_chunk(const FrameParams& P, const InstanceView& in, uint32_t f,
+                                           uint32_t first, uint32_t nseg, uint32_t c, uint32_t lane, SegOut& o) {
+    const uint32_t pos = first + c + lane;
+    const bool has_point = c + lane <= nseg && pos < in.n_indices;
+    float4 r = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    if (has_point) r = fine_vertex(P, in, f, pos);
+    float4 r1;
+    r1.x = __shfl_down_sync(0xFFFFFFFFu, r.x, 1);
+    r1.y = __shfl_down_sync(0xFFFFFFFFu, r.y, 1);
+    r1.z = __shfl_down_sync(0xFFFFFFFFu, r.z, 1);
+    r1.w = __shfl_down_sync(0xFFFFFFFFu, r.w, 1);
+    const bool seg_ok = lane < kFineChunk && c + lane < nseg && pos + 1u < in.n_indices;
+    return seg_ok && fine_segment(P, f, pos, r, r1, o);
+}
+
+// The strand g of frustum f: instance, local strand, segment count, first
+// index and the task's packed field; nseg = 0 when the keep tests drop it.
+struct FineStrand {
+    uint32_t i, s, nseg, meta_offset, packed;
+};
+
+__device__ __forceinline__ FineStrand fine_strand(const FrameParams& P, const InstanceView* __restrict__ inst,
+                                                  const PrepassArgs& A, uint32_t f, uint32_t g) {
+    FineStrand r{0u, 0u, 0u, 0u, 0u};
+    if (g >= P.total_strands) return r;
+    uint32_t lo = 0, hi = P.I;  // last instance with strand_base <= g
+    while (hi - lo > 1u) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (inst[mid].strand_base <= g) lo = mid; else hi = mid;
+    }
+    r.i = lo;
+    r.s = g - inst[lo].strand_base;
+    const InstanceView& in = inst[lo];
+    const fiber_frustum_desc& d = P.frusta[f];
+    const float h = hash_to_unit_float(wang_hash((lo * 16777619u) ^ r.s));
+    bool ok = in.valid && A.inst_visible[lo] != 0u && r.s < in.strand_count && !(h > A.inst_keep[lo]);
+    ok = ok && d.kind <= 1u && r.s < in.n_meta;
+    if (ok) {
+        const fiber_strand_meta m = in.meta[r.s];
+        ok = m.count >= 2u && !(h > A.keep[lo * P.F + f]) && !(d.kind == 1u && light_layer(P, f) == kInvalid);
+        if (ok) {
+            r.nseg = m.count - 1u;
+            r.meta_offset = m.offset;
+            r.packed = ((d.kind == 1u ? 1u : 0u) << 2u) | (f << 3u);
+        }
+    }
+    return r;
+}
+
 __global__ void __launch_bounds__(kFineThreads, 4) k_fine(const FrameParams* __restrict__ Pp,
                                                        const InstanceView* __restrict__ inst, PrepassArgs A) {
     const FrameParams& P = *Pp;
     __shared__ uint32_t s_tile;
     __shared__ uint32_t s_warp_count[kFineWarps];
     __shared__ uint32_t s_base;
-    __shared__ float4 s_proj[kFineWarps][2][32];  // pass A's first-chunk projections, until pass B stores them
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const uint32_t tiles_per_f = ceil_div(P.total_strands, kFineWarps);
+    const uint32_t tiles_per_f = ceil_div(P.total_strands, kFineStrandsPerTile);
     const uint32_t n_tiles = tiles_per_f * P.F;
     for (;;) {
         if (threadIdx.x == 0) s_tile = atomicAdd(A.tile_counter, 1u);
@@ -323,52 +385,19 @@ __global__ void __launch_bounds__(kFineThreads, 4) k_fine(const FrameParams* __r
         const uint32_t tile = s_tile;
         if (tile >= n_tiles) break;
         const uint32_t f = tile / tiles_per_f;
-        const uint32_t g = (tile % tiles_per_f) * kFineWarps + warp;
-        // Resolve the strand (instance, local strand) and the K2/K6 keep tests.
-        uint32_t nseg = 0, i = 0, s = 0, meta_offset = 0, packed = 0;
-        if (g < P.total_strands) {
-            uint32_t lo = 0, hi = P.I;  // last instance with strand_base <= g
-            while (hi - lo > 1u) {
-                uint32_t mid = (lo + hi) >> 1;
-                if (inst[mid].strand_base <= g) lo = mid; else hi = mid;
-            }
-            i = lo;
-            s = g - inst[i].strand_base;
-            const InstanceView& in = inst[i];
-            const fiber_frustum_desc& d = P.frusta[f];
-            float r = hash_to_unit_float(wang_hash((i * 16777619u) ^ s));
-            bool ok = in.valid && A.inst_visible[i] != 0u && s < in.strand_count && !(r > A.inst_keep[i]);
-            ok = ok && d.kind <= 1u && s < in.n_meta;
-            if (ok) {
-                fiber_strand_meta m = in.meta[s];
-                ok = m.count >= 2u && !(r > A.keep[i * P.F + f]) && !(d.kind == 1u && light_layer(P, f) == kInvalid);
-                if (ok) {
-                    nseg = m.count - 1u;
-                    meta_offset = m.offset;
-                    packed = ((d.kind == 1u ? 1u : 0u) << 2u) | (f << 3u);
-                }
-            }
-        }
-        // FRUSTUM_TELEMETRY_RETAINED_STRANDS (:1085): every strand the keep
-        // tests pass (one strand per warp here).
-        if (A.tel && lane == 0 && nseg > 0u) atomicAdd(tel_frustum(A.tel, f, kTelRetainedStrands), 1u);
-        // Pass A: count (results of the first 32 segments stay in registers).
+        const uint32_t g0 = (tile % tiles_per_f) * kFineStrandsPerTile + (uint32_t)warp * kFineStrandsPerWarp;
+        // Pass A: count the clipped segments of the warp's strands.
         uint32_t count = 0;
-        uint32_t first_seg = 0u, first_p0 = 0u, first_p1 = 0u, first_dz = 0u;
-        bool first_ok = false;
-        for (uint32_t c = 0; c < nseg; c += 32u) {
-            SegOut o;
-            bool ok = (c + lane < nseg) && fine_segment(P, inst[i], f, meta_offset + c + lane, o);
-            if (c == 0u) {
-                first_seg = o.seg;
-                first_p0 = o.p0;
-                first_p1 = o.p1;
-                first_dz = o.dz;
-                first_ok = ok;
-                s_proj[warp][0][lane] = o.r0;
-                s_proj[warp][1][lane] = o.r1;
+        for (uint32_t k = 0; k < kFineStrandsPerWarp; ++k) {
+            const FineStrand fs = fine_strand(P, inst, A, f, g0 + k);
+            // FRUSTUM_TELEMETRY_RETAINED_STRANDS (:1085): every strand the
+            // keep tests pass.
+            if (A.tel && lane == 0 && fs.nseg > 0u) atomicAdd(tel_frustum(A.tel, f, kTelRetainedStrands), 1u);
+            for (uint32_t c = 0; c < fs.nseg; c += kFineChunk) {
+                SegOut o;
+                const bool ok = fine_chunk(P, inst[fs.i], f, fs.meta_offset, fs.nseg, c, lane, o);
+                count += __popc(__ballot_sync(0xFFFFFFFFu, ok));
             }
-            count += __popc(__ballot_sync(0xFFFFFFFFu, ok));
         }
         if (lane == 0) s_warp_count[warp] = count;
         __syncthreads();
@@ -389,34 +418,27 @@ __global__ void __launch_bounds__(kFineThreads, 4) k_fine(const FrameParams* __r
         __syncthreads();
         uint32_t out = s_base;
         for (int w = 0; w < warp; ++w) out += s_warp_count[w];
-        // Pass B: write in segment order.
-        for (uint32_t c = 0; c < nseg; c += 32u) {
-            SegOut o;
-            bool ok = first_ok;
-            if (c == 0u) {
-                o.seg = first_seg;
-                o.p0 = first_p0;
-                o.p1 = first_p1;
-                o.dz = first_dz;
-                o.r0 = s_proj[warp][0][lane];
-                o.r1 = s_proj[warp][1][lane];
-            } else {
-                ok = (c + lane < nseg) && fine_segment(P, inst[i], f, meta_offset + c + lane, o);
-            }
-            uint32_t mask = __ballot_sync(0xFFFFFFFFu, ok);
-            if (ok) {
-                uint32_t dst = out + __popc(mask & ((1u << lane) - 1u));
-                if (dst < P.task_capacity) {
-                    reinterpret_cast<uint4*>(A.tasks)[dst] = make_uint4(i, s, o.seg, packed);
-                    fiber_projected_segment ps{o.p0, o.p1, o.dz};
-                    A.projected[dst] = ps;
-                    A.task_proj[2u * (size_t)dst] = o.r0;
-                    A.task_proj[2u * (size_t)dst + 1u] = o.r1;
-                } else {
-                    atomicOr(&A.counters->overflow, 1u);
+        // Pass B: project again and write in segment order.
+        for (uint32_t k = 0; k < kFineStrandsPerWarp; ++k) {
+            const FineStrand fs = fine_strand(P, inst, A, f, g0 + k);
+            for (uint32_t c = 0; c < fs.nseg; c += kFineChunk) {
+                SegOut o;
+                const bool ok = fine_chunk(P, inst[fs.i], f, fs.meta_offset, fs.nseg, c, lane, o);
+                const uint32_t mask = __ballot_sync(0xFFFFFFFFu, ok);
+                if (ok) {
+                    const uint32_t dst = out + __popc(mask & ((1u << lane) - 1u));
+                    if (dst < P.task_capacity) {
+                        reinterpret_cast<uint4*>(A.tasks)[dst] = make_uint4(fs.i, fs.s, o.seg, fs.packed);
+                        fiber_projected_segment ps{o.p0, o.p1, o.dz};
+                        A.projected[dst] = ps;
+                        A.task_proj[2u * (size_t)dst] = o.r0;
+                        A.task_proj[2u * (size_t)dst + 1u] = o.r1;
+                    } else {
+                        atomicOr(&A.counters->overflow, 1u);
+                    }
                 }
+                out += __popc(mask);
             }
-            out += __popc(mask);
         }
         __syncthreads();
     }

@@ -1,21 +1,26 @@
 // fiber_server.cu — the served mode: continuous batching of render requests
 // over scenes kept resident on the device.
 //
-// A server owns S slots. A slot is a fiber_ctx with its own non-blocking
-// stream and worker thread, every resident scene's slabs, and buffers sized at
-// start for the largest scene at the configured maximum frame, so that
-// serving never allocates. Requests queue in arrival order; each worker takes
-// the next request as soon as its previous frame has been read back, so
-// requests that arrive while others are on the GPU are admitted as slots free
-// up, and the frames of different slots overlap on the device. The slot count
-// is what the HBM budget admits (bytes of one sized slot x S <= budget).
+// A server owns S slots. A slot is a fiber_ctx with its own streams and
+// worker thread and buffers sized at start for the largest scene at the
+// configured maximum frame, so that serving never allocates. The scenes'
+// slabs are uploaded once and shared by every slot: a slot switches scenes by
+// loading the shared scene's instance table (host side, no validation kernel,
+// no device synchronisation). The slot count is what the HBM budget admits:
+// (budget - slab bytes) / (bytes of one sized slot's frame buffers), at most
+// kMaxSlots.
 //
-// A request switches its slot to the scene with a host-side table swap (no
-// validation kernel, no device synchronisation), then runs frame_begin, the
-// node sequence and the composite on the slot's stream, with the scene image
-// copied in from host memory and the result copied back. The temporal shadow
-// history is off on every slot, so a request's image is the same whichever
-// requests ran before it or next to it.
+// Requests queue in arrival order; each worker takes the next request as soon
+// as its previous frame has been read back, so requests that arrive while
+// others are on the GPU are admitted as slots free up, and the frames of
+// different slots overlap on the device. A request's frame runs at a stream
+// priority set by its admission order: the oldest frame in flight at the
+// highest, the frames admitted behind it at lower ones, so the device gives
+// the oldest request its blocks first and the younger ones fill the SMs it
+// leaves idle (first come, first served, with backfill).
+//
+// The temporal shadow history is off on every slot, so a request's image is
+// the same whichever requests ran before it or next to it.
 #include <algorithm>
 #include <atomic>
 #include <chrono>
@@ -35,12 +40,14 @@
 
 namespace {
 
-constexpr uint32_t kMaxSlots = 8;
+constexpr uint32_t kMaxSlots = 64;
+constexpr uint32_t kDefaultSlots = 8;  // slots = 0 without an HBM budget
+constexpr uint32_t kMaxLevels = 8;     // stream priority levels used
 
 struct Slot {
     fiber_ctx* ctx = nullptr;
-    cudaStream_t stream = nullptr;
-    std::vector<fiber_scene_state*> scenes;
+    cudaStream_t stream = nullptr;               // sizing frames
+    std::vector<cudaStream_t> streams, sides;    // per priority level: the frame's stream and its side branch
     std::thread worker;
 };
 
@@ -97,7 +104,11 @@ struct fiber_server {
     fiber_settings settings{};
     fiber_server_config cfg{};
     std::vector<Slot> slots;
+    std::vector<fiber_scene_state*> scenes;  // instance tables over slot 0's slabs, shared by all slots
     std::vector<uint64_t> scene_segments;
+    uint64_t slab_bytes = 0;                 // device bytes of the resident scenes
+    std::vector<int> priorities;             // stream priority of each level, highest first
+    uint32_t in_flight = 0;                  // frames rendering now (under mu)
     void* zero_scene = nullptr;  // pinned transparent background, max frame
     void* warm_out = nullptr;    // pinned scratch output of the sizing frames
     std::mutex mu;
@@ -119,29 +130,51 @@ uint64_t fiber_server_now_ns(void) {
 namespace {
 
 void release_slot(Slot& s) {
-    for (fiber_scene_state* st : s.scenes) fiber_scene_state_free(st);
-    s.scenes.clear();
     if (s.ctx) fiber_ctx_destroy(s.ctx);
     if (s.stream) cudaStreamDestroy(s.stream);
-    s.ctx = nullptr;
-    s.stream = nullptr;
+    for (cudaStream_t x : s.streams) cudaStreamDestroy(x);
+    for (cudaStream_t x : s.sides) cudaStreamDestroy(x);
+    s = Slot{};
 }
 
-// One request on one slot; returns when its image is in host memory. A frame
-// whose references overflowed the slot's capacity (sized from the segment
-// count, src/plugin.rs:483-576) raises the slot's reference capacity to what
-// the frame asked for and renders again, so no request returns a truncated
+fiber_status make_slot(fiber_server* srv, Slot& s) {
+    fiber_status st = fiber_ctx_create(srv->device, 0, &s.ctx);
+    if (st == FIBER_OK) st = fiber_settings_set(s.ctx, &srv->settings);
+    if (st == FIBER_OK && cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking) != cudaSuccess) st = FIBER_ECUDA;
+    for (size_t l = 0; l < srv->priorities.size() && st == FIBER_OK; ++l) {
+        cudaStream_t a = nullptr, b = nullptr;
+        if (cudaStreamCreateWithPriority(&a, cudaStreamNonBlocking, srv->priorities[l]) != cudaSuccess ||
+            cudaStreamCreateWithPriority(&b, cudaStreamNonBlocking, srv->priorities[l]) != cudaSuccess) {
+            cudaGetLastError();
+            if (a) cudaStreamDestroy(a);
+            st = FIBER_ECUDA;
+            break;
+        }
+        s.streams.push_back(a);
+        s.sides.push_back(b);
+    }
+    return st;
+}
+
+// One request on one slot at priority `level` (nullptr streams: the sizing
+// stream); returns when its image is in host memory. A frame whose references
+// overflowed the slot's capacity (sized from the segment count,
+// src/plugin.rs:483-576) raises the slot's reference capacity to what the
+// frame asked for and renders again, so no request returns a truncated
 // image; the slot keeps the larger capacity for later requests.
-fiber_status render(fiber_server* srv, Slot& slot, const fiber_server_request& r, uint32_t* renders) {
-    fiber_status st = fiber_ctx_load_scene(slot.ctx, slot.scenes[r.scene]);
+fiber_status render(fiber_server* srv, Slot& slot, const fiber_server_request& r, uint32_t* renders,
+                    int level = -1) {
+    fiber_status st = fiber_ctx_load_scene(slot.ctx, srv->scenes[r.scene]);
+    const cudaStream_t stream = level < 0 ? slot.stream : slot.streams[level];
+    fiber_ctx_set_side_stream(slot.ctx, level < 0 ? nullptr : slot.sides[level]);
     const void* bg = r.scene_rgba16f ? r.scene_rgba16f : srv->zero_scene;
     for (int attempt = 0; st == FIBER_OK && attempt < 3; ++attempt) {
         if (renders) *renders = (uint32_t)attempt + 1u;
-        st = fiber_frame_begin(slot.ctx, &r.camera_cfg, &r.camera, r.light_cfgs, r.lights, r.n_lights, slot.stream);
-        if (st == FIBER_OK) st = fiber_ctx_render_host_nodes(slot.ctx, bg, r.out_rgba16f, slot.stream);
-        if (cudaStreamSynchronize(slot.stream) != cudaSuccess && st == FIBER_OK) st = FIBER_ECUDA;
-        if (st == FIBER_OK) st = fiber_ctx_frame_status(slot.ctx, slot.stream);
-        if (st != FIBER_EOVERFLOW || !fiber_ctx_grow_refs(slot.ctx, slot.stream)) break;
+        st = fiber_frame_begin(slot.ctx, &r.camera_cfg, &r.camera, r.light_cfgs, r.lights, r.n_lights, stream);
+        if (st == FIBER_OK) st = fiber_ctx_render_host_nodes(slot.ctx, bg, r.out_rgba16f, stream);
+        if (cudaStreamSynchronize(stream) != cudaSuccess && st == FIBER_OK) st = FIBER_ECUDA;
+        if (st == FIBER_OK) st = fiber_ctx_frame_status(slot.ctx, stream);
+        if (st != FIBER_EOVERFLOW || !fiber_ctx_grow_refs(slot.ctx, stream)) break;
         st = FIBER_OK;
         srv->rerenders.fetch_add(1u);
     }
@@ -153,21 +186,26 @@ void worker_main(fiber_server* srv, uint32_t si) {
     Slot& slot = srv->slots[si];
     for (;;) {
         Pending p;
+        uint32_t level = 0;
         {
             std::unique_lock<std::mutex> lk(srv->mu);
             srv->cv_work.wait(lk, [&] { return srv->stopping || !srv->queue.empty(); });
             if (srv->queue.empty()) return;
             p = srv->queue.front();
             srv->queue.pop_front();
+            level = std::min<uint32_t>(srv->in_flight, (uint32_t)srv->priorities.size() - 1u);
+            ++srv->in_flight;
         }
         fiber_server_result res{};
         res.slot = si;
+        res.priority = level;
         res.arrival_ns = p.req.arrival_ns;
         res.admit_ns = fiber_server_now_ns();
-        res.status = render(srv, slot, p.req, &res.renders);
+        res.status = render(srv, slot, p.req, &res.renders, (int)level);
         res.done_ns = fiber_server_now_ns();
         {
             std::lock_guard<std::mutex> lk(srv->mu);
+            --srv->in_flight;
             srv->done[p.ticket] = res;
         }
         srv->cv_done.notify_all();
@@ -183,25 +221,30 @@ fiber_status fiber_server_create(int device, const fiber_settings* settings, con
     if (cfg->slots > kMaxSlots || cfg->max_width == 0 || cfg->max_height == 0 ||
         cfg->max_lights > FIBER_SERVER_MAX_LIGHTS || (cfg->max_lights && cfg->max_dom == 0))
         return FIBER_EINVAL;
+    if (cudaSetDevice(device) != cudaSuccess) {
+        cudaGetLastError();
+        return FIBER_EINVAL;
+    }
     fiber_server* srv = new fiber_server();
     srv->device = device;
     srv->cfg = *cfg;
     if (settings) srv->settings = *settings;
     else fiber_settings_default(&srv->settings);
     srv->settings.history_enabled = 0u;
-    const uint32_t n = cfg->slots ? cfg->slots : kMaxSlots;
-    srv->slots.resize(n);
-    fiber_status st = FIBER_OK;
-    if (cudaSetDevice(device) != cudaSuccess) st = FIBER_EINVAL;
-    for (uint32_t i = 0; i < n && st == FIBER_OK; ++i) {
-        Slot& s = srv->slots[i];
-        st = fiber_ctx_create(device, 0, &s.ctx);
-        if (st == FIBER_OK) st = fiber_settings_set(s.ctx, &srv->settings);
-        if (st == FIBER_OK && cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking) != cudaSuccess)
-            st = FIBER_ECUDA;
+    // Priority levels, highest first (CUDA: a lower number is a higher priority).
+    int least = 0, greatest = 0;
+    if (cudaDeviceGetStreamPriorityRange(&least, &greatest) != cudaSuccess) {
+        cudaGetLastError();
+        least = greatest = 0;
     }
+    const uint32_t want = cfg->priority_levels ? std::min<uint32_t>(cfg->priority_levels, kMaxLevels) : kMaxLevels;
+    for (int pr = greatest; pr <= least && srv->priorities.size() < want; ++pr) srv->priorities.push_back(pr);
+    if (srv->priorities.empty()) srv->priorities.push_back(0);
+    // Slot 0 holds the scenes' slabs; the other slots are made at start.
+    srv->slots.resize(1);
+    const fiber_status st = make_slot(srv, srv->slots[0]);
     if (st != FIBER_OK) {
-        for (Slot& s : srv->slots) release_slot(s);
+        release_slot(srv->slots[0]);
         delete srv;
         return st;
     }
@@ -221,30 +264,28 @@ fiber_status fiber_server_add_scene(fiber_server* srv, const fiber_server_scene*
     const void* src[5] = {sc->vertices, sc->indices, sc->meta, &sc->geo, sc->materials};
     const uint32_t kinds[5] = {FIBER_SLAB_VERT, FIBER_SLAB_INDEX, FIBER_SLAB_META, FIBER_SLAB_GEO,
                                FIBER_SLAB_MATERIAL};
-    uint64_t segments = 0;
-    for (Slot& s : srv->slots) {
-        uint32_t ids[5];
-        for (int k = 0; k < 5; ++k) {
-            fiber_devptr dp;
-            fiber_status st = fiber_slab_alloc(s.ctx, kinds[k], bytes[k], &ids[k], &dp);
-            if (st == FIBER_OK) st = fiber_slab_upload(s.ctx, kinds[k], ids[k], 0, src[k], bytes[k], nullptr);
-            if (st != FIBER_OK) return st;
-        }
-        fiber_strand_instance row;
-        std::memset(&row, 0, sizeof(row));
-        row.vertex_id = ids[0];
-        row.index_id = ids[1];
-        row.meta_id = ids[2];
-        row.geo_id = ids[3];
-        row.material_id = ids[4];
-        std::memcpy(row.world_from_local, sc->world_from_local, sizeof(row.world_from_local));
-        invert4(sc->world_from_local, row.local_from_world);
-        fiber_status st = fiber_instance_set(s.ctx, &row, 1u);
+    Slot& s = srv->slots[0];
+    uint32_t ids[5];
+    for (int k = 0; k < 5; ++k) {
+        fiber_devptr dp;
+        fiber_status st = fiber_slab_alloc(s.ctx, kinds[k], bytes[k], &ids[k], &dp);
+        if (st == FIBER_OK) st = fiber_slab_upload(s.ctx, kinds[k], ids[k], 0, src[k], bytes[k], nullptr);
         if (st != FIBER_OK) return st;
-        s.scenes.push_back(fiber_ctx_save_scene(s.ctx));
-        segments = fiber_scene_segments(s.scenes.back());
+        srv->slab_bytes += bytes[k];
     }
-    srv->scene_segments.push_back(segments);
+    fiber_strand_instance row;
+    std::memset(&row, 0, sizeof(row));
+    row.vertex_id = ids[0];
+    row.index_id = ids[1];
+    row.meta_id = ids[2];
+    row.geo_id = ids[3];
+    row.material_id = ids[4];
+    std::memcpy(row.world_from_local, sc->world_from_local, sizeof(row.world_from_local));
+    invert4(sc->world_from_local, row.local_from_world);
+    const fiber_status st = fiber_instance_set(s.ctx, &row, 1u);
+    if (st != FIBER_OK) return st;
+    srv->scenes.push_back(fiber_ctx_save_scene(s.ctx));
+    srv->scene_segments.push_back(fiber_scene_segments(srv->scenes.back()));
     *scene_id = (uint32_t)(srv->scene_segments.size() - 1u);
     return FIBER_OK;
 }
@@ -287,13 +328,24 @@ fiber_status fiber_server_start(fiber_server* srv, uint32_t* slots_started) {
     std::memset(srv->zero_scene, 0, frame_bytes);
     fiber_status st = size_slot(srv, srv->slots[0]);
     if (st != FIBER_OK) return st;
-    // Admission by HBM budget: as many sized slots as the budget holds.
-    const uint64_t per_slot = std::max<uint64_t>(1, fiber_ctx_allocated(srv->slots[0].ctx));
-    uint32_t n = (uint32_t)srv->slots.size();
-    if (srv->cfg.hbm_budget) n = (uint32_t)std::min<uint64_t>(n, std::max<uint64_t>(1, srv->cfg.hbm_budget / per_slot));
-    for (uint32_t i = n; i < srv->slots.size(); ++i) release_slot(srv->slots[i]);
+    // Admission by HBM budget: the slabs once, then as many sized slots as the
+    // rest of the budget holds.
+    // A slot whose request outgrows its reference capacity grows it (render),
+    // so each slot is counted at 1.5 times its sized bytes: the headroom that
+    // lets half the slots double their reference buffers within the budget.
+    const uint64_t held = fiber_ctx_allocated(srv->slots[0].ctx);
+    const uint64_t sized = held > srv->slab_bytes ? held - srv->slab_bytes : held;
+    const uint64_t per_slot = std::max<uint64_t>(1, sized + sized / 2u);
+    uint32_t n = srv->cfg.slots ? srv->cfg.slots : (srv->cfg.hbm_budget ? kMaxSlots : kDefaultSlots);
+    if (srv->cfg.hbm_budget) {
+        const uint64_t room = srv->cfg.hbm_budget > srv->slab_bytes ? srv->cfg.hbm_budget - srv->slab_bytes : 0u;
+        n = (uint32_t)std::min<uint64_t>(n, std::max<uint64_t>(1, room / per_slot));
+    }
     srv->slots.resize(n);
-    for (uint32_t i = 1; i < n && st == FIBER_OK; ++i) st = size_slot(srv, srv->slots[i]);
+    for (uint32_t i = 1; i < n && st == FIBER_OK; ++i) {
+        st = make_slot(srv, srv->slots[i]);
+        if (st == FIBER_OK) st = size_slot(srv, srv->slots[i]);
+    }
     if (st != FIBER_OK) return st;
     srv->started = true;
     for (uint32_t i = 0; i < n; ++i) srv->slots[i].worker = std::thread(worker_main, srv, i);
@@ -347,7 +399,9 @@ fiber_status fiber_server_destroy(fiber_server* srv) {
     for (Slot& s : srv->slots)
         if (s.worker.joinable()) s.worker.join();
     cudaSetDevice(srv->device);
-    for (Slot& s : srv->slots) release_slot(s);
+    // Slot 0 owns the slabs every scene state points into: release it last.
+    for (size_t i = srv->slots.size(); i-- > 0;) release_slot(srv->slots[i]);
+    for (fiber_scene_state* st : srv->scenes) fiber_scene_state_free(st);
     if (srv->zero_scene) cudaFreeHost(srv->zero_scene);
     if (srv->warm_out) cudaFreeHost(srv->warm_out);
     delete srv;

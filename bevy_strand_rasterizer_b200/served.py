@@ -88,7 +88,7 @@ def replay(server, scene_ids, arrivals, requests, outputs) -> dict:
             if tickets[i] == 0 or errors:
                 continue
             try:
-                results[i] = server.wait(tickets[i])
+                results[i] = server.wait(tickets[i], check=False)
             except Exception as e:  # re-raised by the submitting thread
                 errors.append(e)
 
@@ -125,4 +125,5 @@ def replay(server, scene_ids, arrivals, requests, outputs) -> dict:
             "slots_used": len({res.slot for res in results}),
             "failed": n - len(ok),
             "overflowed": sum(1 for res in results if res.status == abi.EOVERFLOW),
+            "statuses": sorted({abi.STATUS_NAMES.get(res.status, str(res.status)) for res in results}),
             "rerendered": sum(1 for res in results if res.renders > 1)}

@@ -34,10 +34,10 @@ def _host_ptr(buf) -> int:
 class FiberServer:
     def __init__(self, device: int = 0, slots: int = 0, max_width: int = 1920, max_height: int = 1080,
                  max_lights: int = 1, max_dom: int = 2048, hbm_budget: int = 0,
-                 settings: abi.Settings | None = None):
+                 settings: abi.Settings | None = None, priority_levels: int = 0):
         self.lib = abi.load_library()
         self.srv = C.c_void_p()
-        cfg = abi.ServerConfig(slots, max_width, max_height, max_lights, max_dom, 0, hbm_budget)
+        cfg = abi.ServerConfig(slots, max_width, max_height, max_lights, max_dom, priority_levels, hbm_budget)
         st = settings if settings is not None else abi.default_settings()
         abi.check(self.lib.fiber_server_create(device, C.byref(st), C.byref(cfg), C.byref(self.srv)),
                   "fiber_server_create")
@@ -94,14 +94,16 @@ class FiberServer:
         self._keep[int(t.value)] = (r, out, scene_rgba16f)
         return int(t.value)
 
-    def wait(self, ticket: int, allow_overflow: bool = True) -> abi.ServerResult:
+    def wait(self, ticket: int, allow_overflow: bool = True, check: bool = True) -> abi.ServerResult:
         """Result of a request. EOVERFLOW (a capacity-sized queue dropped work,
         flagged exactly as the reference flags it; the image was still written)
-        is returned, not raised, unless allow_overflow is False."""
+        is returned, not raised, unless allow_overflow is False; with
+        check=False every status is returned in the result."""
         res = abi.ServerResult()
         abi.check(self.lib.fiber_server_wait(self.srv, ticket, C.byref(res)), "fiber_server_wait")
         self._keep.pop(ticket, None)
-        abi.check(res.status, f"request {ticket}", (abi.OK, abi.EOVERFLOW) if allow_overflow else (abi.OK,))
+        if check:
+            abi.check(res.status, f"request {ticket}", (abi.OK, abi.EOVERFLOW) if allow_overflow else (abi.OK,))
         return res
 
     def close(self):

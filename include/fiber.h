@@ -470,13 +470,16 @@ typedef struct fiber_server fiber_server;
 
 typedef struct fiber_server_config {
     uint32_t slots;        /* frames in flight at once (each slot is a context with
-                              its own stream and worker thread); 0 = as many as the
-                              HBM budget admits, at most 8                         */
+                              its own streams and worker thread); 0 = as many as
+                              the HBM budget admits, at most 64 (8 without a
+                              budget); a budget also caps a non-zero count     */
     uint32_t max_width;    /* largest request resolution; every slot is sized   */
     uint32_t max_height;   /* for it at fiber_server_start                      */
     uint32_t max_lights;   /* most lights of one request (<= 4)                 */
     uint32_t max_dom;      /* largest deep-shadow map side of one request       */
-    uint32_t pad;
+    uint32_t priority_levels; /* stream priorities the frames in flight take by
+                              admission order (oldest highest): 0 = every level
+                              the device offers, 1 = one priority for all   */
     uint64_t hbm_budget;   /* device bytes all slots may hold (0 = no cap)      */
 } fiber_server_config;
 
@@ -515,7 +518,9 @@ typedef struct fiber_server_result {
     uint32_t renders;                /* frames rendered: 1, or 2-3 when the
                                         slot's reference capacity had to grow
                                         (the image is never truncated)     */
-    uint32_t pad;
+    uint32_t priority;               /* stream priority level of its frame:
+                                        0 = highest (admitted with no frame
+                                        in flight)                         */
 } fiber_server_result;
 
 /* Creates a server on `device`; `settings` apply to every slot except that the
@@ -523,7 +528,8 @@ typedef struct fiber_server_result {
  * which requests ran before it on the same slot. */
 fiber_status fiber_server_create(int device, const fiber_settings* settings, const fiber_server_config* cfg,
                                  fiber_server** out);
-/* Uploads a scene to every slot (before fiber_server_start). */
+/* Uploads a scene once (before fiber_server_start); every slot renders from
+ * the same device-resident slabs. */
 fiber_status fiber_server_add_scene(fiber_server* srv, const fiber_server_scene* scene, uint32_t* scene_id);
 /* Sizes every slot for the largest scene at the configured maximum frame,
  * settles the slot count under the HBM budget and starts the workers. */
