@@ -58,6 +58,7 @@ struct PrepassArgs {
     uint32_t* inst_visible;          // [I]
     float* inst_keep;                // [I] max(camera, shadow) keep probability
     fiber_coarse_depth_lut_entry* lut;
+    uint8_t* lut_simple;  // [coarse tiles] 1: the LUT's 16 entries are populated, ordered and disjoint
     fiber_binning_task* tasks;
     fiber_projected_segment* projected;
     uint32_t* page_table;

@@ -252,6 +252,10 @@ __global__ void k_lut(const FrameParams* __restrict__ Pp, PrepassArgs A) {
         maxs[j] = kmax;
     }
     uint32_t out_slice = 0;
+    // simple: all 16 entries populated, each start <= end, each end below the
+    // next start (the lookup in lut_slices may then binary-search).
+    bool simple = true;
+    uint32_t prev_end = 0u;
     for (uint32_t k = 0; k < count; ++k) {
         uint32_t base_slices = max(1u, kDepthSlices / count);
         uint32_t rem = kDepthSlices % count;
@@ -261,9 +265,12 @@ __global__ void k_lut(const FrameParams* __restrict__ Pp, PrepassArgs A) {
             uint32_t start = mins[k] + (span * s) / slices;
             uint32_t excl_end = mins[k] + (span * (s + 1u)) / slices;
             uint32_t end = min(excl_end > start ? excl_end - 1u : start, maxs[k]);
+            simple = simple && start <= end && (out_slice == 0u || prev_end < start);
+            prev_end = end;
             out[out_slice++] = fiber_coarse_depth_lut_entry{start, end, start, max(1u, end - start + 1u)};
         }
     }
+    A.lut_simple[t] = (simple && out_slice == kDepthSlices) ? 1u : 0u;
     for (; out_slice < kDepthSlices; ++out_slice) out[out_slice] = fiber_coarse_depth_lut_entry{0u, 0u, 0u, 0u};
 }
 
@@ -467,6 +474,25 @@ constexpr uint32_t kVisitSlots = 32;  // buffered visits per task; p99 is about 
 constexpr uint32_t kThreadSortMax = 8;
 constexpr uint32_t kWarpSortMax = 256;
 
+// lut_slices for one end point of a LUT whose 16 entries are all populated,
+// each start <= end and each end below the next start: at most one entry
+// holds the quantised depth q, and the nearest entry otherwise is a neighbour
+// of the gap q falls in, so a binary search over the starts returns what the
+// linear scan returns (first holding entry, else first nearest).
+__device__ __forceinline__ uint32_t lut_slice_simple(const fiber_coarse_depth_lut_entry* e, float z) {
+    const uint32_t q = quantize_depth01(z);
+    const uint2* xy = reinterpret_cast<const uint2*>(e);  // entry i: xy[2 i] = (z_min_q, z_max_q)
+    int lo = -1;  // last entry with start <= q
+#pragma unroll
+    for (int step = 16; step > 0; step >>= 1)
+        if (lo + step < (int)kDepthSlices && __ldg(&xy[2 * (lo + step)]).x <= q) lo += step;
+    if (lo < 0) return 0u;
+    const uint2 a = __ldg(&xy[2 * lo]);
+    if (q <= a.y || lo == (int)kDepthSlices - 1) return (uint32_t)lo;
+    const uint32_t next_start = __ldg(&xy[2 * (lo + 1)]).x;
+    return (q - a.y <= next_start - q) ? (uint32_t)lo : (uint32_t)lo + 1u;
+}
+
 // lut_slice for both clipped end points at once: per end point, the first
 // populated slice whose [z_min_q, z_max_q] holds its quantised depth, else the
 // first populated slice nearest to it, else kInvalid. One unrolled pass over
@@ -589,7 +615,12 @@ __device__ __forceinline__ void walk_page(const PrepassArgs& A, F3 p0, const Cli
     const ClipDir cd = clip_dir(c0, c1);  // shared by the slice clips below
     const fiber_coarse_depth_lut_entry* lut = A.lut + (size_t)tile * kDepthSlices;
     uint32_t z0s, z1s;
-    lut_slices(lut, c0.z, c1.z, z0s, z1s);
+    if (A.lut_simple[tile]) {
+        z0s = lut_slice_simple(lut, c0.z);
+        z1s = lut_slice_simple(lut, c1.z);
+    } else {
+        lut_slices(lut, c0.z, c1.z, z0s, z1s);
+    }
     if (z0s == kInvalid || z1s == kInvalid) return;
     for (uint32_t cz = min(z0s, z1s); cz <= max(z0s, z1s); ++cz) {
         fiber_coarse_depth_lut_entry e = lut[cz];
@@ -1233,18 +1264,8 @@ __device__ __forceinline__ void warp_sort_any(const PrepassArgs& A, const Instan
     else warp_sort_cell<8>(A, inst, base, n, lane);
 }
 
-// One thread sorts a cell of at most 8 references in registers: Batcher's
-// odd-even merge network for 8 inputs (19 comparators); padding sorts last.
-__device__ __forceinline__ void thread_sort_cell(const PrepassArgs& A, const InstanceView* __restrict__ inst,
-                                                 uint32_t base, uint32_t n) {
-    unsigned long long k[8];
-    uint32_t task[8];
-#pragma unroll
-    for (int e = 0; e < 8; ++e) {
-        k[e] = ~0ull;
-        task[e] = 0u;
-        if ((uint32_t)e < n) task_entry(A, inst, A.ref_keys[base + e], k[e], task[e]);
-    }
+// Batcher's odd-even merge network for 8 (key, task) pairs in registers.
+__device__ __forceinline__ void sort8(unsigned long long* k, uint32_t* task) {
     auto cas = [&](int a, int b) {
         if (k[a] > k[b]) {
             const unsigned long long tk = k[a]; k[a] = k[b]; k[b] = tk;
@@ -1257,6 +1278,21 @@ __device__ __forceinline__ void thread_sort_cell(const PrepassArgs& A, const Ins
     cas(0, 4); cas(1, 5); cas(2, 6); cas(3, 7);
     cas(2, 4); cas(3, 5);
     cas(1, 2); cas(3, 4); cas(5, 6);
+}
+
+// One thread sorts a cell of at most 8 references in registers: Batcher's
+// odd-even merge network for 8 inputs (19 comparators); padding sorts last.
+__device__ __forceinline__ void thread_sort_cell(const PrepassArgs& A, const InstanceView* __restrict__ inst,
+                                                 uint32_t base, uint32_t n) {
+    unsigned long long k[8];
+    uint32_t task[8];
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+        k[e] = ~0ull;
+        task[e] = 0u;
+        if ((uint32_t)e < n) task_entry(A, inst, A.ref_keys[base + e], k[e], task[e]);
+    }
+    sort8(k, task);
 #pragma unroll
     for (int e = 0; e < 8; ++e)
         if ((uint32_t)e < n) store_entry(A, base + e, k[e], task[e]);
@@ -1362,21 +1398,88 @@ __device__ __forceinline__ void convert_big_cell(const PrepassArgs& A, const Ins
     }
 }
 
+// 32 consecutive small cells at once. k_prefix_pages lists a page's small
+// cells together, in cell order, so their references usually form one span
+// [lo, hi) of the reference array (holes: the page's larger cells). When the
+// span fits kSortSpan, the warp reads it coalesced into shared memory with
+// every entry's gathered key, each lane sorts its cell there (the same
+// network as thread_sort_cell) and the warp writes the span's owned entries
+// back coalesced; otherwise each lane sorts its cell alone.
+constexpr uint32_t kSortSpan = 256;
+struct SortSpanSmem {
+    unsigned long long key[kSortSpan];
+    uint32_t task[kSortSpan];
+    uint8_t own[kSortSpan];
+};
+
+__device__ __forceinline__ void warp_sort_small_cells(const PrepassArgs& A, const InstanceView* __restrict__ inst,
+                                                      uint32_t i0, uint32_t n_small, uint32_t lane,
+                                                      SortSpanSmem& sm) {
+    const uint32_t i = i0 + lane;
+    const bool has = i < n_small;
+    const uint2 e = has ? A.cells_small[i] : make_uint2(0u, 0u);
+    uint32_t lo = has ? e.x : 0xFFFFFFFFu, hi = has ? e.x + e.y : 0u;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        lo = min(lo, __shfl_xor_sync(0xFFFFFFFFu, lo, o));
+        hi = max(hi, __shfl_xor_sync(0xFFFFFFFFu, hi, o));
+    }
+    if (hi <= lo || hi - lo > kSortSpan) {
+        if (has) thread_sort_cell(A, inst, e.x, e.y);
+        return;
+    }
+    const uint32_t span = hi - lo;
+    for (uint32_t j = lane; j < span; j += 32u) sm.own[j] = 0u;
+    __syncwarp();
+    if (has)
+        for (uint32_t r = 0; r < e.y; ++r) sm.own[e.x - lo + r] = 1u;
+    __syncwarp();
+    for (uint32_t j = lane; j < span; j += 32u) {
+        if (!sm.own[j]) continue;
+        unsigned long long key;
+        uint32_t task;
+        task_entry(A, inst, A.ref_keys[lo + j], key, task);
+        sm.key[j] = key;
+        sm.task[j] = task;
+    }
+    __syncwarp();
+    if (has) {
+        unsigned long long k[8];
+        uint32_t task[8];
+        const uint32_t b = e.x - lo;
+#pragma unroll
+        for (uint32_t r = 0; r < 8u; ++r) {
+            k[r] = r < e.y ? sm.key[b + r] : ~0ull;
+            task[r] = r < e.y ? sm.task[b + r] : 0u;
+        }
+        sort8(k, task);
+#pragma unroll
+        for (uint32_t r = 0; r < 8u; ++r)
+            if (r < e.y) {
+                sm.key[b + r] = k[r];
+                sm.task[b + r] = task[r];
+            }
+    }
+    __syncwarp();
+    for (uint32_t j = lane; j < span; j += 32u)
+        if (sm.own[j]) store_entry(A, lo + j, sm.key[j], sm.task[j]);
+    __syncwarp();
+}
+
 // Canonical order inside every cell (projected depth key descending, then
 // instance, then segment), after the fill, over the cell lists k_prefix_pages
-// made: a thread per cell of up to 8 references (nearly all of them), then a
-// warp per larger cell. A cell longer than a warp sort is converted in place
-// by its warp and queued for k_sort_big_cells.
+// made: a warp per 32 cells of up to 8 references (nearly all of them), then
+// a warp per larger cell. A cell longer than a warp sort is converted in
+// place by its warp and queued for k_sort_big_cells.
 __global__ void __launch_bounds__(256, 5) k_sort_cells(const InstanceView* __restrict__ inst, PrepassArgs A) {
     if (frame_failed(A.counters)) return;
+    __shared__ SortSpanSmem s_span[8];
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t n_small = *((volatile uint32_t*)&A.counters->small_cells);
     const uint32_t n_large = *((volatile uint32_t*)&A.counters->large_cells);
     const uint32_t stride = gridDim.x * blockDim.x;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n_small; i += stride) {
-        const uint2 e = A.cells_small[i];
-        thread_sort_cell(A, inst, e.x, e.y);
-    }
+    for (uint32_t i0 = (blockIdx.x * blockDim.x + threadIdx.x) & ~31u; i0 < n_small; i0 += stride)
+        warp_sort_small_cells(A, inst, i0, n_small, lane, s_span[threadIdx.x >> 5]);
     const uint32_t warps = stride >> 5;
     for (uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < n_large; w += warps) {
         const uint2 e = A.cells_large[w];
