@@ -111,7 +111,7 @@ struct fiber_ctx {
     DevBuf d_lut_simple;  // per coarse tile: the LUT takes the binary-search slice lookup
     DevBuf d_lut, d_tasks, d_projected, d_page_table, d_page_meta, d_counts, d_offsets, d_cursors;
     DevBuf d_refs, d_ref_keys, d_active_flags, d_active_list, d_work, d_runs, d_big_cells;
-    DevBuf d_visit_rec, d_visit_task, d_visit_rank, d_task_key, d_task_mat, d_cells_small, d_cells_large;
+    DevBuf d_visit_rec, d_visit_task, d_visit_rank, d_task_key, d_task_mat, d_cells_small, d_cells_mid, d_cells_large;
     DevBuf d_opaque;  // (covered, farthest depth q) per camera fine tile
     DevBuf d_task_proj, d_ref_task;  // k_fine's projected end points per task; each reference's task
     DevBuf d_page_nvis, d_page_vbase, d_page_bucket;  // page-CSR backend
@@ -239,6 +239,7 @@ PrepassArgs prepass_args(fiber_ctx* c) {
     A.task_key = dp<unsigned long long>(c->d_task_key);
     A.task_mat = dp<uint32_t>(c->d_task_mat);
     A.cells_small = dp<uint2>(c->d_cells_small);
+    A.cells_mid = dp<uint2>(c->d_cells_mid);
     A.cells_large = dp<uint2>(c->d_cells_large);
     A.opaque_tiles = dp<uint2>(c->d_opaque);
     A.task_proj = dp<float4>(c->d_task_proj);
@@ -580,7 +581,7 @@ fiber_status fiber_ctx_destroy(fiber_ctx* c) {
                       &c->d_history[0], &c->d_history[1], &c->d_color, &c->d_depth, &c->d_fragments,
                       &c->d_validate, &c->d_host_scene, &c->d_host_depth, &c->d_visit_rec,
                       &c->d_visit_task, &c->d_visit_rank, &c->d_task_key, &c->d_task_mat,
-                      &c->d_cells_small, &c->d_cells_large, &c->d_opaque, &c->d_page_nvis, &c->d_page_vbase,
+                      &c->d_cells_small, &c->d_cells_mid, &c->d_cells_large, &c->d_opaque, &c->d_page_nvis, &c->d_page_vbase,
                       &c->d_page_bucket, &c->d_tel, &c->d_tel_slots, &c->d_dom_page_table, &c->d_dom_pool,
                       &c->d_task_proj, &c->d_ref_task};
     for (DevBuf* b : bufs) release(c, *b);
@@ -892,7 +893,8 @@ fiber_status fiber_frame_begin(fiber_ctx* c, const fiber_froxel_config* cam_cfg,
     ENSURE(c->d_task_mat, task_cap * 4, false);
     // Non-empty cells: at most one per kept reference and one per cell.
     ENSURE(c->d_cells_small, std::min<uint64_t>(ref_cap, page_cap * kPageSize) * sizeof(uint2), false);
-    ENSURE(c->d_cells_large, (ref_cap / 9 + 1) * sizeof(uint2), false);
+    ENSURE(c->d_cells_mid, (ref_cap / 9 + 1) * sizeof(uint2), false);
+    ENSURE(c->d_cells_large, (ref_cap / 33 + 1) * sizeof(uint2), false);
     ENSURE(c->d_opaque, (uint64_t)c->camera_fine_tiles * sizeof(uint2), false);
     ENSURE(c->d_task_proj, task_cap * 2 * sizeof(float4), false);
     ENSURE(c->d_ref_task, ref_cap * 4, false);

@@ -96,11 +96,13 @@ struct FrameCounters {
     uint32_t visit_overflow;      // visit records unused this frame (did not fit, or disabled)
     unsigned long long visits;    // visit records appended by k_visit
     uint32_t small_cells;         // cells of 1..8 references listed for the cell sort
-    uint32_t large_cells;         // cells of more than 8 references listed for the cell sort
+    uint32_t large_cells;         // cells of more than 32 references listed for the cell sort
     uint32_t opaque_bound;        // the opaque fine-tile depths of this frame are written
     uint32_t dom_pages;           // DOM pages requested this frame (sparse residency)
+    uint32_t mid_cells;           // cells of 9..32 references listed for the cell sort
+    uint32_t pad_counters;
 };
-static_assert(sizeof(FrameCounters) == 168, "FrameCounters layout");
+static_assert(sizeof(FrameCounters) == 176, "FrameCounters layout");
 
 // Look-back stages (index into FrameCounters::tile_counter and the status regions).
 enum LookbackStage : uint32_t { kStageFine = 0, kStageAlloc = 1, kStagePrefix = 2, kStageActive = 3, kStageEmit = 4, kStageCount = 5 };

@@ -79,6 +79,7 @@ struct PrepassArgs {
     unsigned long long* task_key;  // [task_capacity] canonical cell-order key of the task's reference
     uint32_t* task_mat;            // [task_capacity] material index of the task's reference
     uint2* cells_small;            // (ref base, count) of cells with 1..8 references
+    uint2* cells_mid;              // (ref base, count) of cells with 9..32 references
     uint2* cells_large;            // (ref base, count) of cells with more than 8
     uint2* opaque_tiles;           // [camera fine tiles] (fully covered, quantised farthest opaque depth)
     float4* task_proj;             // [task_capacity][2] both end points as world_to_screen_raw gave them

@@ -472,6 +472,7 @@ constexpr uint32_t kVisitSlots = 32;  // buffered visits per task; p99 is about 
 // Cell sort sizes: a thread sorts a cell of up to 8 references, a warp one of
 // up to 256 (32 lanes x 8 registers), a block anything longer.
 constexpr uint32_t kThreadSortMax = 8;
+constexpr uint32_t kGroupSortMax = 32;  // 8 lanes x 4 registers: four cells per warp
 constexpr uint32_t kWarpSortMax = 256;
 
 // lut_slices for one end point of a LUT whose 16 entries are all populated,
@@ -1048,25 +1049,27 @@ __global__ void __launch_bounds__(256) k_prefix_pages(const FrameParams* __restr
         const uint4 ca = *reinterpret_cast<const uint4*>(A.counts + g0);
         const uint4 cb = *reinterpret_cast<const uint4*>(A.counts + g0 + 4u);
         const uint32_t c[8] = {ca.x, ca.y, ca.z, ca.w, cb.x, cb.y, cb.z, cb.w};
-        uint32_t e[8], sum = 0u, nsmall = 0u, nlarge = 0u, nz = 0u;
+        uint32_t e[8], sum = 0u, nsmall = 0u, nmid = 0u, nlarge = 0u, nz = 0u;
 #pragma unroll
         for (uint32_t k = 0; k < 8u; ++k) {
             e[k] = sum;
             sum += c[k];
             nsmall += (c[k] >= 1u && c[k] <= kThreadSortMax) ? 1u : 0u;
-            nlarge += c[k] > kThreadSortMax ? 1u : 0u;
+            nmid += (c[k] > kThreadSortMax && c[k] <= kGroupSortMax) ? 1u : 0u;
+            nlarge += c[k] > kGroupSortMax ? 1u : 0u;
             nz |= (c[k] > 0u ? 1u : 0u) << k;
         }
-        // One scan carries the reference count (exclusive per cell) and, packed,
-        // the small / large cell counts for the lists.
-        uint32_t x = sum, y = nsmall | (nlarge << 16);
+        // One scan carries the reference count (exclusive per cell) and, packed
+        // 10 bits each, the small / mid / large cell counts for the lists.
+        const uint32_t mine = nsmall | (nmid << 10) | (nlarge << 20);
+        uint32_t x = sum, y = mine;
 #pragma unroll
         for (uint32_t o = 1; o < 32u; o <<= 1) {
             const uint32_t xa = __shfl_up_sync(0xFFFFFFFFu, x, o), ya = __shfl_up_sync(0xFFFFFFFFu, y, o);
             if (lane >= o) { x += xa; y += ya; }
         }
         const uint32_t total = __shfl_sync(0xFFFFFFFFu, x, 31), both = __shfl_sync(0xFFFFFFFFu, y, 31);
-        const uint32_t lane_base = x - sum, list_base = y - (nsmall | (nlarge << 16));
+        const uint32_t lane_base = x - sum, list_base = y - mine;
 #pragma unroll
         for (uint32_t k = 0; k < 8u; ++k) e[k] += lane_base;
         *reinterpret_cast<uint4*>(A.offsets + g0) = make_uint4(e[0], e[1], e[2], e[3]);
@@ -1094,18 +1097,21 @@ __global__ void __launch_bounds__(256) k_prefix_pages(const FrameParams* __restr
         if (flags != 0u) continue;
         // The page's non-empty cells for k_sort_cells: up to 8 references in the
         // small list, more in the large one, in cell order.
-        uint32_t s_small = 0u, s_large = 0u;
+        uint32_t s_small = 0u, s_mid = 0u, s_large = 0u;
         if (lane == 0u) {
-            const uint32_t ns = both & 0xFFFFu, nl = both >> 16;
+            const uint32_t ns = both & 0x3FFu, nm = (both >> 10) & 0x3FFu, nl = both >> 20;
             s_small = ns ? atomicAdd(&A.counters->small_cells, ns) : 0u;
+            s_mid = nm ? atomicAdd(&A.counters->mid_cells, nm) : 0u;
             s_large = nl ? atomicAdd(&A.counters->large_cells, nl) : 0u;
         }
-        uint32_t ks = __shfl_sync(0xFFFFFFFFu, s_small, 0) + (list_base & 0xFFFFu);
-        uint32_t kl = __shfl_sync(0xFFFFFFFFu, s_large, 0) + (list_base >> 16);
+        uint32_t ks = __shfl_sync(0xFFFFFFFFu, s_small, 0) + (list_base & 0x3FFu);
+        uint32_t km = __shfl_sync(0xFFFFFFFFu, s_mid, 0) + ((list_base >> 10) & 0x3FFu);
+        uint32_t kl = __shfl_sync(0xFFFFFFFFu, s_large, 0) + (list_base >> 20);
 #pragma unroll
         for (uint32_t k = 0; k < 8u; ++k) {
             if (c[k] >= 1u && c[k] <= kThreadSortMax) A.cells_small[ks++] = make_uint2(base + e[k], c[k]);
-            else if (c[k] > kThreadSortMax) A.cells_large[kl++] = make_uint2(base + e[k], c[k]);
+            else if (c[k] > kThreadSortMax && c[k] <= kGroupSortMax) A.cells_mid[km++] = make_uint2(base + e[k], c[k]);
+            else if (c[k] > kGroupSortMax) A.cells_large[kl++] = make_uint2(base + e[k], c[k]);
         }
         // append_active_fine_tile (:2207-2238): each of the page's 16 fine tiles
         // with a non-empty cell that lies on screen. Lanes of one parity hold
@@ -1256,6 +1262,62 @@ __device__ __forceinline__ void warp_sort_cell(const PrepassArgs& A, const Insta
 }
 
 
+// A group of G lanes (G-aligned inside the warp) sorts one cell of up to
+// G x R references: the bitonic network of warp_sort_cell over element
+// e = (lane % G) R + r, shuffles exchanging only inside the group. Groups
+// without a cell (n = 0) take part with padding. Every lane of the warp calls
+// it.
+template <int G, int R>
+__device__ __forceinline__ void group_sort_cell(const PrepassArgs& A, const InstanceView* __restrict__ inst,
+                                                uint32_t base, uint32_t n, int lane) {
+    const int gl = lane & (G - 1);
+    unsigned long long k[R];
+    uint32_t task[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const uint32_t e = (uint32_t)gl * R + r;
+        k[r] = ~0ull;
+        task[r] = 0u;
+        if (e < n) task_entry(A, inst, A.ref_keys[base + e], k[r], task[r]);
+    }
+#pragma unroll
+    for (int size = 2; size <= G * R; size <<= 1) {
+#pragma unroll
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            if (stride >= R) {
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    const int e = gl * R + r;
+                    unsigned long long ok = __shfl_xor_sync(0xFFFFFFFFu, k[r], stride / R);
+                    uint32_t om = __shfl_xor_sync(0xFFFFFFFFu, task[r], stride / R);
+                    const bool up = (e & size) == 0;
+                    const bool lower = (e & stride) == 0;
+                    const bool take_other = lower == up ? (ok < k[r]) : (ok > k[r]);
+                    if (take_other) { k[r] = ok; task[r] = om; }
+                }
+            } else {
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    const int r2 = r ^ stride;
+                    if (r2 > r) {
+                        const int e = gl * R + r;
+                        const bool up = (e & size) == 0;
+                        if (up ? (k[r] > k[r2]) : (k[r] < k[r2])) {
+                            unsigned long long tk = k[r]; k[r] = k[r2]; k[r2] = tk;
+                            uint32_t tt = task[r]; task[r] = task[r2]; task[r2] = tt;
+                        }
+                    }
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const uint32_t e = (uint32_t)gl * R + r;
+        if (e < n) store_entry(A, base + e, k[r], task[r]);
+    }
+}
+
 __device__ __forceinline__ void warp_sort_any(const PrepassArgs& A, const InstanceView* __restrict__ inst,
                                               uint32_t base, uint32_t n, int lane) {
     if (n <= 32u) warp_sort_cell<1>(A, inst, base, n, lane);
@@ -1401,14 +1463,18 @@ __device__ __forceinline__ void convert_big_cell(const PrepassArgs& A, const Ins
 // 32 consecutive small cells at once. k_prefix_pages lists a page's small
 // cells together, in cell order, so their references usually form one span
 // [lo, hi) of the reference array (holes: the page's larger cells). When the
-// span fits kSortSpan, the warp reads it coalesced into shared memory with
-// every entry's gathered key, each lane sorts its cell there (the same
-// network as thread_sort_cell) and the warp writes the span's owned entries
-// back coalesced; otherwise each lane sorts its cell alone.
+// span fits kSortSpan, each lane loads the task index of every 32nd entry of
+// the span (8 independent loads), gathers those tasks' keys and materials (16
+// independent loads), and parks them in shared memory; each lane then sorts
+// its own cell there with the network of thread_sort_cell and the warp writes
+// the span's own entries back coalesced. Otherwise each lane sorts its cell
+// alone.
 constexpr uint32_t kSortSpan = 256;
+constexpr uint32_t kSortPerLane = kSortSpan / 32u;
 struct SortSpanSmem {
     unsigned long long key[kSortSpan];
     uint32_t task[kSortSpan];
+    uint32_t mat[kSortSpan];
     uint8_t own[kSortSpan];
 };
 
@@ -1429,40 +1495,69 @@ __device__ __forceinline__ void warp_sort_small_cells(const PrepassArgs& A, cons
         return;
     }
     const uint32_t span = hi - lo;
-    for (uint32_t j = lane; j < span; j += 32u) sm.own[j] = 0u;
+#pragma unroll
+    for (uint32_t m = 0; m < kSortPerLane; ++m) sm.own[lane + 32u * m] = 0u;
     __syncwarp();
     if (has)
         for (uint32_t r = 0; r < e.y; ++r) sm.own[e.x - lo + r] = 1u;
     __syncwarp();
-    for (uint32_t j = lane; j < span; j += 32u) {
-        if (!sm.own[j]) continue;
-        unsigned long long key;
-        uint32_t task;
-        task_entry(A, inst, A.ref_keys[lo + j], key, task);
-        sm.key[j] = key;
-        sm.task[j] = task;
+    uint32_t tk[kSortPerLane];
+#pragma unroll
+    for (uint32_t m = 0; m < kSortPerLane; ++m) {
+        const uint32_t j = lane + 32u * m;
+        tk[m] = (j < span && sm.own[j]) ? A.ref_keys[lo + j] : kInvalid;
+    }
+    unsigned long long kk[kSortPerLane];
+    uint32_t mt[kSortPerLane];
+#pragma unroll
+    for (uint32_t m = 0; m < kSortPerLane; ++m) {
+        kk[m] = tk[m] != kInvalid ? A.task_key[tk[m]] : ~0ull;
+        mt[m] = tk[m] != kInvalid ? A.task_mat[tk[m]] : 0u;
+    }
+#pragma unroll
+    for (uint32_t m = 0; m < kSortPerLane; ++m) {
+        const uint32_t j = lane + 32u * m;
+        sm.key[j] = kk[m];
+        sm.task[j] = tk[m];
+        sm.mat[j] = mt[m];
     }
     __syncwarp();
     if (has) {
+        // Sort (key, position); the task and material follow their position.
         unsigned long long k[8];
-        uint32_t task[8];
+        uint32_t pos[8];
         const uint32_t b = e.x - lo;
 #pragma unroll
         for (uint32_t r = 0; r < 8u; ++r) {
             k[r] = r < e.y ? sm.key[b + r] : ~0ull;
-            task[r] = r < e.y ? sm.task[b + r] : 0u;
+            pos[r] = b + min(r, e.y - 1u);
         }
-        sort8(k, task);
+        sort8(k, pos);
+        uint32_t t[8], mm[8];
+#pragma unroll
+        for (uint32_t r = 0; r < 8u; ++r) {
+            t[r] = sm.task[pos[r]];
+            mm[r] = sm.mat[pos[r]];
+        }
 #pragma unroll
         for (uint32_t r = 0; r < 8u; ++r)
             if (r < e.y) {
                 sm.key[b + r] = k[r];
-                sm.task[b + r] = task[r];
+                sm.task[b + r] = t[r];
+                sm.mat[b + r] = mm[r];
             }
     }
     __syncwarp();
-    for (uint32_t j = lane; j < span; j += 32u)
-        if (sm.own[j]) store_entry(A, lo + j, sm.key[j], sm.task[j]);
+#pragma unroll
+    for (uint32_t m = 0; m < kSortPerLane; ++m) {
+        const uint32_t j = lane + 32u * m;
+        if (j < span && sm.own[j]) {
+            const unsigned long long key = sm.key[j];
+            A.refs[lo + j] = fiber_fine_seg_ref{(uint32_t)(key >> 32) & 0x7FFFu, (uint32_t)key, sm.mat[j]};
+            A.ref_keys[lo + j] = 0x1FFFFu - (uint32_t)(key >> 47);
+            A.ref_task[lo + j] = sm.task[j];
+        }
+    }
     __syncwarp();
 }
 
@@ -1481,6 +1576,14 @@ __global__ void __launch_bounds__(256, 5) k_sort_cells(const InstanceView* __res
     for (uint32_t i0 = (blockIdx.x * blockDim.x + threadIdx.x) & ~31u; i0 < n_small; i0 += stride)
         warp_sort_small_cells(A, inst, i0, n_small, lane, s_span[threadIdx.x >> 5]);
     const uint32_t warps = stride >> 5;
+    // Cells of 9..32 references: four per warp, eight lanes each.
+    const uint32_t n_mid = *((volatile uint32_t*)&A.counters->mid_cells);
+    for (uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w * 4u < n_mid; w += warps) {
+        const uint32_t ci = w * 4u + (lane >> 3);
+        const uint2 e = ci < n_mid ? A.cells_mid[ci] : make_uint2(0u, 0u);
+        group_sort_cell<8, 4>(A, inst, e.x, e.y, (int)lane);
+    }
+    // Cells of more than 32: a warp per cell.
     for (uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < n_large; w += warps) {
         const uint2 e = A.cells_large[w];
         const uint32_t b = e.x, n = e.y;
