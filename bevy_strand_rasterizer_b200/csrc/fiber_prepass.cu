@@ -1563,9 +1563,10 @@ __device__ __forceinline__ void warp_sort_small_cells(const PrepassArgs& A, cons
 
 // Canonical order inside every cell (projected depth key descending, then
 // instance, then segment), after the fill, over the cell lists k_prefix_pages
-// made: a warp per 32 cells of up to 8 references (nearly all of them), then
-// a warp per larger cell. A cell longer than a warp sort is converted in
-// place by its warp and queued for k_sort_big_cells.
+// made: a warp per 32 cells of up to 8 references (a lane per cell), four
+// cells of 9..32 references per warp (eight lanes each), then a warp per
+// larger cell. A cell longer than a warp sort is converted in place by its
+// warp and queued for k_sort_big_cells.
 __global__ void __launch_bounds__(256, 5) k_sort_cells(const InstanceView* __restrict__ inst, PrepassArgs A) {
     if (frame_failed(A.counters)) return;
     __shared__ SortSpanSmem s_span[8];
