@@ -264,6 +264,19 @@ class StrandRasterizerPlugin:
         self._register()
         return len(self.assets) - 1
 
+    def add_strand_cache(self, cache, material: StrandMaterial | None = None,
+                         world_from_local: np.ndarray | None = None) -> int:
+        """A StrandCache component (src/components.rs:17, loaded by
+        set_cached_strand_geometry, src/plugin.rs:1468-1497): `cache` is a
+        `.strands` path or a parsed strand_cache.StrandCacheFile."""
+        from . import strand_cache
+        if not isinstance(cache, strand_cache.StrandCacheFile):
+            cache = strand_cache.load(str(cache))
+        packed = strand_cache.to_packed(cache)
+        if packed is None:
+            raise abi.FiberError(abi.EINVAL, "strand cache: no strand with two points")
+        return self.add_geometry(packed, material, world_from_local)
+
     def _register(self):
         rows = (abi.StrandInstance * max(1, len(self.assets)))()
         for i, a in enumerate(self.assets):

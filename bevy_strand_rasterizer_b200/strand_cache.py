@@ -116,3 +116,13 @@ def load(path: str) -> StrandCacheFile:
         cache = parse_cache(f.read())
     validate_cache(cache)
     return cache
+
+
+def to_packed(cache: StrandCacheFile):
+    """set_cached_strand_geometry (src/plugin.rs:1468-1497): the cache's vertices
+    times its scale (one binary32 product per component), then
+    pack_indexed_strands over its strands and shared index buffer. None when no
+    strand has two points (the reference warns and skips the entity)."""
+    from .plugin import pack_indexed_strands
+    v = np.ascontiguousarray(cache.vertices, np.float32) * np.float32(cache.scale)
+    return pack_indexed_strands(v, cache.counts, cache.offsets, cache.indices)

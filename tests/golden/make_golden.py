@@ -2,6 +2,10 @@
 
 strand_cache_kat.strands: the 3-vertex, 1-strand binary cache that the
 reference's unit test builds by hand (src/strand_cache.rs:254-281).
+curly_600.strands: a seeded asset in the binary `.strands` layout (600 curly
+strands x 12 points) for the loader-to-GPU parity test: the vertices are
+stored at twice their size with a scale of 0.5 and in a shuffled order that
+the index buffer undoes, so the loader's scale and indexing both matter.
 oracle_tiny.json: SHA-256 digests of the oracle's integer outputs for the
 seeded "tiny" scene; they pin the oracle against unintended drift (the
 reference cannot run here, so these are oracle-produced, not reference-produced).
@@ -45,7 +49,22 @@ def oracle_digests() -> dict:
     return out
 
 
+def curly_asset_bytes() -> bytes:
+    import numpy as np
+    from bevy_strand_rasterizer_b200.scene import scalp_hair
+    from bevy_strand_rasterizer_b200.strand_cache import StrandCacheFile, write_binary_cache
+    sl = scalp_hair(600, 12, 2024, curly=True)
+    pts = np.asarray(sl.vertices, np.float32)[np.asarray(sl.indices)]  # points in strand order
+    perm = np.random.default_rng(2024).permutation(pts.shape[0])     # stored order
+    stored = np.empty_like(pts)
+    stored[perm] = pts * np.float32(2.0)                              # point k lives at row perm[k]
+    cache = StrandCacheFile(1, None, 0.5, stored, np.asarray(sl.strand_counts, np.uint32),
+                            np.asarray(sl.strand_offsets, np.uint32), perm.astype(np.uint32))
+    return write_binary_cache(cache)
+
+
 if __name__ == "__main__":
+    (HERE / "curly_600.strands").write_bytes(curly_asset_bytes())
     (HERE / "strand_cache_kat.strands").write_bytes(kat_bytes())
     (HERE / "oracle_tiny.json").write_text(json.dumps(oracle_digests(), indent=1, sort_keys=True) + "\n")
     print("wrote", HERE / "strand_cache_kat.strands", HERE / "oracle_tiny.json")

@@ -10,7 +10,11 @@ import pytest
 from bevy_strand_rasterizer_b200.dsf import DsfError, INCH_TO_METRE, load_dsf, parse_dsf_polylines
 from bevy_strand_rasterizer_b200.plugin import pack_strands
 
-PIXIE = Path("/root/reference/assets/dForce Pixie Cut_708408.dsf")
+import os
+
+# The reference tree's Pixie Cut asset (assets/dForce Pixie Cut_708408.dsf of the
+# reference project), given by path in FIBER_PIXIE_DSF; the test skips without it.
+PIXIE = Path(os.environ.get("FIBER_PIXIE_DSF", "")) if os.environ.get("FIBER_PIXIE_DSF") else None
 
 
 def _doc(geometries):
@@ -49,7 +53,7 @@ def test_index_cast_and_errors():
         parse_dsf_polylines(_doc([{"vertices": {"values": [[0, 0, 0]]}, "polyline_list": {"values": [[0, 0, 1]]}}]))
 
 
-@pytest.mark.skipif(not PIXIE.exists(), reason="the reference's Pixie Cut asset is not present")
+@pytest.mark.skipif(PIXIE is None or not PIXIE.exists(), reason="FIBER_PIXIE_DSF does not name the Pixie Cut asset")
 def test_pixie_cut_through_the_oracle():
     sl = load_dsf(PIXIE)
     assert sl.vertices.shape == (236136, 3)

@@ -79,3 +79,20 @@ def test_json_cache_and_roundtrip():
     packed = pack_indexed_strands(c.vertices, c.counts, c.offsets, c.indices)
     assert packed.strand_count == 2 and packed.index_count == 5
     assert packed.vertices.shape == (5, 4) and np.all(packed.vertices[:, 3] == 1.0)
+
+
+def test_committed_curly_asset_loads_to_the_seeded_strands():
+    # tests/golden/curly_600.strands (tests/golden/make_golden.py): vertices
+    # stored doubled with scale 0.5 in a shuffled order; the loader's scale and
+    # index buffer give back the seeded strands point for point.
+    from bevy_strand_rasterizer_b200.scene import scalp_hair
+    from bevy_strand_rasterizer_b200.strand_cache import load, to_packed
+    cache = load(str(Path(__file__).parent / "golden" / "curly_600.strands"))
+    assert cache.scale == 0.5 and cache.counts.shape[0] == 600
+    packed = to_packed(cache)
+    sl = scalp_hair(600, 12, 2024, curly=True)
+    want = np.asarray(sl.vertices, np.float32)[np.asarray(sl.indices)]
+    got = packed.vertices[packed.indices][:, :3]
+    assert np.array_equal(got, want)
+    assert np.all(packed.vertices[:, 3] == 1.0)
+    assert packed.meta["count"].tolist() == np.asarray(sl.strand_counts).tolist()
