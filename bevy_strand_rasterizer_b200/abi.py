@@ -110,11 +110,12 @@ class Stats(C.Structure):
 
 # Request server (fiber_server_*).
 SERVER_MAX_LIGHTS = 4
+PRIORITY_ARRIVAL, PRIORITY_COST = 0, 1
 
 
 class ServerConfig(C.Structure):
     _fields_ = [("slots", u32), ("max_width", u32), ("max_height", u32), ("max_lights", u32), ("max_dom", u32),
-                ("priority_levels", u32), ("hbm_budget", C.c_uint64)]
+                ("priority_levels", u32), ("hbm_budget", C.c_uint64), ("priority_order", u32), ("pad", u32)]
 
 
 class ServerScene(C.Structure):

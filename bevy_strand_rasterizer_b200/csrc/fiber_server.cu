@@ -181,6 +181,29 @@ fiber_status render(fiber_server* srv, Slot& slot, const fiber_server_request& r
     return st;
 }
 
+// Predicted cost of a request: segments x frusta + camera pixels + shadow
+// texels (as fiber_ctx_frame_cost), and its priority level under
+// FIBER_PRIORITY_COST: 0 (highest) for the costliest request the server can
+// get (the largest scene at the largest shape), one level lower per halving.
+uint64_t request_cost(const fiber_server* srv, const fiber_server_request& r) {
+    uint64_t c = srv->scene_segments[r.scene] * (1u + r.n_lights) +
+                 (uint64_t)r.camera_cfg.screen_width * r.camera_cfg.screen_height;
+    for (uint32_t l = 0; l < r.n_lights; ++l)
+        c += (uint64_t)r.light_cfgs[l].screen_width * r.light_cfgs[l].screen_height;
+    return std::max<uint64_t>(c, 1u);
+}
+
+uint32_t cost_level(const fiber_server* srv, const fiber_server_request& r) {
+    uint64_t top = 1u;
+    for (uint64_t segs : srv->scene_segments) top = std::max<uint64_t>(top, segs);
+    top = top * (1u + srv->cfg.max_lights) + (uint64_t)srv->cfg.max_width * srv->cfg.max_height +
+          (uint64_t)srv->cfg.max_lights * srv->cfg.max_dom * srv->cfg.max_dom;
+    const uint64_t c = request_cost(srv, r);
+    uint32_t level = 0;
+    while (level + 1u < srv->priorities.size() && (c << (level + 1u)) <= top) ++level;
+    return level;
+}
+
 void worker_main(fiber_server* srv, uint32_t si) {
     cudaSetDevice(srv->device);
     Slot& slot = srv->slots[si];
@@ -193,7 +216,9 @@ void worker_main(fiber_server* srv, uint32_t si) {
             if (srv->queue.empty()) return;
             p = srv->queue.front();
             srv->queue.pop_front();
-            level = std::min<uint32_t>(srv->in_flight, (uint32_t)srv->priorities.size() - 1u);
+            level = srv->cfg.priority_order == FIBER_PRIORITY_COST
+                        ? cost_level(srv, p.req)
+                        : std::min<uint32_t>(srv->in_flight, (uint32_t)srv->priorities.size() - 1u);
             ++srv->in_flight;
         }
         fiber_server_result res{};
@@ -218,7 +243,7 @@ fiber_status fiber_server_create(int device, const fiber_settings* settings, con
                                  fiber_server** out) {
     if (!cfg || !out) return FIBER_EINVAL;
     *out = nullptr;
-    if (cfg->slots > kMaxSlots || cfg->max_width == 0 || cfg->max_height == 0 ||
+    if (cfg->slots > kMaxSlots || cfg->max_width == 0 || cfg->max_height == 0 || cfg->priority_order > 1u ||
         cfg->max_lights > FIBER_SERVER_MAX_LIGHTS || (cfg->max_lights && cfg->max_dom == 0))
         return FIBER_EINVAL;
     if (cudaSetDevice(device) != cudaSuccess) {

@@ -34,10 +34,12 @@ def _host_ptr(buf) -> int:
 class FiberServer:
     def __init__(self, device: int = 0, slots: int = 0, max_width: int = 1920, max_height: int = 1080,
                  max_lights: int = 1, max_dom: int = 2048, hbm_budget: int = 0,
-                 settings: abi.Settings | None = None, priority_levels: int = 0):
+                 settings: abi.Settings | None = None, priority_levels: int = 0,
+                 priority_order: int = abi.PRIORITY_ARRIVAL):
         self.lib = abi.load_library()
         self.srv = C.c_void_p()
-        cfg = abi.ServerConfig(slots, max_width, max_height, max_lights, max_dom, priority_levels, hbm_budget)
+        cfg = abi.ServerConfig(slots, max_width, max_height, max_lights, max_dom, priority_levels, hbm_budget,
+                               priority_order, 0)
         st = settings if settings is not None else abi.default_settings()
         abi.check(self.lib.fiber_server_create(device, C.byref(st), C.byref(cfg), C.byref(self.srv)),
                   "fiber_server_create")

@@ -481,7 +481,14 @@ typedef struct fiber_server_config {
                               admission order (oldest highest): 0 = every level
                               the device offers, 1 = one priority for all   */
     uint64_t hbm_budget;   /* device bytes all slots may hold (0 = no cap)      */
+    uint32_t priority_order; /* FIBER_PRIORITY_ARRIVAL: the oldest frame in flight
+                              highest; FIBER_PRIORITY_COST: the costliest request
+                              (segments x frusta + pixels + shadow texels)
+                              highest, one level lower per halving of cost   */
+    uint32_t pad;
 } fiber_server_config;
+#define FIBER_PRIORITY_ARRIVAL 0u
+#define FIBER_PRIORITY_COST 1u
 
 /* One resident scene: a strand instance in the reference's slab format
  * (pack_strands / pack_indexed_strands, src/plugin.rs:1315-1393), host memory. */

@@ -28,7 +28,7 @@ def test_exports_every_declared_symbol():
 @pytest.mark.parametrize("ctype,size", [
     (abi.DevicePtr, 12), (abi.Aabb, 32), (abi.StrandGeo, 64), (abi.StrandMaterialC, 64),
     (abi.StrandInstance, 160), (abi.FroxelConfigC, 20), (abi.Camera, 80), (abi.Light, 96), (abi.Image, 24),
-    (abi.ServerConfig, 32), (abi.ServerScene, 192), (abi.ServerRequest, 600), (abi.ServerResult, 40),
+    (abi.ServerConfig, 40), (abi.ServerScene, 192), (abi.ServerRequest, 600), (abi.ServerResult, 40),
     (abi.BatchTuning, 16), (abi.FrustumTelemetry, 44), (abi.Telemetry, 864), (abi.Stats, 408),
 ])
 def test_struct_sizes(ctype, size):
