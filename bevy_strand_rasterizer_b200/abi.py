@@ -77,6 +77,13 @@ class Light(C.Structure):
                 ("color", f32 * 4)]
 
 
+class View(C.Structure):
+    """fiber_view: one view of a multi-view frame (fiber_frame_begin_views)."""
+    _fields_ = [("camera_cfg", FroxelConfigC), ("camera", Camera), ("light_cfgs", C.POINTER(FroxelConfigC)),
+                ("lights", C.POINTER(Light)), ("n_lights", u32), ("instance_first", u32), ("instance_count", u32),
+                ("pad", u32)]
+
+
 class Settings(C.Structure):
     _fields_ = [("stochastic_cull_enabled", u32), ("target_strands_per_pixel", f32),
                 ("min_keep_probability", f32), ("shadow_keep_probability", f32),
@@ -187,6 +194,7 @@ class BatchTuning(C.Structure):
 EXPORTS = [
     "fiber_ctx_create", "fiber_ctx_destroy", "fiber_settings_default", "fiber_settings_set",
     "fiber_slab_alloc", "fiber_slab_upload", "fiber_slab_free", "fiber_instance_set", "fiber_frame_begin",
+    "fiber_frame_begin_views",
     "fiber_opaque_depth", "fiber_prepass", "fiber_shadows", "fiber_shading", "fiber_raster", "fiber_composite", "fiber_frame_fused",
     "fiber_render_host", "fiber_stats_get", "fiber_telemetry_get", "fiber_dump", "fiber_output_image", "fiber_span_count", "fiber_span_name",
     "fiber_span_times", "fiber_status_string", "fiber_server_create", "fiber_server_add_scene",
@@ -225,6 +233,7 @@ def load_library(path: Path | str | None = None) -> C.CDLL:
         "fiber_slab_free": (C.c_int, [vp, u32, u32]),
         "fiber_instance_set": (C.c_int, [vp, pp(StrandInstance), u32]),
         "fiber_frame_begin": (C.c_int, [vp, pp(FroxelConfigC), pp(Camera), pp(FroxelConfigC), pp(Light), u32, vp]),
+        "fiber_frame_begin_views": (C.c_int, [vp, pp(View), u32, vp]),
         "fiber_opaque_depth": (C.c_int, [vp, pp(Image), u32, vp]),
         "fiber_prepass": (C.c_int, [vp, vp]),
         "fiber_shadows": (C.c_int, [vp, vp]),

@@ -135,6 +135,14 @@ struct fiber_ctx {
     // Smallest reference capacity of the next frames (the request server
     // raises it after a frame whose references overflowed).
     uint64_t ref_floor = 0;
+    // The frame's views (fiber_frame_begin_views) and the pixels of their
+    // concatenated colour / depth / fragment images.
+    uint32_t n_views = 1;
+    uint64_t out_pixels = 0;
+    // The last fiber_frame_begin's view, for a batch's multi-view frame.
+    fiber_view last_view{};
+    std::vector<fiber_froxel_config> last_light_cfgs;
+    std::vector<fiber_light> last_lights;
     DevBuf d_dom_depth, d_dom_opacity, d_shadow_map, d_atlas, d_history[2];
     DevBuf d_color, d_depth, d_fragments, d_validate, d_host_scene, d_host_depth;
     int hist_cur = 0;
@@ -312,13 +320,13 @@ fiber_status check_launch() {
 fiber_status frame_resets(fiber_ctx* c, cudaStream_t s) {
     const FrameParams& P = c->P;
     const uint64_t table = (uint64_t)P.total_coarse_tiles * kDepthSlices;
-    const uint64_t W = P.width, H = P.height, L = P.L, D = P.dom_size, S = P.shadow_map_size;
+    const uint64_t WH = c->out_pixels, L = P.L, D = P.dom_size, S = P.shadow_map_size;
     FIBER_CUDA(cudaMemsetAsync(c->d_counters.p, 0, sizeof(FrameCounters), s));
     FIBER_CUDA(cudaMemsetAsync(c->d_page_table.p, 0, table * 4, s));
     FIBER_CUDA(cudaMemsetAsync(c->d_active_flags.p, 0, table * 4, s));
-    FIBER_CUDA(cudaMemsetAsync(c->d_color.p, 0, W * H * 8, s));
-    FIBER_CUDA(cudaMemsetAsync(c->d_depth.p, 0, W * H * 4, s));
-    if (P.fragment_counts) FIBER_CUDA(cudaMemsetAsync(c->d_fragments.p, 0, W * H * 4, s));
+    FIBER_CUDA(cudaMemsetAsync(c->d_color.p, 0, WH * 8, s));
+    FIBER_CUDA(cudaMemsetAsync(c->d_depth.p, 0, WH * 4, s));
+    if (P.fragment_counts) FIBER_CUDA(cudaMemsetAsync(c->d_fragments.p, 0, WH * 4, s));
     if (L) {
         if (P.dom_pool_pages) {
             const uint64_t ppx = P.dom_pages_x;
@@ -444,6 +452,7 @@ uint32_t fmt_bytes(uint32_t fmt) {
 // `samples` floats per pixel, rows 4-byte aligned and wide enough).
 fiber_status opaque_source(const fiber_ctx* c, const fiber_image* im, uint32_t samples, OpaqueSource& o) {
     if (!im || !im->ptr || im->format != FIBER_FMT_R32F || (samples != 1u && samples != 4u)) return FIBER_EINVAL;
+    if (c->n_views != 1u) return FIBER_EINVAL;  // the opaque-scene cull is one camera's
     if (im->width != c->P.width || im->height != c->P.height) return FIBER_EINVAL;
     const uint64_t row = (uint64_t)im->width * samples * 4u;
     const uint64_t pitch = im->pitch ? im->pitch : row;
@@ -458,6 +467,7 @@ fiber_status run_composite(fiber_ctx* c, const fiber_image* scene_color, const f
                            fiber_image* out, cudaStream_t s) {
     record(c, 12, s);
     if (!scene_color || !out || !scene_color->ptr || !out->ptr) return FIBER_EINVAL;
+    if (c->n_views != 1u) return FIBER_EINVAL;  // a multi-view frame has no single scene image
     if (scene_color->width != c->P.width || scene_color->height != c->P.height || out->width != c->P.width ||
         out->height != c->P.height)
         return FIBER_EINVAL;
@@ -723,37 +733,72 @@ fiber_status fiber_instance_set(fiber_ctx* c, const fiber_strand_instance* rows,
     return FIBER_OK;
 }
 
-fiber_status fiber_frame_begin(fiber_ctx* c, const fiber_froxel_config* cam_cfg, const fiber_camera* cam,
-                               const fiber_froxel_config* light_cfgs, const fiber_light* lights, uint32_t n_lights,
-                               void* stream_) {
-    if (!c || !cam_cfg || !cam || (n_lights && (!light_cfgs || !lights))) return FIBER_EINVAL;
-    if (1u + n_lights > kMaxFrusta) return FIBER_EINVAL;
-    cudaStream_t s = (cudaStream_t)stream_;
-    cudaSetDevice(c->device);
+// The frame tables of one frame of nv views (use_prepass_buffers,
+// src/plugin.rs:264-1209): frusta, clip matrices, capacities, buffers, resets.
+// A frame of fiber_frame_begin is one view over every instance.
+static fiber_status frame_begin_views(fiber_ctx* c, const fiber_view* views, uint32_t nv, cudaStream_t s) {
+    if (!c || !views || nv == 0u || nv > kMaxViews) return FIBER_EINVAL;
+    const fiber_settings& st = c->settings;
+    const uint32_t I = (uint32_t)c->views.size();
     auto cfg_ok = [](const fiber_froxel_config& g) {
         return g.screen_width && g.screen_height && g.froxel_size_x && g.froxel_size_y && g.screen_width <= 16384u &&
                g.screen_height <= 16384u;
     };
-    if (!cfg_ok(*cam_cfg)) return FIBER_EINVAL;
-    for (uint32_t l = 0; l < n_lights; ++l) {
-        if (!cfg_ok(light_cfgs[l])) return FIBER_EINVAL;
-        // Dense deep-opacity layers: every light map is square and the same size.
-        if (light_cfgs[l].screen_width != light_cfgs[l].screen_height ||
-            light_cfgs[l].screen_width != light_cfgs[0].screen_width)
-            return FIBER_EINVAL;
+    uint32_t n_frusta = 0, n_lights = 0, dmax = 0, inst_next = 0;
+    for (uint32_t v = 0; v < nv; ++v) {
+        const fiber_view& w = views[v];
+        if (!cfg_ok(w.camera_cfg) || (w.n_lights && (!w.light_cfgs || !w.lights))) return FIBER_EINVAL;
+        // The views' instances follow one another in the instance table, and
+        // every view of several has strands (its frusta then have tasks' bases).
+        if (w.instance_first != inst_next || w.instance_first + w.instance_count > I) return FIBER_EINVAL;
+        if (nv > 1u) {
+            uint32_t ns = 0;
+            for (uint32_t i = w.instance_first; i < w.instance_first + w.instance_count; ++i)
+                ns += c->views[i].strand_count;
+            if (ns == 0u) return FIBER_EINVAL;
+        }
+        inst_next += w.instance_count;
+        for (uint32_t l = 0; l < w.n_lights; ++l) {
+            const fiber_froxel_config& g = w.light_cfgs[l];
+            // Dense deep-opacity layers are square; one view's maps are one size.
+            if (!cfg_ok(g) || g.screen_width != g.screen_height || g.screen_width != w.light_cfgs[0].screen_width)
+                return FIBER_EINVAL;
+            dmax = std::max(dmax, g.screen_width);
+        }
+        n_frusta += 1u + w.n_lights;
+        n_lights += w.n_lights;
     }
-    const fiber_settings& st = c->settings;
+    if (inst_next != I && nv > 1u) return FIBER_EINVAL;
+    if (nv == 1u ? n_frusta > FIBER_MAX_FRUSTA : n_frusta > kMaxFrusta) return FIBER_EINVAL;
+    // Several views: dense layers of the largest map, no per-frustum telemetry
+    // beyond its 16 frusta, no opaque-scene cull (a single camera's).
+    if (nv > 1u && (st.dom_page_pool != 0u || (st.telemetry_enabled && n_frusta > FIBER_TELEMETRY_MAX_FRUSTA)))
+        return FIBER_EINVAL;
+    cudaSetDevice(c->device);
     FrameParams& P = c->P;
     std::memset(&P, 0, sizeof(P));
     P.lb_spin_limit = c->stall_limit;
     P.lb_stall_stage = c->stall_stage;
     P.lb_stall_tile = c->stall_tile;
     c->stall_stage = c->stall_tile = c->stall_limit = 0;
-    // Frustum table (src/plugin.rs:386-482): camera first, then lights.
+    for (uint32_t i = 0; i < I; ++i) c->views[i].view = 0u;
+    for (uint32_t v = 0; v < nv && nv > 1u; ++v)
+        for (uint32_t i = views[v].instance_first; i < views[v].instance_first + views[v].instance_count; ++i)
+            c->views[i].view = v;
+    // Frustum table (src/plugin.rs:386-482): the cameras first (frustum v is
+    // view v's camera), then each view's lights in order.
     c->frusta.clear();
-    uint32_t bucket = 0, coarse = 0, fine = 0, cam_tiles = 0;
-    for (uint32_t f = 0; f < 1u + n_lights; ++f) {
-        const fiber_froxel_config& g = f == 0 ? *cam_cfg : light_cfgs[f - 1];
+    uint32_t bucket = 0, coarse = 0, fine = 0, cam_tiles = 0, light = 0;
+    uint64_t out_pixels = 0;
+    for (uint32_t f = 0; f < n_frusta; ++f) {
+        const bool cam = f < nv;
+        uint32_t v = f, l = 0;  // view, light index inside the view
+        if (!cam) {
+            uint32_t k = f - nv;
+            for (v = 0; k >= views[v].n_lights; ++v) k -= views[v].n_lights;
+            l = k;
+        }
+        const fiber_froxel_config& g = cam ? views[v].camera_cfg : views[v].light_cfgs[l];
         uint32_t tx, ty;
         cfg_tiles(g, tx, ty);
         uint32_t ctx_ = std::max(1u, (tx + 3u) / 4u), cty = std::max(1u, (ty + 3u) / 4u);
@@ -765,7 +810,7 @@ fiber_status fiber_frame_begin(fiber_ctx* c, const fiber_froxel_config* cam_cfg,
         d.depth_slices = g.depth_slices;
         d.bucket_base = bucket;
         d.bucket_count = tx * ty * g.depth_slices;
-        d.kind = f == 0 ? 0u : 1u;
+        d.kind = cam ? 0u : 1u;
         d.coarse_depth_tile_base = coarse;
         d.coarse_depth_tile_count = ctx_ * cty;
         d.coarse_tiles_x = ctx_;
@@ -776,30 +821,58 @@ fiber_status fiber_frame_begin(fiber_ctx* c, const fiber_froxel_config* cam_cfg,
         bucket += d.bucket_count;
         coarse += d.coarse_depth_tile_count;
         fine += tx * ty;
-        if (f == 0) {
-            cam_tiles = coarse;
-            c->camera_fine_tiles = tx * ty;
-        }
+        if (f == 0) c->camera_fine_tiles = tx * ty;
+        if (f + 1u == nv) cam_tiles = coarse;
         P.frusta[f] = d;
-        std::memcpy(P.clip[f], f == 0 ? cam->clip_from_world : lights[f - 1].clip_from_world, 64);
+        P.fview[f] = v;
+        P.flayer[f] = kInvalid;
+        if (cam) {
+            std::memcpy(P.clip[f], views[v].camera.clip_from_world, 64);
+            P.out_base[f] = (uint32_t)out_pixels;
+            out_pixels += (uint64_t)g.screen_width * g.screen_height;
+        } else {
+            const fiber_light& lt = views[v].lights[l];
+            std::memcpy(P.clip[f], lt.clip_from_world, 64);
+            std::memcpy(P.light_dir[light], lt.direction_to_light, 12);
+            std::memcpy(P.light_color[light], lt.color, 16);
+            P.flayer[f] = light;
+            P.layer_frustum[light] = f;
+            ++light;
+        }
     }
-    for (uint32_t l = 0; l < n_lights; ++l) {
-        std::memcpy(P.light_dir[l], lights[l].direction_to_light, 12);
-        std::memcpy(P.light_color[l], lights[l].color, 16);
+    if (out_pixels >= 0xFFFFFFFFull) return FIBER_EINVAL;
+    c->out_pixels = out_pixels;
+    c->n_views = nv;
+    for (uint32_t v = 0, l0 = 0; v < nv; ++v) {
+        P.view_layer0[v] = l0;
+        P.view_layers[v] = views[v].n_lights;
+        l0 += views[v].n_lights;
+        std::memcpy(P.view_cam_pos[v], views[v].camera.world_position, 12);
+        const uint32_t i0 = nv > 1u ? views[v].instance_first : 0u;
+        const uint32_t ni = nv > 1u ? views[v].instance_count : I;
+        P.view_inst0[v] = i0;
+        P.view_strand0[v] = ni && i0 < I ? c->views[i0].strand_base : c->total_strand_count;
+        uint32_t ns = 0;
+        for (uint32_t i = i0; i < i0 + ni; ++i) ns += c->views[i].strand_count;
+        P.view_strands[v] = ns;
     }
-    std::memcpy(P.camera_pos, cam->world_position, 12);
+    P.fine_tile_base[0] = 0u;
+    for (uint32_t f = 0; f < n_frusta; ++f)
+        P.fine_tile_base[f + 1] =
+            P.fine_tile_base[f] + (P.view_strands[P.fview[f]] + kFineStrandsPerTile - 1u) / kFineStrandsPerTile;
+    P.n_views = nv;
+    std::memcpy(P.camera_pos, views[0].camera.world_position, 12);
     std::memcpy(P.ambient, st.ambient_color, 16);
-    const uint32_t I = (uint32_t)c->views.size();
-    P.F = 1u + n_lights;
+    P.F = n_frusta;
     P.I = I;
     P.L = n_lights;
     P.K = st.dom_slices;
     P.total_coarse_tiles = coarse;
     P.total_strands = c->total_strand_count;
     P.max_strands = c->max_strand_count;
-    P.camera_frustum_end = 1u;
+    P.camera_frustum_end = nv;
     P.camera_tile_end = cam_tiles;
-    P.dom_size = n_lights ? light_cfgs[0].screen_width : 0u;
+    P.dom_size = dmax;
     P.shadow_map_size = n_lights ? (st.shadow_map_size ? st.shadow_map_size : P.dom_size) : 0u;
     P.dom_pool_pages = n_lights ? st.dom_page_pool : 0u;
     P.dom_pages_x = (P.dom_size + kDomPage - 1u) / kDomPage;
@@ -810,23 +883,37 @@ fiber_status fiber_frame_begin(fiber_ctx* c, const fiber_froxel_config* cam_cfg,
     // Capacities (src/plugin.rs:483-576): prepass = next_pow2(strands) >= 2048,
     // binning = next_pow2(next_pow2(segments) >= prepass, x frusta), refs =
     // next_pow2(factor x binning). Pages and work items are sized so that only
-    // the reference list can overflow.
+    // the reference list can overflow. Several views: binning =
+    // next_pow2(sum over views of segments x the view's frusta), as each view's
+    // strands meet its own frusta only.
     auto next_pow2 = [](uint64_t x) {
         uint64_t p = 1;
         while (p < x) p <<= 1;
         return p;
     };
     const uint64_t table = (uint64_t)coarse * kDepthSlices;
-    const uint64_t prepass_cap = std::max<uint64_t>(next_pow2(c->total_strands), 2048);
-    const uint64_t base_binning = std::max<uint64_t>(next_pow2(c->total_segments), prepass_cap);
-    const uint64_t task_cap = std::max<uint64_t>(next_pow2(base_binning * P.F), base_binning);
+    uint64_t task_cap = 0;
+    if (nv == 1u) {
+        const uint64_t prepass_cap = std::max<uint64_t>(next_pow2(c->total_strands), 2048);
+        const uint64_t base_binning = std::max<uint64_t>(next_pow2(c->total_segments), prepass_cap);
+        task_cap = std::max<uint64_t>(next_pow2(base_binning * P.F), base_binning);
+    } else {
+        uint64_t sum = 0;
+        for (uint32_t v = 0; v < nv; ++v) {
+            uint64_t segs = 0;
+            for (uint32_t i = views[v].instance_first; i < views[v].instance_first + views[v].instance_count; ++i)
+                segs += c->inst_segments[i];
+            sum += segs * (1u + views[v].n_lights);
+        }
+        task_cap = std::max<uint64_t>(next_pow2(sum), 2048);
+    }
     const uint64_t page_cap = std::max<uint64_t>(1, table / st.page_capacity_divisor);
     const uint64_t ref_cap = std::max<uint64_t>(
         std::max<uint64_t>(next_pow2(task_cap * st.ref_capacity_factor), std::max<uint64_t>(task_cap, 1024)),
         next_pow2(c->ref_floor));
     const uint64_t fine_tiles = table;  // coarse tiles x 16 fine tiles
     const uint64_t work_cap = std::max<uint64_t>(1, std::min<uint64_t>(ref_cap, 256ull * fine_tiles));
-    if (ref_cap >= 0xFFFFFFFFull || work_cap >= 0xFFFFFFFFull) return FIBER_ENOMEM;
+    if (task_cap >= 0xFFFFFFFFull || ref_cap >= 0xFFFFFFFFull || work_cap >= 0xFFFFFFFFull) return FIBER_ENOMEM;
     P.task_capacity = (uint32_t)task_cap;
     P.page_capacity = (uint32_t)page_cap;
     P.ref_capacity = (uint32_t)ref_cap;
@@ -837,10 +924,10 @@ fiber_status fiber_frame_begin(fiber_ctx* c, const fiber_froxel_config* cam_cfg,
     P.shadow_keep_probability = st.shadow_keep_probability;
     P.history_valid = st.history_enabled ? 1u : 0u;
     P.fragment_counts = st.fragment_counts_enabled;
-    P.width = cam_cfg->screen_width;
-    P.height = cam_cfg->screen_height;
+    P.width = views[0].camera_cfg.screen_width;
+    P.height = views[0].camera_cfg.screen_height;
     // Look-back status regions.
-    uint64_t fine_tiles_lb = (uint64_t)P.F * ((P.total_strands + kFineStrandsPerTile - 1u) / kFineStrandsPerTile);
+    uint64_t fine_tiles_lb = P.fine_tile_base[P.F];
     uint64_t lb_sizes[kStageCount] = {fine_tiles_lb + 1, table / 1024 + 2, page_cap + 1, table / 1024 + 2,
                                       fine_tiles + 1};
     uint64_t lb_total = 0;
@@ -848,7 +935,7 @@ fiber_status fiber_frame_begin(fiber_ctx* c, const fiber_froxel_config* cam_cfg,
         c->lb_offset[i] = (uint32_t)lb_total;
         lb_total += lb_sizes[i];
     }
-    const uint64_t W = P.width, H = P.height, L = n_lights, D = P.dom_size, S = P.shadow_map_size, K = P.K;
+    const uint64_t L = n_lights, D = P.dom_size, S = P.shadow_map_size, K = P.K;
     const uint64_t FI = (uint64_t)I * P.F;
     fiber_status e = FIBER_OK;
 #define ENSURE(buf, bytes, zero)                     \
@@ -927,9 +1014,9 @@ fiber_status fiber_frame_begin(fiber_ctx* c, const fiber_froxel_config* cam_cfg,
         cudaMemsetAsync(c->d_history[1].p, 0, c->d_history[1].bytes, s);
         c->hist_cur = 0;
     }
-    ENSURE(c->d_color, W * H * 8, false);
-    ENSURE(c->d_depth, W * H * 4, false);
-    ENSURE(c->d_fragments, W * H * 4, false);
+    ENSURE(c->d_color, out_pixels * 8, false);
+    ENSURE(c->d_depth, out_pixels * 4, false);
+    ENSURE(c->d_fragments, out_pixels * 4, false);
 #undef ENSURE
     c->epoch = (c->epoch + 1u) & 0x3FFFFFFFu;
     if (c->epoch_dirty) c->epoch = 0u;  // a batch graph moved the device epoch on
@@ -949,6 +1036,33 @@ fiber_status fiber_frame_begin(fiber_ctx* c, const fiber_froxel_config* cam_cfg,
     c->frame_ready = true;
     c->opaque_frame = false;
     return FIBER_OK;
+}
+
+fiber_status fiber_frame_begin(fiber_ctx* c, const fiber_froxel_config* cam_cfg, const fiber_camera* cam,
+                               const fiber_froxel_config* light_cfgs, const fiber_light* lights, uint32_t n_lights,
+                               void* stream) {
+    if (!c || !cam_cfg || !cam || (n_lights && (!light_cfgs || !lights))) return FIBER_EINVAL;
+    fiber_view v{};
+    v.camera_cfg = *cam_cfg;
+    v.camera = *cam;
+    v.light_cfgs = light_cfgs;
+    v.lights = lights;
+    v.n_lights = n_lights;
+    v.instance_first = 0u;
+    v.instance_count = (uint32_t)c->views.size();
+    const fiber_status st = frame_begin_views(c, &v, 1u, (cudaStream_t)stream);
+    if (st == FIBER_OK) {
+        // Kept for a batch that renders this context's view inside a
+        // multi-view frame.
+        c->last_view = v;
+        c->last_light_cfgs.assign(light_cfgs, light_cfgs + n_lights);
+        c->last_lights.assign(lights, lights + n_lights);
+    }
+    return st;
+}
+
+fiber_status fiber_frame_begin_views(fiber_ctx* c, const fiber_view* views, uint32_t n_views, void* stream) {
+    return frame_begin_views(c, views, n_views, (cudaStream_t)stream);
 }
 
 fiber_status fiber_opaque_depth(fiber_ctx* c, const fiber_image* depth, uint32_t samples, void* stream) {
@@ -1050,7 +1164,7 @@ fiber_status fiber_frame_fused(fiber_ctx* c, const fiber_image* scene_color, con
                                     composite ? pitch_of(scene_color) : 0u,
                                     composite ? pitch_of(out) : 0u,
                                     scene_depth ? pitch_of(scene_depth) : 0u,
-                                    ((uint64_t)c->P.width << 32) | c->P.height,
+                                    ((uint64_t)c->P.width << 32) | c->P.height ^ (c->out_pixels << 1),
                                     ((uint64_t)c->P.I << 32) | c->P.total_coarse_tiles,
                                     ((uint64_t)c->P.K << 32) | c->P.L};
     bool reuse = c->graph && std::memcmp(key, c->graph_key, sizeof(key)) == 0;
@@ -1089,6 +1203,7 @@ fiber_status fiber_render_host(fiber_ctx* c, const void* scene_host, const float
                                void* stream_) {
     if (!c || !scene_host || !out_host) return FIBER_EINVAL;
     if (!c->frame_ready) return FIBER_ENOTREADY;
+    if (c->n_views != 1u) return FIBER_EINVAL;
     cudaSetDevice(c->device);
     cudaStream_t s = (cudaStream_t)stream_;
     const uint64_t W = c->P.width, H = c->P.height;
@@ -1221,7 +1336,7 @@ void fiber_ctx_shape_key(const fiber_ctx* c, uint64_t key[kFrameShapeWords]) {
     key[0] = c->buffer_generation;
     key[1] = ((uint64_t)P.I << 32) | P.total_coarse_tiles;
     key[2] = ((uint64_t)P.K << 32) | P.L;
-    key[3] = ((uint64_t)P.width << 32) | P.height;
+    key[3] = (((uint64_t)P.width << 32) | P.height) ^ (c->out_pixels << 1) ^ ((uint64_t)P.F << 56);
     key[4] = ((uint64_t)P.dom_size << 32) | P.shadow_map_size;
     key[5] = ((uint64_t)P.fragment_counts << 32) | (c->frame_ready ? 1u : 0u);
 }
@@ -1232,7 +1347,7 @@ void fiber_ctx_mark_replayed(fiber_ctx* c, cudaStream_t s) {
 }
 
 uint64_t fiber_ctx_frame_cost(const fiber_ctx* c) {
-    return c->total_segments * (uint64_t)c->P.F + (uint64_t)c->P.width * c->P.height +
+    return c->total_segments * (uint64_t)c->P.F + c->out_pixels +
            (uint64_t)c->P.L * c->P.dom_size * c->P.dom_size;
 }
 
@@ -1245,6 +1360,7 @@ void fiber_ctx_set_side_stream(fiber_ctx* c, cudaStream_t side) {
 fiber_status fiber_ctx_render_host_nodes(fiber_ctx* c, const void* scene_host, void* out_host, cudaStream_t s) {
     if (!c || !scene_host || !out_host) return FIBER_EINVAL;
     if (!c->frame_ready) return FIBER_ENOTREADY;
+    if (c->n_views != 1u) return FIBER_EINVAL;
     const uint64_t W = c->P.width, H = c->P.height;
     fiber_status e = ensure(c, c->d_host_scene, W * H * 8, false);
     if (e != FIBER_OK) return e;
@@ -1377,7 +1493,7 @@ fiber_status fiber_dump(fiber_ctx* c, uint32_t what, void* host, uint64_t capaci
     FIBER_CUDA(cudaMemcpy(&h, c->d_counters.p, sizeof(h), cudaMemcpyDeviceToHost));
     const FrameParams& P = c->P;
     const uint64_t table = (uint64_t)P.total_coarse_tiles * kDepthSlices;
-    const uint64_t W = P.width, H = P.height, L = P.L, D = P.dom_size, S = P.shadow_map_size, K = P.K;
+    const uint64_t L = P.L, D = P.dom_size, S = P.shadow_map_size, K = P.K;
     const void* src = nullptr;
     uint64_t bytes = 0;
     std::vector<uint32_t> tmp;
@@ -1439,9 +1555,9 @@ fiber_status fiber_dump(fiber_ctx* c, uint32_t what, void* host, uint64_t capaci
         case FIBER_DUMP_SHADOW_MAP: src = c->d_shadow_map.p; bytes = L * S * S * 4; break;
         case FIBER_DUMP_ATLAS: src = c->d_atlas.p; bytes = (uint64_t)P.I * P.atlas_cap * 8; break;
         case FIBER_DUMP_HISTORY: src = c->d_history[c->hist_cur].p; bytes = (uint64_t)P.I * P.atlas_cap * 4; break;
-        case FIBER_DUMP_COLOR: src = c->d_color.p; bytes = W * H * 8; break;
-        case FIBER_DUMP_DEPTH: src = c->d_depth.p; bytes = W * H * 4; break;
-        case FIBER_DUMP_FRAGMENTS: src = c->d_fragments.p; bytes = W * H * 4; break;
+        case FIBER_DUMP_COLOR: src = c->d_color.p; bytes = c->out_pixels * 8; break;
+        case FIBER_DUMP_DEPTH: src = c->d_depth.p; bytes = c->out_pixels * 4; break;
+        case FIBER_DUMP_FRAGMENTS: src = c->d_fragments.p; bytes = c->out_pixels * 4; break;
         case FIBER_DUMP_OPAQUE_TILES:
             // The reference clears the tiles when no opaque depth is bound.
             bytes = (uint64_t)c->camera_fine_tiles * sizeof(uint2);

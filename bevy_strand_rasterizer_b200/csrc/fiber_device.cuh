@@ -21,7 +21,8 @@ constexpr uint32_t kPageSize = 256;        // COARSE_COUNT_PAGE_SIZE (src/plugin
 constexpr uint32_t kDepthQuantMax = 16777215u;
 constexpr uint32_t kInvalid = 0xFFFFFFFFu;
 constexpr uint32_t kMarked = 0xFFFFFFFEu;  // MARKED_COUNT_PAGE (strand_prepass.wgsl:69)
-constexpr uint32_t kMaxFrusta = 16;
+constexpr uint32_t kMaxFrusta = 128;  // frusta of a frame (a multi-view frame: every view's camera and lights)
+constexpr uint32_t kMaxViews = 64;    // views of a multi-view frame
 constexpr uint32_t kPixelSlots = 64;       // strand_rasterizer.wgsl:309,839
 // Strands per look-back tile of the fine prepass (k_fine).
 constexpr uint32_t kFineStrandsPerTile = 64;
@@ -41,7 +42,7 @@ struct InstanceView {
     uint32_t strand_count;       // min(meta count, geo.strand_count)
     uint32_t strand_base;        // prefix of strand_count over instances
     uint32_t valid;              // all slab pointers resolved
-    uint32_t pad;
+    uint32_t view;               // view of a multi-view frame the instance belongs to (0 otherwise)
     fiber_aabb aabb;
     float world_from_local[16];
 };
@@ -77,6 +78,18 @@ struct FrameParams {
     uint32_t lb_spin_limit;       // polls before a look-back wait gives up
     uint32_t lb_stall_stage;      // 1 + look-back stage with a tile that never publishes (0: none)
     uint32_t lb_stall_tile;       // that tile (fiber_debug_stall_lookback; one frame only)
+    // Views (a frame of fiber_frame_begin is one view). Frusta: every view's
+    // camera first (frustum v is view v's camera), then the lights view by view.
+    uint32_t n_views;
+    uint32_t fview[kMaxFrusta];          // view of each frustum
+    uint32_t flayer[kMaxFrusta];         // DOM layer of a light frustum, kInvalid otherwise
+    uint32_t layer_frustum[kMaxFrusta];  // frustum of each DOM layer
+    uint32_t out_base[kMaxFrusta];       // first pixel of a camera's colour / depth / fragment image
+    uint32_t fine_tile_base[kMaxFrusta + 1];  // k_fine's tiles of each frustum (prefix)
+    uint32_t view_strand0[kMaxViews], view_strands[kMaxViews];  // a view's strands (global strand indices)
+    uint32_t view_layer0[kMaxViews], view_layers[kMaxViews];    // a view's lights (DOM layers, light indices)
+    float view_cam_pos[kMaxViews][4];    // a view's camera position
+    uint32_t view_inst0[kMaxViews];      // a view's first instance (the keep hash takes view-local ids)
 };
 
 // Device counters of one frame (zeroed at frame start).
@@ -102,7 +115,7 @@ struct FrameCounters {
     uint32_t mid_cells;           // cells of 9..32 references listed for the cell sort
     uint32_t pad_counters;
 };
-static_assert(sizeof(FrameCounters) == 176, "FrameCounters layout");
+static_assert(sizeof(FrameCounters) == 176 + 4 * (kMaxFrusta - 16), "FrameCounters layout");
 
 // Look-back stages (index into FrameCounters::tile_counter and the status regions).
 enum LookbackStage : uint32_t { kStageFine = 0, kStageAlloc = 1, kStagePrefix = 2, kStageActive = 3, kStageEmit = 4, kStageCount = 5 };
@@ -253,19 +266,22 @@ __device__ __forceinline__ float div_by(float v, uint32_t n) {
     return v / u2f(n);
 }
 
+// Frustum of a coarse tile: frusta own consecutive, increasing tile ranges.
 __device__ __forceinline__ uint32_t frustum_for_tile(const FrameParams& P, uint32_t tile) {
-    for (uint32_t f = 0; f < P.F; ++f) {
-        const fiber_frustum_desc& d = P.frusta[f];
-        if (tile >= d.coarse_depth_tile_base && tile < d.coarse_depth_tile_base + d.coarse_depth_tile_count) return f;
+    if (P.F == 0u) return kInvalid;
+    uint32_t lo = 0, hi = P.F;  // last frustum whose range starts at or before tile
+    while (hi - lo > 1u) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (P.frusta[mid].coarse_depth_tile_base <= tile) lo = mid; else hi = mid;
     }
-    return kInvalid;
+    const fiber_frustum_desc& d = P.frusta[lo];
+    return tile >= d.coarse_depth_tile_base && tile < d.coarse_depth_tile_base + d.coarse_depth_tile_count ? lo
+                                                                                                          : kInvalid;
 }
+// DOM layer of a light frustum (the count of light frusta before it), kInvalid
+// for a camera or beyond the frame's lights.
 __device__ __forceinline__ uint32_t light_layer(const FrameParams& P, uint32_t f) {
-    if (f >= P.F || P.frusta[f].kind != 1u) return kInvalid;
-    uint32_t layer = 0;
-    for (uint32_t i = 0; i < f; ++i)
-        if (P.frusta[i].kind == 1u) ++layer;
-    return layer >= P.L ? kInvalid : layer;
+    return f < P.F ? P.flayer[f] : kInvalid;
 }
 
 // ---------------------------------------------------------------------------

@@ -111,7 +111,8 @@ __global__ void k_broad(const FrameParams* __restrict__ Pp, const InstanceView* 
             float k = 0.0f;
             uint32_t slot = i * P.F + f;
             A.range_valid[slot] = 0u;
-            if (d.kind <= 1u) {
+            // A frustum of another view of a multi-view frame does not see it.
+            if (d.kind <= 1u && P.fview[f] == in.view) {
                 // emit_coarse_asset_range_for_aabb (strand_prepass.wgsl:575-682)
                 bool vis = false;
                 float vw = u2f(d.screen_width), vh = u2f(d.screen_height);
@@ -350,9 +351,9 @@ struct FineStrand {
 };
 
 __device__ __forceinline__ FineStrand fine_strand(const FrameParams& P, const InstanceView* __restrict__ inst,
-                                                  const PrepassArgs& A, uint32_t f, uint32_t g) {
+                                                  const PrepassArgs& A, uint32_t f, uint32_t g, uint32_t g_end) {
     FineStrand r{0u, 0u, 0u, 0u, 0u};
-    if (g >= P.total_strands) return r;
+    if (g >= g_end) return r;
     uint32_t lo = 0, hi = P.I;  // last instance with strand_base <= g
     while (hi - lo > 1u) {
         uint32_t mid = (lo + hi) >> 1;
@@ -362,8 +363,12 @@ __device__ __forceinline__ FineStrand fine_strand(const FrameParams& P, const In
     r.s = g - inst[lo].strand_base;
     const InstanceView& in = inst[lo];
     const fiber_frustum_desc& d = P.frusta[f];
-    const float h = hash_to_unit_float(wang_hash((lo * 16777619u) ^ r.s));
-    bool ok = in.valid && A.inst_visible[lo] != 0u && r.s < in.strand_count && !(h > A.inst_keep[lo]);
+    // The keep hash takes the instance's id inside its view, so a view keeps
+    // the same strands in a multi-view frame as alone (one view: the id).
+    const uint32_t local_i = lo - P.view_inst0[P.fview[f]];
+    const float h = hash_to_unit_float(wang_hash((local_i * 16777619u) ^ r.s));
+    bool ok = in.valid && in.view == P.fview[f] && A.inst_visible[lo] != 0u && r.s < in.strand_count &&
+              !(h > A.inst_keep[lo]);
     ok = ok && d.kind <= 1u && r.s < in.n_meta;
     if (ok) {
         const fiber_strand_meta m = in.meta[r.s];
@@ -384,19 +389,27 @@ __global__ void __launch_bounds__(kFineThreads, 4) k_fine(const FrameParams* __r
     __shared__ uint32_t s_warp_count[kFineWarps];
     __shared__ uint32_t s_base;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const uint32_t tiles_per_f = ceil_div(P.total_strands, kFineStrandsPerTile);
-    const uint32_t n_tiles = tiles_per_f * P.F;
+    // Each frustum's tiles cover its view's strands (every strand of a
+    // single-view frame): fine_tile_base is their prefix over frusta.
+    const uint32_t n_tiles = P.fine_tile_base[P.F];
     for (;;) {
         if (threadIdx.x == 0) s_tile = atomicAdd(A.tile_counter, 1u);
         __syncthreads();
         const uint32_t tile = s_tile;
         if (tile >= n_tiles) break;
-        const uint32_t f = tile / tiles_per_f;
-        const uint32_t g0 = (tile % tiles_per_f) * kFineStrandsPerTile + (uint32_t)warp * kFineStrandsPerWarp;
+        uint32_t f = 0, fhi = P.F;  // last frustum whose tiles start at or before tile
+        while (fhi - f > 1u) {
+            const uint32_t mid = (f + fhi) >> 1;
+            if (P.fine_tile_base[mid] <= tile) f = mid; else fhi = mid;
+        }
+        const uint32_t lt = tile - P.fine_tile_base[f];
+        const uint32_t v = P.fview[f];
+        const uint32_t g_end = P.view_strand0[v] + P.view_strands[v];
+        const uint32_t g0 = P.view_strand0[v] + lt * kFineStrandsPerTile + (uint32_t)warp * kFineStrandsPerWarp;
         // Pass A: count the clipped segments of the warp's strands.
         uint32_t count = 0;
         for (uint32_t k = 0; k < kFineStrandsPerWarp; ++k) {
-            const FineStrand fs = fine_strand(P, inst, A, f, g0 + k);
+            const FineStrand fs = fine_strand(P, inst, A, f, g0 + k, g_end);
             // FRUSTUM_TELEMETRY_RETAINED_STRANDS (:1085): every strand the
             // keep tests pass.
             if (A.tel && lane == 0 && fs.nseg > 0u) atomicAdd(tel_frustum(A.tel, f, kTelRetainedStrands), 1u);
@@ -415,7 +428,7 @@ __global__ void __launch_bounds__(kFineThreads, 4) k_fine(const FrameParams* __r
                                               lb_withheld(P, kStageFine));
             if (threadIdx.x == 0) {
                 s_base = base;
-                if (tile % tiles_per_f == 0u) A.counters->frustum_task_base[f] = base;
+                if (lt == 0u) A.counters->frustum_task_base[f] = base;
                 if (tile == n_tiles - 1u) {
                     A.counters->tasks = base + agg;
                     A.counters->frustum_task_base[P.F] = base + agg;
@@ -427,7 +440,7 @@ __global__ void __launch_bounds__(kFineThreads, 4) k_fine(const FrameParams* __r
         for (int w = 0; w < warp; ++w) out += s_warp_count[w];
         // Pass B: project again and write in segment order.
         for (uint32_t k = 0; k < kFineStrandsPerWarp; ++k) {
-            const FineStrand fs = fine_strand(P, inst, A, f, g0 + k);
+            const FineStrand fs = fine_strand(P, inst, A, f, g0 + k, g_end);
             for (uint32_t c = 0; c < fs.nseg; c += kFineChunk) {
                 SegOut o;
                 const bool ok = fine_chunk(P, inst[fs.i], f, fs.meta_offset, fs.nseg, c, lane, o);
@@ -1828,7 +1841,7 @@ __global__ void __launch_bounds__(256) k_telemetry(const FrameParams* __restrict
         tel[1] = *((volatile uint32_t*)&A.counters->tasks);
         tel[3] = *((volatile uint32_t*)&A.counters->refs);
         tel[6] = P.F;
-        for (uint32_t f = 0; f < P.F && f < kMaxFrusta; ++f) {
+        for (uint32_t f = 0; f < P.F && f < FIBER_TELEMETRY_MAX_FRUSTA; ++f) {
             const uint32_t a = A.counters->frustum_task_base[f], b = A.counters->frustum_task_base[f + 1];
             *tel_frustum(tel, f, kTelEmittedSegments) = b - a;
         }

@@ -751,7 +751,7 @@ __global__ void __launch_bounds__(kCamThreads) k_raster(const FrameParams* __res
         if (active) {
             float4 o = fin;
             if (o.w > 1e-6f && o.w < 1.0f) o = make_float4(o.x / o.w, o.y / o.w, o.z / o.w, o.w);
-            size_t pi = (size_t)py * P.width + px;
+            size_t pi = (size_t)P.out_base[f] + (size_t)py * d.screen_width + px;
             reinterpret_cast<uint2*>(R.color)[pi] = pack_half4(o.x, o.y, o.z, o.w);
             R.depth[pi] = gdepth;
             if (P.fragment_counts) R.fragments[pi] = frags;

@@ -42,12 +42,7 @@ __device__ __forceinline__ F3 sub_scaled3(F3 v, F3 w, float s) {
 }
 
 __device__ float sample_dom(const FrameParams& P, const RenderArgs& R, F3 pw, uint32_t layer) {
-    uint32_t f = kInvalid;
-    for (uint32_t i = 0, l = 0; i < P.F; ++i) {
-        if (P.frusta[i].kind != 1u) continue;
-        if (l == layer) { f = i; break; }
-        ++l;
-    }
+    const uint32_t f = layer < P.L ? P.layer_frustum[layer] : kInvalid;
     if (f == kInvalid) return 1.0f;
     const fiber_frustum_desc& d = P.frusta[f];
     float vw = u2f(d.screen_width), vh = u2f(d.screen_height);
@@ -246,17 +241,21 @@ __global__ void __launch_bounds__(128, 8) k_shade(const FrameParams* __restrict_
     __syncthreads();
     const uint32_t n = *((volatile uint32_t*)&R.counters->frustum_task_base[P.camera_frustum_end]);
     const uint32_t cap = P.atlas_cap;
-    const uint32_t nl = min(P.L, 4u);
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
         const uint4 t = reinterpret_cast<const uint4*>(R.tasks)[k];
         const uint32_t i = t.x, seg = t.z;
+        // The task's view: its camera position and its own lights.
+        const uint32_t view = P.fview[min(t.w >> 3, kMaxFrusta - 1u)];
+        const float* camera_pos = P.view_cam_pos[view];
+        const uint32_t l0 = P.view_layer0[view], nlv = P.view_layers[view];
+        const uint32_t nl = min(nlv, 4u);
         const InstanceView& in = inst[i];
         const fiber_strand_meta sm = in.meta[t.y];
         float4 v0, v1;
         segment_world(in, seg, v0, v1);
         F3 U = nrm3(f3(__fsub_rn(v1.x, v0.x), __fsub_rn(v1.y, v0.y), __fsub_rn(v1.z, v0.z)));
-        F3 cam = nrm3(f3(__fsub_rn(P.camera_pos[0], v0.x), __fsub_rn(P.camera_pos[1], v0.y),
-                         __fsub_rn(P.camera_pos[2], v0.z)));
+        F3 cam = nrm3(f3(__fsub_rn(camera_pos[0], v0.x), __fsub_rn(camera_pos[1], v0.y),
+                         __fsub_rn(camera_pos[2], v0.z)));
         F3 B = nrm3(cross3(U, cam));
         F3 V = nrm3(cross3(B, U));
         const fiber_strand_material mat = in.materials[sm.material_idx];
@@ -266,7 +265,7 @@ __global__ void __launch_bounds__(128, 8) k_shade(const FrameParams* __restrict_
         float cur = 1.0f;
         if (nl != 0u) {
             float vs = 0.0f;
-            for (uint32_t l = 0; l < nl; ++l) vs = vs + sample_dom(P, R, mid, l);
+            for (uint32_t l = 0; l < nl; ++l) vs = vs + sample_dom(P, R, mid, l0 + l);
             cur = vs / u2f(nl);
         }
         const size_t hidx = (size_t)i * cap + atlas_idx;
@@ -277,7 +276,7 @@ __global__ void __launch_bounds__(128, 8) k_shade(const FrameParams* __restrict_
         reinterpret_cast<__half2*>(hist_next)[hidx] = __halves2half2(__float2half_rn(vis), __float2half_rn(cur));
         float occ = 1.0f - vis;
         const Detector det_azim = make_detector(sqrtf(mat.beta * mat.beta));
-        for (uint32_t j = 0; j < P.L; ++j) {
+        for (uint32_t j = l0; j < l0 + nlv; ++j) {
             const float* ld = P.light_dir[j];
             F3 L = nrm3(f3(ld[0], ld[1], ld[2]));
             F3 b = marschner(L, V, U, mat, occ, s_quad, det_azim);

@@ -330,6 +330,36 @@ class StrandRasterizerPlugin:
         abi.check(self.lib.fiber_frame_begin(self.ctx, C.byref(camera_cfg.to_c()), C.byref(cam), cfgs, lights_c, n,
                                              _stream_handle(stream)), "fiber_frame_begin")
 
+    def frame_begin_views(self, views: list, stream=None):
+        """One frame of several independent views (fiber_frame_begin_views).
+        views: list of (camera_cfg: FroxelConfig, cam: abi.Camera, light_cfgs:
+        list[FroxelConfig], lights_c: abi.Light array, instance_first,
+        instance_count); a view's instances follow the previous view's. Returns
+        the first pixel of each view's colour / depth / fragment image."""
+        arr = (abi.View * len(views))()
+        keep = []
+        bases, px = [], 0
+        for k, (cfg, cam, lcfgs, lights_c, first, count) in enumerate(views):
+            v = arr[k]
+            v.camera_cfg = cfg.to_c()
+            v.camera = cam
+            n = len(lcfgs)
+            lc = (abi.FroxelConfigC * max(1, n))(*[c.to_c() for c in lcfgs])
+            keep += [lc, lights_c]
+            v.light_cfgs = C.cast(lc, C.POINTER(abi.FroxelConfigC))
+            v.lights = C.cast(lights_c, C.POINTER(abi.Light))
+            v.n_lights = n
+            v.instance_first = first
+            v.instance_count = count
+            bases.append(px)
+            px += cfg.screen_width * cfg.screen_height
+        self.camera_cfg = views[0][0]
+        self.light_cfgs = [c for view in views for c in view[2]]
+        abi.check(self.lib.fiber_frame_begin_views(self.ctx, arr, len(views), _stream_handle(stream)),
+                  "fiber_frame_begin_views")
+        del keep
+        return bases
+
     # Render-graph nodes ------------------------------------------------------
     def depth_reduce(self, opaque_depth: abi.Image, samples: int = 1, stream=None):
         """reduce_opaque_depth (src/pipelines/prepass.rs:780-815): the camera's

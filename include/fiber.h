@@ -406,6 +406,33 @@ fiber_status fiber_raster(fiber_ctx* ctx, uint32_t view, void* stream);
  * (loaded). scene_depth may be NULL (no opaque scene: depth 0). */
 fiber_status fiber_composite(fiber_ctx* ctx, uint32_t view, const fiber_image* scene_color,
                              const fiber_image* scene_depth, fiber_image* out, void* stream);
+/* One view of a multi-view frame: a camera, its lights and the instances it
+ * sees. No counterpart in the reference, which records each view's nodes in
+ * turn; it is the batched configuration of the path's specification. */
+typedef struct fiber_view {
+    fiber_froxel_config camera_cfg;
+    fiber_camera camera;
+    const fiber_froxel_config* light_cfgs;  /* n_lights square maps of one size  */
+    const fiber_light* lights;
+    uint32_t n_lights;
+    uint32_t instance_first;   /* the view's instances: [first, first + count) of
+                                  the instance table; views follow one another */
+    uint32_t instance_count;
+    uint32_t pad;
+} fiber_view;
+
+/* fiber_frame_begin for several independent views rendered by one frame: every
+ * kernel of the frame covers all views, with each view's tasks, pages and
+ * runs at offsets from the frame's single prefix sums, and each view seeing
+ * only its own instances and lights. Frusta: the cameras (frustum v is view
+ * v's camera), then each view's lights. The colour, depth and fragment images
+ * of the views follow one another (view v's starts at the sum of the earlier
+ * views' pixels); deep-opacity layer l is the l-th light, layers as large as
+ * the largest map. At most 64 views and 128 frusta; dense deep-opacity layers
+ * only, telemetry only up to 16 frusta, and no composite or opaque depth (those
+ * are one camera's). Each view's images equal what the view renders alone. */
+fiber_status fiber_frame_begin_views(fiber_ctx* ctx, const fiber_view* views, uint32_t n_views, void* stream);
+
 /* All nodes of one frame in order, replayed from a CUDA graph after the first
  * call with the same frame shape. A scene_depth also feeds the opaque-tile
  * reduce (fiber_opaque_depth at 1 sample) ahead of the prepass. */

@@ -29,7 +29,7 @@ def test_exports_every_declared_symbol():
     (abi.DevicePtr, 12), (abi.Aabb, 32), (abi.StrandGeo, 64), (abi.StrandMaterialC, 64),
     (abi.StrandInstance, 160), (abi.FroxelConfigC, 20), (abi.Camera, 80), (abi.Light, 96), (abi.Image, 24),
     (abi.ServerConfig, 40), (abi.ServerScene, 192), (abi.ServerRequest, 600), (abi.ServerResult, 40),
-    (abi.BatchTuning, 16), (abi.FrustumTelemetry, 44), (abi.Telemetry, 864), (abi.Stats, 408),
+    (abi.BatchTuning, 16), (abi.FrustumTelemetry, 44), (abi.Telemetry, 864), (abi.Stats, 408), (abi.View, 136),
 ])
 def test_struct_sizes(ctype, size):
     assert C.sizeof(ctype) == size
