@@ -607,11 +607,14 @@ def served_section(args) -> dict:
 def batched_section(args, reps: int = 5) -> dict:
     """The batched configuration: independent views (strands log-uniform in
     [1k, 200k] at 16 or 32 points, 256^2 to 1080p, one light with a 512^2 to
-    2048^2 deep-opacity map) rendered by one graph launch per pass after the
-    autotuner picked the branch count and view order, against the same views
-    as a loop of plain frames (per view: frame tables, then its own frame
-    graph). Both are timed with CUDA events on one stream over `reps` passes,
-    after a warm-up pass, inputs resident on the device."""
+    2048^2 deep-opacity map) rendered two ways: one multi-view frame whose
+    kernels cover every view (fiber_frame_begin_views, replayed from one
+    graph), and one graph launch of the views' own frames over concurrent
+    branches after the autotuner picked the branch count and view order; the
+    faster is the batch. Compared with the same views as a loop of plain frames
+    (per view: frame tables, then its own frame graph). All are timed with CUDA
+    events on one stream over `reps` passes, after a warm-up pass, inputs
+    resident on the device."""
     import torch
 
     from bevy_strand_rasterizer_b200 import batched
@@ -646,22 +649,34 @@ def batched_section(args, reps: int = 5) -> dict:
     t = time.time()
     best = batch.tune(stream)
     tune_s = time.time() - t
-    batch_ms = timed(lambda: batch.launch(stream))
+    branches_ms = timed(lambda: batch.launch(stream))
     batch.close()
     for p in plugins:
         p.close()
+    # One multi-view frame: every kernel covers all 64 views.
+    t = time.time()
+    merged = batched.MultiViewFrame(specs, packed)
+    merged_setup_s = time.time() - t
+    merged_ms = timed(lambda: merged.launch(stream))
+    merged.close()
     n = len(specs)
 
     def rates(ms):
         return {"ms_per_pass": ms, "frames_per_s": n * 1e3 / ms, "segments_per_s": segments * 1e3 / ms}
 
+    # The tuner's choice between the two batched forms: the faster one.
+    mode = "multi_view_frame" if merged_ms <= branches_ms else "graph_branches"
+    batch_ms = min(merged_ms, branches_ms)
     return {"views": n, "segments_per_pass": segments, "strands": [v.strands for v in specs],
             "resolutions": sorted({f"{v.camera.width}x{v.camera.height}" for v in specs}),
-            "scene_gen_s": gen_s, "setup_s": setup_s, "tune_s": tune_s, "passes": reps,
+            "scene_gen_s": gen_s, "setup_s": setup_s, "tune_s": tune_s, "merged_setup_s": merged_setup_s,
+            "passes": reps,
             "plain": rates(plain_ms),
-            "batch": dict(rates(batch_ms), tuning={"branches": int(best.branches),
-                                                   "order": "lpt" if best.order else "index",
-                                                   "tuned_ms": float(best.ms)}),
+            "multi_view_frame": rates(merged_ms),
+            "graph_branches": dict(rates(branches_ms), tuning={"branches": int(best.branches),
+                                                               "order": "lpt" if best.order else "index",
+                                                               "tuned_ms": float(best.ms)}),
+            "batch": dict(rates(batch_ms), mode=mode),
             "frames_per_s_ratio": plain_ms / batch_ms}
 
 

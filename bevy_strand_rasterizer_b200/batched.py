@@ -1,6 +1,8 @@
 """The batched configuration: many independent views, each with its own strand
-set, camera, light and resolution, rendered by one CUDA graph launch
-(fiber_batch_*), and the same views as a loop of plain frames for comparison.
+set, camera, light and resolution, rendered either by one multi-view frame
+(MultiViewFrame: every kernel covers all views) or by one CUDA graph launch of
+the views' own frames over concurrent branches (fiber_batch_*), and the same
+views as a loop of plain frames for comparison.
 
 Views: strand counts log-uniform in [1k, 200k] at 16 or 32 points per strand
 (straight scalp hair), a resolution from {256^2, 512^2, 1280x720, 1920x1080},
@@ -73,6 +75,43 @@ def plain_frame(plugin: StrandRasterizerPlugin, spec: ViewSpec, stream=None):
     the frame's nodes replayed from the context's own graph."""
     plugin.frame_begin(spec.camera_cfg, spec.camera, [(spec.light_cfg, spec.light)], stream)
     plugin.frame_fused(None, None, None, stream)
+
+
+class MultiViewFrame:
+    """Every view rendered by one multi-view frame (fiber_frame_begin_views):
+    one context holds each view's strand set as an instance, every kernel of the
+    frame covers all views (each view's tasks, pages and runs at offsets from the
+    frame's single prefix sums), and the frame is replayed from one CUDA graph.
+    Each view's image is the one it renders alone (tests/test_gpu_views.py)."""
+
+    def __init__(self, specs: list[ViewSpec], packed: list[PackedStrandBuffers], device: int = 0, **kw):
+        kw.setdefault("history", False)
+        kw.setdefault("dom_slices", 8)
+        self.plugin = StrandRasterizerPlugin(device=device, **kw)
+        for p in packed:
+            self.plugin.add_geometry(p)
+        self.views = []
+        self._keep = []
+        for k, (s, p) in enumerate(zip(specs, packed)):
+            cam = abi.Camera()
+            cam.clip_from_world[:] = [float(x) for x in s.camera.clip_from_world()]
+            cam.world_position[:] = [float(x) for x in s.camera.eye]
+            lights = (abi.Light * 1)()
+            lights[0].clip_from_world[:] = [float(x) for x in s.light.clip_from_world(p.aabb_min, p.aabb_max)]
+            lights[0].direction_to_light[:] = [float(x) for x in s.light.direction()]
+            lights[0].color[:] = [float(x) for x in s.light.color4()]
+            self._keep.append((cam, lights))
+            self.views.append((s.camera_cfg, cam, [s.light_cfg], lights, k, 1))
+
+    def launch(self, stream=None) -> list:
+        """One frame of every view; returns each view's first pixel in the
+        concatenated colour / depth / fragment images."""
+        bases = self.plugin.frame_begin_views(self.views, stream)
+        self.plugin.frame_fused(None, None, None, stream)
+        return bases
+
+    def close(self):
+        self.plugin.close()
 
 
 class FiberBatch:
