@@ -571,7 +571,7 @@ constexpr uint32_t kCamCap = 128;
 constexpr uint32_t kCamWords = kCamCap / 32;
 constexpr uint16_t kEntryInvalid = 0x8000u;
 
-__global__ void __launch_bounds__(kCamThreads) k_raster(const FrameParams* __restrict__ Pp,
+__global__ void __launch_bounds__(kCamThreads, 14) k_raster(const FrameParams* __restrict__ Pp,
                                                         const InstanceView* __restrict__ inst, RenderArgs R) {
     if (frame_failed(R.counters)) return;
     const FrameParams& P = *Pp;
@@ -611,6 +611,7 @@ __global__ void __launch_bounds__(kCamThreads) k_raster(const FrameParams* __res
         const uint32_t px = tx * d.froxel_size_x + slot % d.froxel_size_x;
         const uint32_t py = ty * d.froxel_size_y + slot / d.froxel_size_x;
         const bool active = slot < d.froxel_size_x * d.froxel_size_y && px < d.screen_width && py < d.screen_height;
+        const size_t pi = (size_t)P.out_base[f] + (size_t)py * d.screen_width + px;  // this pixel's output
         const float pcx = u2f(px) + 0.5f, pcy = u2f(py) + 0.5f;
         const float tile_max = fmaxf(u2f((tx + 1u) * d.froxel_size_x), u2f((ty + 1u) * d.froxel_size_y)) + 1.0f;
         for (uint32_t i = threadIdx.x; i < n_items; i += blockDim.x) {
@@ -751,7 +752,6 @@ __global__ void __launch_bounds__(kCamThreads) k_raster(const FrameParams* __res
         if (active) {
             float4 o = fin;
             if (o.w > 1e-6f && o.w < 1.0f) o = make_float4(o.x / o.w, o.y / o.w, o.z / o.w, o.w);
-            size_t pi = (size_t)P.out_base[f] + (size_t)py * d.screen_width + px;
             reinterpret_cast<uint2*>(R.color)[pi] = pack_half4(o.x, o.y, o.z, o.w);
             R.depth[pi] = gdepth;
             if (P.fragment_counts) R.fragments[pi] = frags;
