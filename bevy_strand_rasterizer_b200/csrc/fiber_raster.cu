@@ -153,10 +153,11 @@ __device__ __forceinline__ uint32_t warp_transpose32(uint32_t x, uint32_t lane) 
 
 // Columns i (pixel centre x0 + i) of one pixel row where a linear function
 // f = f0 + g i lies in [lo, hi]: [ilo, ihi] as floats, unclamped. A slope
-// below 1e-20 makes the test the same for the whole row.
-__device__ __forceinline__ void row_interval(float f0, float g, float lo, float hi, float& ilo, float& ihi) {
+// below 1e-20 makes the test the same for the whole row. `inv` = 1 / g,
+// computed once per entry (the slope is the same on every row).
+__device__ __forceinline__ void row_interval(float f0, float g, float inv, float lo, float hi, float& ilo,
+                                             float& ihi) {
     if (fabsf(g) > 1e-20f) {
-        const float inv = 1.0f / g;
         const float a = (lo - f0) * inv, b = (hi - f0) * inv;
         ilo = fminf(a, b) - 1e-3f;
         ihi = fmaxf(a, b) + 1e-3f;
@@ -189,13 +190,15 @@ __device__ __forceinline__ void candidate_word(const Band& B, bool v, float x0, 
             const uint32_t cols = min(fsx, 64u);
             const uint32_t rows = min(fsy, (64u + fsx - 1u) / fsx);
             const float cmax = u2f(cols - 1u);
+            const float inv_n = fabsf(B.nx) > 1e-20f ? 1.0f / B.nx : 0.0f;
+            const float inv_u = fabsf(B.ux) > 1e-20f ? 1.0f / B.ux : 0.0f;
             for (uint32_t j = 0; j < rows; ++j) {
                 const float ys = y0 + u2f(j);
                 const float dj = __fmaf_rn(B.nx, x0, __fmaf_rn(B.ny, ys, -B.c));
                 const float sj = __fmaf_rn(B.ux, x0, __fmaf_rn(B.uy, ys, -B.cu));
                 float dlo, dhi, slo, shi;
-                row_interval(dj, B.nx, -B.thr, B.thr, dlo, dhi);
-                row_interval(sj, B.ux, B.slo, B.shi, slo, shi);
+                row_interval(dj, B.nx, inv_n, -B.thr, B.thr, dlo, dhi);
+                row_interval(sj, B.ux, inv_u, B.slo, B.shi, slo, shi);
                 const float lo = fmaxf(ceilf(fmaxf(dlo, slo)), 0.0f);
                 const float hi = fminf(floorf(fminf(dhi, shi)), cmax);
                 if (lo <= hi) {
@@ -315,9 +318,24 @@ __global__ void __launch_bounds__(kShadowThreads, 14) k_shadow(const FrameParams
             return (q - 1u) * 32u + bit;
         };
 
+        // Exact coverage of staged entry bi at this pixel (0 when the pixel's
+        // projection falls outside the segment) and the depth there.
+        auto coverage = [&](uint32_t bi, float& qz) -> float {
+            const float ax = sp0x[bi], ay = sp0y[bi], bx = sp1x[bi], by = sp1y[bi];
+            const float t = line_t(pfx, pfy, ax, ay, bx, by);
+            const float qx = wmix(ax, bx, t), qy = wmix(ay, by, t);
+            qz = wmix(sp0z[bi], sp1z[bi], t);
+            const float rr = wmix(srmin[bi], srmax[bi], wclamp(qz, 0.0f, 1.0f));
+            const float dx = pfx - qx, dy = pfy - qy;
+            const float cov = wclamp(1.0f - sqrtf(dx * dx + dy * dy) / rr, 0.0f, 1.0f);
+            return (t < 0.0f || t > 1.0f) ? 0.0f : cov;
+        };
+
         // ---- Pass 1: nearest covered depth = max depth of the covered entries
         // of the first run item holding one; the walk stops once the next
-        // candidate lies past that item.
+        // candidate lies past that item. Candidates are taken two at a time:
+        // both coverages are computed side by side, then applied in entry
+        // order.
         uint32_t best = kInvalid;  // first item with a covered entry
         float z0 = -1.0f;          // its max covered depth
         bool complete = !active;   // the best item is fully processed
@@ -346,19 +364,25 @@ __global__ void __launch_bounds__(kShadowThreads, 14) k_shadow(const FrameParams
             if (!complete) {
                 const uint32_t nq = (rp.n + 31u) >> 5;
                 uint32_t q = 0u, m = 0u;
-                for (uint32_t bi; (bi = next_candidate(nq, q, m)) != kInvalid;) {
-                    const uint32_t item = (uint32_t)(s_item[bi] >> 2);
-                    if (best != kInvalid && item > best) break;
-                    float t = line_t(pfx, pfy, sp0x[bi], sp0y[bi], sp1x[bi], sp1y[bi]);
-                    if (t < 0.0f || t > 1.0f) continue;
-                    float qx = wmix(sp0x[bi], sp1x[bi], t), qy = wmix(sp0y[bi], sp1y[bi], t);
-                    float qz = wmix(sp0z[bi], sp1z[bi], t);
-                    float rr = wmix(srmin[bi], srmax[bi], wclamp(qz, 0.0f, 1.0f));
-                    float dx = pfx - qx, dy = pfy - qy;
-                    float cov = wclamp(1.0f - sqrtf(dx * dx + dy * dy) / rr, 0.0f, 1.0f);
-                    if (cov > 0.0f) {
-                        if (best == kInvalid) { best = item; z0 = wmax(-1.0f, qz); }
-                        else z0 = wmax(z0, qz);
+                for (;;) {
+                    const uint32_t b0 = next_candidate(nq, q, m);
+                    if (b0 == kInvalid) break;
+                    const uint32_t b1 = next_candidate(nq, q, m);
+                    const bool two = b1 != kInvalid;
+                    const uint32_t c1 = two ? b1 : b0;
+                    const uint32_t item0 = (uint32_t)(s_item[b0] >> 2), item1 = (uint32_t)(s_item[c1] >> 2);
+                    float qz0, qz1;
+                    const float cov0 = coverage(b0, qz0);
+                    const float cov1 = coverage(c1, qz1);
+                    if (best != kInvalid && item0 > best) break;
+                    if (cov0 > 0.0f) {
+                        if (best == kInvalid) { best = item0; z0 = wmax(-1.0f, qz0); }
+                        else z0 = wmax(z0, qz0);
+                    }
+                    if (!two || (best != kInvalid && item1 > best)) break;
+                    if (cov1 > 0.0f) {
+                        if (best == kInvalid) { best = item1; z0 = wmax(-1.0f, qz1); }
+                        else z0 = wmax(z0, qz1);
                     }
                 }
                 complete = best != kInvalid && (best + 1u < rp.hi || rp.completes);
@@ -397,28 +421,42 @@ __global__ void __launch_bounds__(kShadowThreads, 14) k_shadow(const FrameParams
                 if (found) {
                     const uint32_t nq = (rp.n + 31u) >> 5;
                     uint32_t q = 0u, m = 0u;
-                    for (uint32_t bi; (bi = next_candidate(nq, q, m)) != kInvalid;) {
-                        float t = line_t(pfx, pfy, sp0x[bi], sp0y[bi], sp1x[bi], sp1y[bi]);
-                        if (t < 0.0f || t > 1.0f) continue;
-                        float qx = wmix(sp0x[bi], sp1x[bi], t), qy = wmix(sp0y[bi], sp1y[bi], t);
-                        float qz = wmix(sp0z[bi], sp1z[bi], t);
-                        float rr = wmix(srmin[bi], srmax[bi], wclamp(qz, 0.0f, 1.0f));
-                        float dx = pfx - qx, dy = pfy - qy;
-                        float cov = wclamp(1.0f - sqrtf(dx * dx + dy * dy) / rr, 0.0f, 1.0f);
-                        if (cov <= 0.0f) continue;
-                        float dzp = wmax(0.0f, alpha_z0 - qz) * inv_span;
-                        float u = wclamp(dzp, 0.0f, 1.0f);  // pow(u, DOM_GAMMA = 1)
-                        float tl = u * u2f(K);
-                        uint32_t si = min(f2u(floorf(tl)), K - 1u);
-                        float wf = tl - floorf(tl);
-                        float al = cov * sabs[bi] * 0.5f;
-                        float* pw = partial + ((uint32_t)(s_item[bi] & 3u) * K + si) * kShadowThreads;
-                        float a0 = pw[0];
+                    // Slice, weight and opacity of one covered entry; the
+                    // deposits into the worker's partials keep entry order.
+                    auto split = [&](uint32_t bi, float cov, float qz, float*& pw, float& wf, float& al, bool& next) {
+                        const float dzp = wmax(0.0f, alpha_z0 - qz) * inv_span;
+                        const float u = wclamp(dzp, 0.0f, 1.0f);  // pow(u, DOM_GAMMA = 1)
+                        const float tl = u * u2f(K);
+                        const uint32_t si = min(f2u(floorf(tl)), K - 1u);
+                        wf = tl - floorf(tl);
+                        al = cov * sabs[bi] * 0.5f;
+                        pw = partial + ((uint32_t)(s_item[bi] & 3u) * K + si) * kShadowThreads;
+                        next = si + 1u < K;
+                    };
+                    auto deposit = [&](float* pw, float wf, float al, bool next) {
+                        const float a0 = pw[0];
                         pw[0] = wclamp(a0 + (1.0f - a0) * (1.0f - wf) * al, 0.0f, 1.0f);
-                        if (si + 1u < K) {
-                            float a1 = pw[kShadowThreads];
+                        if (next) {
+                            const float a1 = pw[kShadowThreads];
                             pw[kShadowThreads] = wclamp(a1 + (1.0f - a1) * wf * al, 0.0f, 1.0f);
                         }
+                    };
+                    for (;;) {
+                        const uint32_t b0 = next_candidate(nq, q, m);
+                        if (b0 == kInvalid) break;
+                        const uint32_t b1 = next_candidate(nq, q, m);
+                        const bool two = b1 != kInvalid;
+                        const uint32_t c1 = two ? b1 : b0;
+                        float qz0, qz1;
+                        const float cov0 = coverage(b0, qz0);
+                        const float cov1 = coverage(c1, qz1);
+                        float *pw0, *pw1, wf0, wf1, al0, al1;
+                        bool n0, n1;
+                        split(b0, cov0, qz0, pw0, wf0, al0, n0);
+                        split(c1, cov1, qz1, pw1, wf1, al1, n1);
+                        if (cov0 > 0.0f) deposit(pw0, wf0, al0, n0);
+                        if (!two) break;
+                        if (cov1 > 0.0f) deposit(pw1, wf1, al1, n1);
                     }
                 }
                 if (staged_all) break;
