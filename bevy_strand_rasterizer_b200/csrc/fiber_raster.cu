@@ -151,18 +151,43 @@ __device__ __forceinline__ uint32_t warp_transpose32(uint32_t x, uint32_t lane) 
     return transpose_stage<1u, 0x55555555u>(x, lane);
 }
 
-// Columns i (pixel centre x0 + i) of one pixel row where a linear function
-// f = f0 + g i lies in [lo, hi]: [ilo, ihi] as floats, unclamped. A slope
-// below 1e-20 makes the test the same for the whole row. `inv` = 1 / g,
-// computed once per entry (the slope is the same on every row).
-__device__ __forceinline__ void row_interval(float f0, float g, float inv, float lo, float hi, float& ilo,
-                                             float& ihi) {
-    if (fabsf(g) > 1e-20f) {
-        const float a = (lo - f0) * inv, b = (hi - f0) * inv;
-        ilo = fminf(a, b) - 1e-3f;
-        ihi = fmaxf(a, b) + 1e-3f;
+// The columns of the tile where a linear function f = f00 + g i + h j (i the
+// column, j the row) lies in [lo, hi] are, on row j, the interval
+// [L + G j, H + G j] with G = -h / g. `line_columns` sets L, H, G once per
+// entry; `row_columns` evaluates one row. A slope |g| <= 1e-20 makes the test
+// the same for the whole row (flat): the row is in or out as a whole. The
+// interval ends are widened by 1e-3 column; their rounding (a few ulps of
+// (|f00| + |lo| + |hi| + 8 |h|) / |g|) stays far inside the band's own slack
+// (0.01 px + 1e-5 of the largest coordinate, divided by |g| in columns), so
+// the set stays a superset of the pixels the exact tests can cover.
+struct RowLine {
+    float L, H, G;
+    bool flat;
+};
+
+__device__ __forceinline__ RowLine line_columns(float f00, float g, float h, float lo, float hi) {
+    RowLine r;
+    r.flat = !(fabsf(g) > 1e-20f);
+    if (!r.flat) {
+        const float inv = 1.0f / g;
+        const float e0 = (lo - f00) * inv, e1 = (hi - f00) * inv;
+        r.L = fminf(e0, e1) - 1e-3f;
+        r.H = fmaxf(e0, e1) + 1e-3f;
+        r.G = -h * inv;
     } else {
-        const bool in = !(f0 < lo) && !(f0 > hi);
+        r.L = r.H = r.G = 0.0f;
+    }
+    return r;
+}
+
+__device__ __forceinline__ void row_columns(const RowLine& r, float f00, float h, float lo, float hi, float jf,
+                                            float& ilo, float& ihi) {
+    if (!r.flat) {
+        ilo = __fmaf_rn(r.G, jf, r.L);
+        ihi = __fmaf_rn(r.G, jf, r.H);
+    } else {
+        const float f = __fmaf_rn(h, jf, f00);
+        const bool in = !(f < lo) && !(f > hi);
         ilo = in ? -1.0f : 1.0f;
         ihi = in ? 1e30f : -1.0f;
     }
@@ -171,13 +196,12 @@ __device__ __forceinline__ void row_interval(float f0, float g, float inv, float
 // Candidate bits of one 32-entry word: lane = entry (valid if v), against the
 // tile's pixel slots p = j fsx + i (p < 64), pixel centres (x0 + i, y0 + j).
 // Per pixel row the band is an interval of columns: |d| <= thr gives one
-// through the row's normal distance at column 0 and the slope nx, and
-// slo <= s <= shi another through u; their intersection sets the row's bits.
-// The 64-bit per-entry masks are then transposed to per-pixel words, written
-// to out[p]. The interval ends are widened by 1e-3 column beyond the band's
-// own slack, so the set is a superset of the per-pixel band test. An entry
-// with a non-finite band parameter (degenerate or NaN segments) is a
-// candidate of every pixel.
+// through the normal distance d, and slo <= s <= shi another through the
+// distance s along u; their intersection sets the row's bits. The 64-bit
+// per-entry masks are then transposed to per-pixel words, written to out[p].
+// An entry with a non-finite band parameter (degenerate or NaN segments) is a
+// candidate of every pixel; a NaN interval end drops that bound (fmaxf and
+// fminf ignore NaN), which only widens the set.
 __device__ __forceinline__ void candidate_word(const Band& B, bool v, float x0, float y0, uint32_t fsx, uint32_t fsy,
                                                uint32_t lane, uint32_t* out) {
     unsigned long long bits = 0ull;
@@ -190,15 +214,15 @@ __device__ __forceinline__ void candidate_word(const Band& B, bool v, float x0, 
             const uint32_t cols = min(fsx, 64u);
             const uint32_t rows = min(fsy, (64u + fsx - 1u) / fsx);
             const float cmax = u2f(cols - 1u);
-            const float inv_n = fabsf(B.nx) > 1e-20f ? 1.0f / B.nx : 0.0f;
-            const float inv_u = fabsf(B.ux) > 1e-20f ? 1.0f / B.ux : 0.0f;
+            const float d00 = __fmaf_rn(B.nx, x0, __fmaf_rn(B.ny, y0, -B.c));
+            const float s00 = __fmaf_rn(B.ux, x0, __fmaf_rn(B.uy, y0, -B.cu));
+            const RowLine rd = line_columns(d00, B.nx, B.ny, -B.thr, B.thr);
+            const RowLine rs = line_columns(s00, B.ux, B.uy, B.slo, B.shi);
             for (uint32_t j = 0; j < rows; ++j) {
-                const float ys = y0 + u2f(j);
-                const float dj = __fmaf_rn(B.nx, x0, __fmaf_rn(B.ny, ys, -B.c));
-                const float sj = __fmaf_rn(B.ux, x0, __fmaf_rn(B.uy, ys, -B.cu));
+                const float jf = u2f(j);
                 float dlo, dhi, slo, shi;
-                row_interval(dj, B.nx, inv_n, -B.thr, B.thr, dlo, dhi);
-                row_interval(sj, B.ux, inv_u, B.slo, B.shi, slo, shi);
+                row_columns(rd, d00, B.ny, -B.thr, B.thr, jf, dlo, dhi);
+                row_columns(rs, s00, B.uy, B.slo, B.shi, jf, slo, shi);
                 const float lo = fmaxf(ceilf(fmaxf(dlo, slo)), 0.0f);
                 const float hi = fminf(floorf(fminf(dhi, shi)), cmax);
                 if (lo <= hi) {
