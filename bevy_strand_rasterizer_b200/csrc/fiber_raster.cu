@@ -89,8 +89,20 @@ constexpr uint32_t kShadowWords = kShadowCap / 32;
 constexpr int kMaxDomSlices = 16;
 
 size_t shadow_smem_bytes(uint32_t K) {
-    return (size_t)kShadowCap * 9 * sizeof(float) + (size_t)kShadowThreads * 4u * K * sizeof(float);
+    return (size_t)kShadowCap * (2 * sizeof(float4) + 3 * sizeof(float)) + (size_t)kShadowThreads * 4u * K * sizeof(float);
 }
+
+// Asynchronous global -> shared copies (cp.async): a thread's copies land
+// without holding registers; cp_async_wait_all waits for the thread's own.
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+    const uint32_t d = (uint32_t)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const uint32_t d = (uint32_t)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 // Coverage candidates. The exact test below covers pixel p (cov > 0) only if
 // p lies within the radius bound rb = rmin + (rmax - rmin) clamp(max z) of the
@@ -240,16 +252,18 @@ __global__ void __launch_bounds__(kShadowThreads, 14) k_shadow(const FrameParams
                                                            const InstanceView* __restrict__ inst, RenderArgs R) {
     if (frame_failed(R.counters)) return;
     const FrameParams& P = *Pp;
-    extern __shared__ float s_dyn[];
-    float* sp0x = s_dyn;
-    float* sp0y = sp0x + kShadowCap;
-    float* sp0z = sp0y + kShadowCap;
-    float* sp1x = sp0z + kShadowCap;
-    float* sp1y = sp1x + kShadowCap;
-    float* sp1z = sp1y + kShadowCap;
-    float* srmin = sp1z + kShadowCap;
+    extern __shared__ float4 s_dyn4[];
+    // Per staged entry: the projected end points (x, y, normalised depth, w),
+    // radii and opacity. The radius and opacity words first receive the
+    // entry's task, instance and material index (the first copy level).
+    float4* sa = s_dyn4;
+    float4* sb = sa + kShadowCap;
+    float* srmin = reinterpret_cast<float*>(sb + kShadowCap);
     float* srmax = srmin + kShadowCap;
     float* sabs = srmax + kShadowCap;
+    uint32_t* s_task = reinterpret_cast<uint32_t*>(srmin);
+    uint32_t* s_inst = reinterpret_cast<uint32_t*>(srmax);
+    uint32_t* s_midx = reinterpret_cast<uint32_t*>(sabs);
     // [worker][K][pixel]: a warp's 32 pixels hit 32 banks whatever the slice.
     float* s_partial = sabs + kShadowCap;
     __shared__ uint32_t s_wbase[kMaxRunItems], s_wcount[kMaxRunItems], s_prefix[kMaxRunItems + 1];
@@ -297,26 +311,37 @@ __global__ void __launch_bounds__(kShadowThreads, 14) k_shadow(const FrameParams
         __syncthreads();
 
         // Stage a round (projection, radii, run item and worker of each entry),
-        // then build the candidate bits: warp per 32-entry word.
+        // then build the candidate bits: warp per 32-entry word. The entries'
+        // data arrive by asynchronous copies in two levels: the reference's
+        // task, instance and material index, then the task's projected end
+        // points (as k_fine projected them for this frustum:
+        // world_to_screen_raw of the segment's vertices), so a round waits
+        // for each level's latency once, whatever its entries.
         auto stage = [&](const RoundPlan& rp) {
             for (uint32_t s = threadIdx.x; s < rp.n; s += blockDim.x) {
                 uint32_t item, j;
                 slot_source(s_prefix, rp, s, item, j);
-                const uint32_t slot = s_wbase[item] + j;
-                const fiber_fine_seg_ref ref = R.refs[slot];
-                const InstanceView& in = inst[ref.inst_id];
-                // The end points as k_fine projected them for this frustum
-                // (world_to_screen_raw of the segment's vertices).
-                const uint32_t t = __ldg(R.ref_task + slot);
-                const float4 a = __ldg(R.task_proj + 2u * (size_t)t), b = __ldg(R.task_proj + 2u * (size_t)t + 1u);
-                const fiber_strand_material& m = in.materials[ref.material_idx];
-                sp0x[s] = a.x; sp0y[s] = a.y; sp0z[s] = normalize_depth01(a.z);
-                sp1x[s] = b.x; sp1y[s] = b.y; sp1z[s] = normalize_depth01(b.z);
-                float rmin = wmax(m.min_radius_pixels, 1e-4f);
+                const uint32_t g = s_wbase[item] + j;
+                cp_async4(s_task + s, R.ref_task + g);
+                cp_async4(s_inst + s, &R.refs[g].inst_id);
+                cp_async4(s_midx + s, &R.refs[g].material_idx);
+                s_item[s] = (uint16_t)((item << 2) | (j & 3u));
+            }
+            cp_async_wait_all();
+            for (uint32_t s = threadIdx.x; s < rp.n; s += blockDim.x) {
+                const size_t t = s_task[s];
+                cp_async16(sa + s, R.task_proj + 2u * t);
+                cp_async16(sb + s, R.task_proj + 2u * t + 1u);
+                const fiber_strand_material& m = inst[s_inst[s]].materials[s_midx[s]];
+                const float rmin = wmax(m.min_radius_pixels, 1e-4f);
                 srmin[s] = rmin;
                 srmax[s] = wmax(m.max_radius_pixels, rmin);
                 sabs[s] = m.absorption_color[3];
-                s_item[s] = (uint16_t)((item << 2) | (j & 3u));
+            }
+            cp_async_wait_all();
+            for (uint32_t s = threadIdx.x; s < rp.n; s += blockDim.x) {
+                sa[s].z = normalize_depth01(sa[s].z);
+                sb[s].z = normalize_depth01(sb[s].z);
             }
             __syncthreads();
             const uint32_t nq = (rp.n + 31u) >> 5;
@@ -324,8 +349,8 @@ __global__ void __launch_bounds__(kShadowThreads, 14) k_shadow(const FrameParams
                 const uint32_t s = q * 32u + lane;
                 const bool v = s < rp.n;
                 const uint32_t e = v ? s : 0u;
-                const Band B = make_band(sp0x[e], sp0y[e], sp1x[e], sp1y[e], sp0z[e], sp1z[e], srmin[e], srmax[e],
-                                         tile_max);
+                const float4 ea = sa[e], eb = sb[e];
+                const Band B = make_band(ea.x, ea.y, eb.x, eb.y, ea.z, eb.z, srmin[e], srmax[e], tile_max);
                 candidate_word(B, v, x0, y0, d.froxel_size_x, d.froxel_size_y, lane, s_pmask + q * kPixelSlots);
             }
         };
@@ -345,10 +370,10 @@ __global__ void __launch_bounds__(kShadowThreads, 14) k_shadow(const FrameParams
         // Exact coverage of staged entry bi at this pixel (0 when the pixel's
         // projection falls outside the segment) and the depth there.
         auto coverage = [&](uint32_t bi, float& qz) -> float {
-            const float ax = sp0x[bi], ay = sp0y[bi], bx = sp1x[bi], by = sp1y[bi];
-            const float t = line_t(pfx, pfy, ax, ay, bx, by);
-            const float qx = wmix(ax, bx, t), qy = wmix(ay, by, t);
-            qz = wmix(sp0z[bi], sp1z[bi], t);
+            const float4 ea = sa[bi], eb = sb[bi];
+            const float t = line_t(pfx, pfy, ea.x, ea.y, eb.x, eb.y);
+            const float qx = wmix(ea.x, eb.x, t), qy = wmix(ea.y, eb.y, t);
+            qz = wmix(ea.z, eb.z, t);
             const float rr = wmix(srmin[bi], srmax[bi], wclamp(qz, 0.0f, 1.0f));
             const float dx = pfx - qx, dy = pfy - qy;
             const float cov = wclamp(1.0f - sqrtf(dx * dx + dy * dy) / rr, 0.0f, 1.0f);
