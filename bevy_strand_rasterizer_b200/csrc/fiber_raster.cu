@@ -774,63 +774,74 @@ __global__ void __launch_bounds__(kCamThreads, 14) k_raster(const FrameParams* _
                 candidate_word(B, v, x0, y0, d.froxel_size_x, d.froxel_size_y, lane, s_pmask + q * kPixelSlots);
             }
             __syncthreads();
-            uint32_t pos = 0u;  // next entry of this pixel's walk
+            // The walk takes one candidate entry per step, so every live lane
+            // runs the coverage and shading arithmetic on each step; the
+            // entry lands in its worker's part of the current group, and the
+            // group is blended when the walk reaches the next group.
+            uint32_t pos = 0u;            // next entry of this pixel's walk
+            uint32_t cur_lead = kInvalid;  // first entry of the group being gathered
+            float4 g0 = make_float4(0.0f, 0.0f, 0.0f, 0.0f), g1 = g0, g2 = g0, g3 = g0;
+            float e0 = 0.0f, e1 = 0.0f, e2 = 0.0f, e3 = 0.0f;
+            // (w0 over w1) over (w2 over w3), depth max.
+            auto flush_group = [&]() {
+                if (cur_lead == kInvalid) return;
+                fin = over(fin, over(over(g0, g1), over(g2, g3)));
+                gdepth = wmax(gdepth, wmax(wmax(e0, e1), wmax(e2, e3)));
+                g0 = g1 = g2 = g3 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                e0 = e1 = e2 = e3 = 0.0f;
+                cur_lead = kInvalid;
+            };
             while (!done) {
                 // first candidate entry >= pos
                 uint32_t q = pos >> 5;
                 uint32_t m = q < nq ? (s_pmask[q * kPixelSlots + slot] & (0xFFFFFFFFu << (pos & 31u))) : 0u;
                 while (m == 0u && q + 1u < nq) m = s_pmask[(++q) * kPixelSlots + slot];
                 if (m == 0u) break;
-                const uint32_t c = q * 32u + (uint32_t)(__ffs(m) - 1);
-                const uint32_t item = (uint32_t)((s_item[c] >> 2) & 0x3FFu);
-                if (pending != kInvalid && item > pending) {
-                    end_of_item();
-                    if (done) break;
+                const uint32_t bi = q * 32u + (uint32_t)(__ffs(m) - 1);
+                const uint32_t tag = s_item[bi];
+                const uint32_t w = tag & 3u;
+                const uint32_t lead = bi - w;
+                if (lead != cur_lead) {
+                    flush_group();
+                    const uint32_t item = (tag >> 2) & 0x3FFu;
+                    if (pending != kInvalid && item > pending) {
+                        end_of_item();
+                        if (done) break;
+                    }
+                    cur_lead = lead;
+                    pending = item;
                 }
-                const uint32_t lead = c - (s_item[c] & 3u);
-                const uint32_t end = min(lead + 4u, s_prefix[item - rp.lo + 1u]);
-                pos = end;
-                pending = item;
-                float4 part[4];
-                float pd[4];
-#pragma unroll
-                for (uint32_t w = 0; w < 4u; ++w) {
-                    part[w] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-                    pd[w] = 0.0f;
-                    const uint32_t bi = lead + w;
-                    if (bi >= end || !((s_pmask[(bi >> 5) * kPixelSlots + slot] >> (bi & 31u)) & 1u)) continue;
-                    const float ax = sp0x[bi], ay = sp0y[bi], bx = sp1x[bi], by = sp1y[bi];
-                    const float rmax = srmax[bi];
-                    if ((pcx < wmin(ax, bx) - rmax || pcy < wmin(ay, by) - rmax) ||
-                        (pcx > wmax(ax, bx) + rmax || pcy > wmax(ay, by) + rmax))
-                        continue;
-                    const float abx = bx - ax, aby = by - ay;
-                    float t = ((pcx - ax) * abx + (pcy - ay) * aby) * sinv[bi];
-                    if (!(t >= 0.0f && t <= 1.0f)) continue;
-                    float fx = ax + abx * t, fy = ay + aby * t;
-                    float pz = wmix(sz0[bi], sz1[bi], t);
-                    float rr = wmix(srmin[bi], rmax, wclamp(normalize_depth01(pz), 0.0f, 1.0f));
-                    float dx = pcx - fx, dy = pcy - fy;
-                    float d2 = dx * dx + dy * dy;
-                    if (!(d2 < rr * rr)) continue;
-                    float cov = wclamp(1.0f - sqrtf(d2) / rr, 0.0f, 1.0f);
-                    // perspective_correct_line_t (:149-154)
-                    float aw0 = wmax(fabsf(sw0[bi]), 1e-6f), aw1 = wmax(fabsf(sw1[bi]), 1e-6f);
-                    float tw = (t * aw0) / ((1.0f - t) * aw1 + t * aw0);
-                    float4 c0 = load_half4(reinterpret_cast<const __half*>(&ss0[bi]));
-                    float4 c1 = load_half4(reinterpret_cast<const __half*>(&ss1[bi]));
-                    float sr = wmix(c0.x, c1.x, tw), sg = wmix(c0.y, c1.y, tw);
-                    float sbl = wmix(c0.z, c1.z, tw), sa = wmix(c0.w, c1.w, tw);
-                    float alpha = sa * cov;
-                    float vsb = svis[bi];
-                    part[w] = make_float4(sr * vsb * alpha, sg * vsb * alpha, sbl * vsb * alpha, alpha);
-                    pd[w] = pz;
-                    ++frags;
-                }
-                // (w0 over w1) over (w2 over w3), depth max.
-                fin = over(fin, over(over(part[0], part[1]), over(part[2], part[3])));
-                gdepth = wmax(gdepth, wmax(wmax(pd[0], pd[1]), wmax(pd[2], pd[3])));
+                pos = bi + 1u;
+                const float ax = sp0x[bi], ay = sp0y[bi], bx = sp1x[bi], by = sp1y[bi];
+                const float rmax = srmax[bi];
+                const bool in_box = !((pcx < wmin(ax, bx) - rmax || pcy < wmin(ay, by) - rmax) ||
+                                      (pcx > wmax(ax, bx) + rmax || pcy > wmax(ay, by) + rmax));
+                const float abx = bx - ax, aby = by - ay;
+                const float t = ((pcx - ax) * abx + (pcy - ay) * aby) * sinv[bi];
+                const float fx = ax + abx * t, fy = ay + aby * t;
+                const float pz = wmix(sz0[bi], sz1[bi], t);
+                const float rr = wmix(srmin[bi], rmax, wclamp(normalize_depth01(pz), 0.0f, 1.0f));
+                const float dx = pcx - fx, dy = pcy - fy;
+                const float d2 = dx * dx + dy * dy;
+                if (!(in_box && t >= 0.0f && t <= 1.0f && d2 < rr * rr)) continue;
+                const float cov = wclamp(1.0f - sqrtf(d2) / rr, 0.0f, 1.0f);
+                // perspective_correct_line_t (:149-154)
+                const float aw0 = wmax(fabsf(sw0[bi]), 1e-6f), aw1 = wmax(fabsf(sw1[bi]), 1e-6f);
+                const float tw = (t * aw0) / ((1.0f - t) * aw1 + t * aw0);
+                const float4 c0 = load_half4(reinterpret_cast<const __half*>(&ss0[bi]));
+                const float4 c1 = load_half4(reinterpret_cast<const __half*>(&ss1[bi]));
+                const float sr = wmix(c0.x, c1.x, tw), sg = wmix(c0.y, c1.y, tw);
+                const float sbl = wmix(c0.z, c1.z, tw), sa = wmix(c0.w, c1.w, tw);
+                const float alpha = sa * cov;
+                const float vsb = svis[bi];
+                const float4 v = make_float4(sr * vsb * alpha, sg * vsb * alpha, sbl * vsb * alpha, alpha);
+                if (w == 0u) { g0 = v; e0 = pz; }
+                else if (w == 1u) { g1 = v; e1 = pz; }
+                else if (w == 2u) { g2 = v; e2 = pz; }
+                else { g3 = v; e3 = pz; }
+                ++frags;
             }
+            flush_group();
             // The last item blended into ends in this round unless the round
             // stops inside it.
             if (pending != kInvalid && (pending + 1u < rp.hi || rp.completes)) end_of_item();
