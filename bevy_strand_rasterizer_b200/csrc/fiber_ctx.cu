@@ -108,7 +108,7 @@ struct fiber_ctx {
     uint32_t lb_offset[kStageCount] = {0};
     // device buffers
     DevBuf d_params, d_inst, d_counters, d_lb, d_range_valid, d_ranges, d_keep, d_inst_visible, d_inst_keep;
-    DevBuf d_lut_simple;  // per coarse tile: the LUT takes the binary-search slice lookup
+    DevBuf d_lut_tree;  // per coarse tile: the slice lookup's search tree (kLutTreeWords)
     DevBuf d_lut, d_tasks, d_projected, d_page_table, d_page_meta, d_counts, d_offsets, d_cursors;
     DevBuf d_refs, d_ref_keys, d_active_flags, d_active_list, d_work, d_runs, d_big_cells;
     DevBuf d_visit_rec, d_visit_task, d_visit_rank, d_task_key, d_task_mat, d_cells_small, d_cells_mid, d_cells_large;
@@ -226,7 +226,7 @@ PrepassArgs prepass_args(fiber_ctx* c) {
     A.inst_visible = dp<uint32_t>(c->d_inst_visible);
     A.inst_keep = dp<float>(c->d_inst_keep);
     A.lut = dp<fiber_coarse_depth_lut_entry>(c->d_lut);
-    A.lut_simple = dp<uint8_t>(c->d_lut_simple);
+    A.lut_tree = dp<uint32_t>(c->d_lut_tree);
     A.tasks = dp<fiber_binning_task>(c->d_tasks);
     A.projected = dp<fiber_projected_segment>(c->d_projected);
     A.page_table = dp<uint32_t>(c->d_page_table);
@@ -584,7 +584,7 @@ fiber_status fiber_ctx_destroy(fiber_ctx* c) {
         for (auto& s : v)
             if (s.live && s.ptr) cudaFree(s.ptr);
     DevBuf* bufs[] = {&c->d_params, &c->d_inst, &c->d_counters, &c->d_lb, &c->d_range_valid, &c->d_ranges,
-                      &c->d_keep, &c->d_inst_visible, &c->d_inst_keep, &c->d_lut, &c->d_lut_simple, &c->d_tasks, &c->d_projected,
+                      &c->d_keep, &c->d_inst_visible, &c->d_inst_keep, &c->d_lut, &c->d_lut_tree, &c->d_tasks, &c->d_projected,
                       &c->d_page_table, &c->d_page_meta, &c->d_counts, &c->d_offsets, &c->d_cursors, &c->d_refs,
                       &c->d_ref_keys, &c->d_active_flags, &c->d_active_list, &c->d_work, &c->d_runs,
                       &c->d_big_cells, &c->d_dom_depth, &c->d_dom_opacity, &c->d_shadow_map, &c->d_atlas,
@@ -954,7 +954,7 @@ static fiber_status frame_begin_views(fiber_ctx* c, const fiber_view* views, uin
     ENSURE(c->d_inst_visible, (uint64_t)I * 4, false);
     ENSURE(c->d_inst_keep, (uint64_t)I * 4, false);
     ENSURE(c->d_lut, table * sizeof(fiber_coarse_depth_lut_entry), false);
-    ENSURE(c->d_lut_simple, (uint64_t)coarse + 1u, false);
+    ENSURE(c->d_lut_tree, ((uint64_t)coarse + 1u) * kLutTreeWords * 4u, false);
     ENSURE(c->d_tasks, task_cap * sizeof(fiber_binning_task), false);
     ENSURE(c->d_projected, task_cap * sizeof(fiber_projected_segment), false);
     ENSURE(c->d_page_table, table * 4, false);

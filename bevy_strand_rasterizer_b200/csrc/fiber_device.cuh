@@ -17,6 +17,7 @@ namespace fiber {
 
 constexpr uint32_t kCoarseExtent = 4;      // COARSE_FINE_TILE_EXTENT (src/plugin.rs:58)
 constexpr uint32_t kDepthSlices = 16;      // COARSE_DEPTH_SLICES (src/plugin.rs:59)
+constexpr uint32_t kLutTreeWords = 36;  // 4 quarter starts + 4 x (4 starts, 4 ends)
 constexpr uint32_t kPageSize = 256;        // COARSE_COUNT_PAGE_SIZE (src/plugin.rs:61)
 constexpr uint32_t kDepthQuantMax = 16777215u;
 constexpr uint32_t kInvalid = 0xFFFFFFFFu;

@@ -58,7 +58,11 @@ struct PrepassArgs {
     uint32_t* inst_visible;          // [I]
     float* inst_keep;                // [I] max(camera, shadow) keep probability
     fiber_coarse_depth_lut_entry* lut;
-    uint8_t* lut_simple;  // [coarse tiles] 1: the LUT's 16 entries are populated, ordered and disjoint
+    // [coarse tiles][kLutTreeWords]: the slice lookup's search tree of a LUT
+    // whose 16 entries are populated, ordered and disjoint (word 0 = kInvalid
+    // otherwise): the starts of entries 0, 4, 8, 12, then per quarter the
+    // starts and the ends of its four entries.
+    uint32_t* lut_tree;
     fiber_binning_task* tasks;
     fiber_projected_segment* projected;
     uint32_t* page_table;

@@ -271,8 +271,20 @@ __global__ void k_lut(const FrameParams* __restrict__ Pp, PrepassArgs A) {
             out[out_slice++] = fiber_coarse_depth_lut_entry{start, end, start, max(1u, end - start + 1u)};
         }
     }
-    A.lut_simple[t] = (simple && out_slice == kDepthSlices) ? 1u : 0u;
-    for (; out_slice < kDepthSlices; ++out_slice) out[out_slice] = fiber_coarse_depth_lut_entry{0u, 0u, 0u, 0u};
+    for (uint32_t k = out_slice; k < kDepthSlices; ++k) out[k] = fiber_coarse_depth_lut_entry{0u, 0u, 0u, 0u};
+    // The search tree of a simple LUT (read back from this thread's own
+    // entries); word 0 = kInvalid marks a LUT that takes the linear lookup.
+    uint4* tree = reinterpret_cast<uint4*>(A.lut_tree + (size_t)t * kLutTreeWords);
+    if (simple && out_slice == kDepthSlices) {
+        tree[0] = make_uint4(out[0].z_min_q, out[4].z_min_q, out[8].z_min_q, out[12].z_min_q);
+        for (uint32_t g = 0; g < 4u; ++g) {
+            const fiber_coarse_depth_lut_entry* e = out + 4u * g;
+            tree[1u + 2u * g] = make_uint4(e[0].z_min_q, e[1].z_min_q, e[2].z_min_q, e[3].z_min_q);
+            tree[2u + 2u * g] = make_uint4(e[0].z_max_q, e[1].z_max_q, e[2].z_max_q, e[3].z_max_q);
+        }
+    } else {
+        tree[0] = make_uint4(kInvalid, kInvalid, kInvalid, kInvalid);
+    }
 }
 
 // ===========================================================================
@@ -491,20 +503,22 @@ constexpr uint32_t kWarpSortMax = 256;
 // lut_slices for one end point of a LUT whose 16 entries are all populated,
 // each start <= end and each end below the next start: at most one entry
 // holds the quantised depth q, and the nearest entry otherwise is a neighbour
-// of the gap q falls in, so a binary search over the starts returns what the
-// linear scan returns (first holding entry, else first nearest).
-__device__ __forceinline__ uint32_t lut_slice_simple(const fiber_coarse_depth_lut_entry* e, float z) {
+// of the gap q falls in, so the last entry whose start is <= q (the starts
+// increase strictly) answers what the linear scan answers (first holding
+// entry, else first nearest). The search reads the LUT's tree: the quarter
+// starts (piv, shared by both end points), then the quarter's starts and ends.
+__device__ __forceinline__ uint32_t lut_slice_tree(const uint4* tree, const uint4& piv, float z) {
     const uint32_t q = quantize_depth01(z);
-    const uint2* xy = reinterpret_cast<const uint2*>(e);  // entry i: xy[2 i] = (z_min_q, z_max_q)
-    int lo = -1;  // last entry with start <= q
-#pragma unroll
-    for (int step = 16; step > 0; step >>= 1)
-        if (lo + step < (int)kDepthSlices && __ldg(&xy[2 * (lo + step)]).x <= q) lo += step;
-    if (lo < 0) return 0u;
-    const uint2 a = __ldg(&xy[2 * lo]);
-    if (q <= a.y || lo == (int)kDepthSlices - 1) return (uint32_t)lo;
-    const uint32_t next_start = __ldg(&xy[2 * (lo + 1)]).x;
-    return (q - a.y <= next_start - q) ? (uint32_t)lo : (uint32_t)lo + 1u;
+    if (piv.x > q) return 0u;  // no entry starts at or below q: the first is nearest
+    const uint32_t g = (piv.y <= q ? 1u : 0u) + (piv.z <= q ? 1u : 0u) + (piv.w <= q ? 1u : 0u);
+    const uint4 st = __ldg(tree + 1u + 2u * g), en = __ldg(tree + 2u + 2u * g);
+    const uint32_t r = (st.y <= q ? 1u : 0u) + (st.z <= q ? 1u : 0u) + (st.w <= q ? 1u : 0u);
+    const uint32_t lo = 4u * g + r;
+    const uint32_t end = r == 0u ? en.x : (r == 1u ? en.y : (r == 2u ? en.z : en.w));
+    if (q <= end || lo == kDepthSlices - 1u) return lo;
+    const uint32_t next_piv = g == 0u ? piv.y : (g == 1u ? piv.z : piv.w);
+    const uint32_t next_start = r == 0u ? st.y : (r == 1u ? st.z : (r == 2u ? st.w : next_piv));
+    return (q - end <= next_start - q) ? lo : lo + 1u;
 }
 
 // lut_slice for both clipped end points at once: per end point, the first
@@ -604,11 +618,11 @@ struct FillSink {
 };
 
 // opq: the opaque fine tiles of the camera (null when none are bound); pd:
-// the segment's clip direction (p1 - p0 and its reciprocals).
+// the segment's clip direction (p1 - p0 and its reciprocals); (ccx, ccy): the
+// coarse tile's column and row in the frustum.
 template <class Sink>
 __device__ __forceinline__ void walk_page(const PrepassArgs& A, F3 p0, const ClipDir& pd, const fiber_frustum_desc& d,
-                                          uint32_t tile, uint32_t local, const uint2* opq, Sink& sink) {
-    uint32_t ccx = local % d.coarse_tiles_x, ccy = local / d.coarse_tiles_x;
+                                          uint32_t tile, uint32_t ccx, uint32_t ccy, const uint2* opq, Sink& sink) {
     // fine_tile_occluded_by_opaque (:551-573) applies to the camera only. The
     // opaque tiles hold the camera's fine tiles alone, so the camera's
     // fine_depth_tile_base (0) is not added.
@@ -628,10 +642,12 @@ __device__ __forceinline__ void walk_page(const PrepassArgs& A, F3 p0, const Cli
     if (!clip_segment_pre(p0, pd, f3(ox, oy, 0.0f), bmax, c0, c1)) return;
     const ClipDir cd = clip_dir(c0, c1);  // shared by the slice clips below
     const fiber_coarse_depth_lut_entry* lut = A.lut + (size_t)tile * kDepthSlices;
+    const uint4* tree = reinterpret_cast<const uint4*>(A.lut_tree + (size_t)tile * kLutTreeWords);
+    const uint4 piv = __ldg(tree);
     uint32_t z0s, z1s;
-    if (A.lut_simple[tile]) {
-        z0s = lut_slice_simple(lut, c0.z);
-        z1s = lut_slice_simple(lut, c1.z);
+    if (piv.x != kInvalid) {
+        z0s = lut_slice_tree(tree, piv, c0.z);
+        z1s = lut_slice_tree(tree, piv, c1.z);
     } else {
         lut_slices(lut, c0.z, c1.z, z0s, z1s);
     }
@@ -765,7 +781,7 @@ __device__ __forceinline__ void walk_task(const FrameParams& P, const PrepassArg
         if (fx < (int32_t)min_cx || fx > (int32_t)max_cx || fy < (int32_t)min_cy || fy > (int32_t)max_cy) break;
         uint32_t local = (uint32_t)fy * d.coarse_tiles_x + (uint32_t)fx;
         if (local < d.coarse_depth_tile_count)
-            walk_page(A, w.p0, pd, d, d.coarse_depth_tile_base + local, local, opq, sink);
+            walk_page(A, w.p0, pd, d, d.coarse_depth_tile_base + local, (uint32_t)fx, (uint32_t)fy, opq, sink);
         if (fx == ex && fy == ey) break;
         if (tx <= ty) { fx += sx; tx += ddx; } else { fy += sy; ty += ddy; }
         ++safety;
