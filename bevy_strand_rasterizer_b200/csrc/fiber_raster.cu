@@ -98,6 +98,10 @@ __device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
     const uint32_t d = (uint32_t)__cvta_generic_to_shared(smem);
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(gmem) : "memory");
 }
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+    const uint32_t d = (uint32_t)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(gmem) : "memory");
+}
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
     const uint32_t d = (uint32_t)__cvta_generic_to_shared(smem);
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(gmem) : "memory");
@@ -292,8 +296,6 @@ __global__ void __launch_bounds__(kShadowThreads, 14) k_shadow(const FrameParams
         if (run.work_count == 0u || layer == kInvalid) continue;
         const uint32_t n_items = min(run.work_count, kMaxRunItems);
         const fiber_frustum_desc& d = P.frusta[f];
-        const float* clip = P.clip[f];
-        const float vw = u2f(d.screen_width), vh = u2f(d.screen_height);
         const uint32_t ftx = ceil_div(d.screen_width, d.froxel_size_x);
         const uint32_t tx = run.screen_tile_id % ftx, ty = run.screen_tile_id / ftx;
         const uint32_t px = tx * d.froxel_size_x + slot % d.froxel_size_x;
@@ -662,11 +664,15 @@ __global__ void __launch_bounds__(kCamThreads, 14) k_raster(const FrameParams* _
                                                         const InstanceView* __restrict__ inst, RenderArgs R) {
     if (frame_failed(R.counters)) return;
     const FrameParams& P = *Pp;
-    // Per staged entry: 64 B of projection, radii and shading texels, the run
-    // item and position in it (bit 15: behind the camera, never a candidate).
-    __shared__ float sp0x[kCamCap], sp0y[kCamCap], sp1x[kCamCap], sp1y[kCamCap], sinv[kCamCap];
-    __shared__ float sz0[kCamCap], sz1[kCamCap], sw0[kCamCap], sw1[kCamCap], srmin[kCamCap], srmax[kCamCap];
-    __shared__ float svis[kCamCap];
+    // Per staged entry: 68 B of projection (x, y, z, w of both end points),
+    // radii and shading texels, the run item and position in it (bit 15:
+    // behind the camera, never a candidate). The words of sinv, srmin, srmax
+    // and svis first receive the reference's task, instance, segment and
+    // material index (the first copy level); s_hist receives the history
+    // texel pair (visibility, current).
+    __shared__ float4 sa[kCamCap], sb[kCamCap];
+    __shared__ float sinv[kCamCap], srmin[kCamCap], srmax[kCamCap], svis[kCamCap];
+    __shared__ uint32_t s_hist[kCamCap];
     __shared__ uint2 ss0[kCamCap], ss1[kCamCap];
     __shared__ uint16_t s_item[kCamCap];
     __shared__ uint32_t s_pmask[kCamWords * kPixelSlots];  // [word][pixel] candidate bits
@@ -691,8 +697,6 @@ __global__ void __launch_bounds__(kCamThreads, 14) k_raster(const FrameParams* _
         if (run.work_count == 0u || f >= P.camera_frustum_end) continue;
         const uint32_t n_items = min(run.work_count, kMaxRunItems);
         const fiber_frustum_desc& d = P.frusta[f];
-        const float* clip = P.clip[f];
-        const float vw = u2f(d.screen_width), vh = u2f(d.screen_height);
         const uint32_t ftx = ceil_div(d.screen_width, d.froxel_size_x);
         const uint32_t tx = run.screen_tile_id % ftx, ty = run.screen_tile_id / ftx;
         const uint32_t px = tx * d.froxel_size_x + slot % d.froxel_size_x;
@@ -730,36 +734,51 @@ __global__ void __launch_bounds__(kCamThreads, 14) k_raster(const FrameParams* _
             __syncthreads();
             if (!s_more) break;
             const RoundPlan rp = s_plan;
+            // The entries arrive by asynchronous copies in two levels: the
+            // reference (task, instance, segment, material index), then the
+            // task's projected end points (as k_fine projected them for this
+            // frustum) and the segment's shading and history texels.
+            uint32_t* s_task = reinterpret_cast<uint32_t*>(sinv);
+            uint32_t* s_inst = reinterpret_cast<uint32_t*>(srmin);
+            uint32_t* s_seg = reinterpret_cast<uint32_t*>(srmax);
+            uint32_t* s_midx = reinterpret_cast<uint32_t*>(svis);
             for (uint32_t s = threadIdx.x; s < rp.n; s += blockDim.x) {
                 uint32_t item, j;
                 slot_source(s_prefix, rp, s, item, j);
-                const uint32_t slot = s_wbase[item] + j;
-                const fiber_fine_seg_ref ref = R.refs[slot];
-                const InstanceView& in = inst[ref.inst_id];
-                // The end points as k_fine projected them for this frustum.
-                const uint32_t t = __ldg(R.ref_task + slot);
-                const float4 a = __ldg(R.task_proj + 2u * (size_t)t), b = __ldg(R.task_proj + 2u * (size_t)t + 1u);
-                uint16_t tag = (uint16_t)((item << 2) | (j & 3u));
+                const uint32_t g = s_wbase[item] + j;
+                cp_async4(s_task + s, R.ref_task + g);
+                cp_async4(s_inst + s, &R.refs[g].inst_id);
+                cp_async4(s_seg + s, &R.refs[g].seg_id);
+                cp_async4(s_midx + s, &R.refs[g].material_idx);
+                s_item[s] = (uint16_t)((item << 2) | (j & 3u));
+            }
+            cp_async_wait_all();
+            for (uint32_t s = threadIdx.x; s < rp.n; s += blockDim.x) {
+                const size_t t = s_task[s];
+                const uint32_t ii = s_inst[s], i0 = min(s_seg[s], cap - 1u), i1 = min(i0 + 1u, cap - 1u);
+                const fiber_strand_material& m = inst[ii].materials[s_midx[s]];
+                const size_t t0 = (size_t)ii * cap + i0, t1 = (size_t)ii * cap + i1;
+                cp_async16(sa + s, R.task_proj + 2u * t);
+                cp_async16(sb + s, R.task_proj + 2u * t + 1u);
+                cp_async8(ss0 + s, R.atlas + t0 * 4);
+                cp_async8(ss1 + s, R.atlas + t1 * 4);
+                cp_async4(s_hist + s, hist + t0 * 2);
+                // min_radius = max(rmin, 1e-4) and max(rmax, min_radius) are
+                // idempotent on these values, so they are applied once here.
+                const float rmin = wmax(m.min_radius_pixels, 1e-4f);
+                srmin[s] = rmin;
+                srmax[s] = wmax(m.max_radius_pixels, rmin);
+            }
+            cp_async_wait_all();
+            for (uint32_t s = threadIdx.x; s < rp.n; s += blockDim.x) {
+                const float4 a = sa[s], b = sb[s];
                 if (!(a.x < 0.0f && b.x < 0.0f)) {
-                    const fiber_strand_material& m = in.materials[ref.material_idx];
-                    float rmin = wmax(m.min_radius_pixels, 1e-4f);
-                    float rmax = wmax(m.max_radius_pixels, rmin);
-                    uint32_t i0 = ref.seg_id, i1 = min(i0 + 1u, cap - 1u);
-                    size_t t0 = (size_t)ref.inst_id * cap + i0, t1 = (size_t)ref.inst_id * cap + i1;
-                    float abx = b.x - a.x, aby = b.y - a.y;
-                    sp0x[s] = a.x; sp0y[s] = a.y; sp1x[s] = b.x; sp1y[s] = b.y;
+                    const float abx = b.x - a.x, aby = b.y - a.y;
                     sinv[s] = 1.0f / (abx * abx + aby * aby);
-                    sz0[s] = a.z; sz1[s] = b.z; sw0[s] = a.w; sw1[s] = b.w;
-                    // min_radius = max(rmin, 1e-4) and max(rmax, min_radius) are
-                    // idempotent on these values, so they are applied once here.
-                    srmin[s] = rmin; srmax[s] = rmax;
-                    ss0[s] = *reinterpret_cast<const uint2*>(R.atlas + t0 * 4);
-                    ss1[s] = *reinterpret_cast<const uint2*>(R.atlas + t1 * 4);
-                    svis[s] = __half2float(hist[t0 * 2]);
+                    svis[s] = __low2float(*reinterpret_cast<const __half2*>(s_hist + s));
                 } else {
-                    tag |= kEntryInvalid;
+                    s_item[s] |= kEntryInvalid;
                 }
-                s_item[s] = tag;
             }
             __syncthreads();
             // Candidate bits: warp per 32-entry word. The radius bound uses the
@@ -769,8 +788,9 @@ __global__ void __launch_bounds__(kCamThreads, 14) k_raster(const FrameParams* _
                 const uint32_t s = q * 32u + lane;
                 const bool v = s < rp.n && !(s_item[s] & kEntryInvalid);
                 const uint32_t e = v ? s : 0u;
-                const Band B = make_band(sp0x[e], sp0y[e], sp1x[e], sp1y[e], normalize_depth01(sz0[e]),
-                                         normalize_depth01(sz1[e]), srmin[e], srmax[e], tile_max);
+                const float4 ea = sa[e], eb = sb[e];
+                const Band B = make_band(ea.x, ea.y, eb.x, eb.y, normalize_depth01(ea.z), normalize_depth01(eb.z),
+                                         srmin[e], srmax[e], tile_max);
                 candidate_word(B, v, x0, y0, d.froxel_size_x, d.froxel_size_y, lane, s_pmask + q * kPixelSlots);
             }
             __syncthreads();
@@ -778,7 +798,6 @@ __global__ void __launch_bounds__(kCamThreads, 14) k_raster(const FrameParams* _
             // runs the coverage and shading arithmetic on each step; the
             // entry lands in its worker's part of the current group, and the
             // group is blended when the walk reaches the next group.
-            uint32_t pos = 0u;            // next entry of this pixel's walk
             uint32_t cur_lead = kInvalid;  // first entry of the group being gathered
             float4 g0 = make_float4(0.0f, 0.0f, 0.0f, 0.0f), g1 = g0, g2 = g0, g3 = g0;
             float e0 = 0.0f, e1 = 0.0f, e2 = 0.0f, e3 = 0.0f;
@@ -791,13 +810,49 @@ __global__ void __launch_bounds__(kCamThreads, 14) k_raster(const FrameParams* _
                 e0 = e1 = e2 = e3 = 0.0f;
                 cur_lead = kInvalid;
             };
-            while (!done) {
-                // first candidate entry >= pos
-                uint32_t q = pos >> 5;
-                uint32_t m = q < nq ? (s_pmask[q * kPixelSlots + slot] & (0xFFFFFFFFu << (pos & 31u))) : 0u;
-                while (m == 0u && q + 1u < nq) m = s_pmask[(++q) * kPixelSlots + slot];
-                if (m == 0u) break;
-                const uint32_t bi = q * 32u + (uint32_t)(__ffs(m) - 1);
+            // Candidates are taken two at a time: both entries' arithmetic
+            // runs side by side, then they land in entry order.
+            uint32_t q = 0u, m = 0u;
+            auto next = [&]() -> uint32_t {
+                while (m == 0u && q < nq) {
+                    m = s_pmask[q * kPixelSlots + slot];
+                    ++q;
+                }
+                if (m == 0u) return kInvalid;
+                const uint32_t bit = (uint32_t)(__ffs(m) - 1);
+                m &= m - 1u;
+                return (q - 1u) * 32u + bit;
+            };
+            // Coverage and shaded, premultiplied colour of entry bi at this pixel.
+            auto eval = [&](uint32_t bi, float4& v, float& pz) -> bool {
+                const float4 ea = sa[bi], eb = sb[bi];
+                const float ax = ea.x, ay = ea.y, bx = eb.x, by = eb.y;
+                const float rmax = srmax[bi];
+                const bool in_box = !((pcx < wmin(ax, bx) - rmax || pcy < wmin(ay, by) - rmax) ||
+                                      (pcx > wmax(ax, bx) + rmax || pcy > wmax(ay, by) + rmax));
+                const float abx = bx - ax, aby = by - ay;
+                const float t = ((pcx - ax) * abx + (pcy - ay) * aby) * sinv[bi];
+                const float fx = ax + abx * t, fy = ay + aby * t;
+                pz = wmix(ea.z, eb.z, t);
+                const float rr = wmix(srmin[bi], rmax, wclamp(normalize_depth01(pz), 0.0f, 1.0f));
+                const float dx = pcx - fx, dy = pcy - fy;
+                const float d2 = dx * dx + dy * dy;
+                const float cov = wclamp(1.0f - sqrtf(d2) / rr, 0.0f, 1.0f);
+                // perspective_correct_line_t (:149-154)
+                const float aw0 = wmax(fabsf(ea.w), 1e-6f), aw1 = wmax(fabsf(eb.w), 1e-6f);
+                const float tw = (t * aw0) / ((1.0f - t) * aw1 + t * aw0);
+                const float4 c0 = load_half4(reinterpret_cast<const __half*>(&ss0[bi]));
+                const float4 c1 = load_half4(reinterpret_cast<const __half*>(&ss1[bi]));
+                const float sr = wmix(c0.x, c1.x, tw), sg = wmix(c0.y, c1.y, tw);
+                const float sbl = wmix(c0.z, c1.z, tw), sa_ = wmix(c0.w, c1.w, tw);
+                const float alpha = sa_ * cov;
+                const float vsb = svis[bi];
+                v = make_float4(sr * vsb * alpha, sg * vsb * alpha, sbl * vsb * alpha, alpha);
+                return in_box && t >= 0.0f && t <= 1.0f && d2 < rr * rr;
+            };
+            // Entry bi into its worker's part of the current group; false once
+            // the pixel is done (early out at the end of an item).
+            auto land = [&](uint32_t bi, bool covered, const float4& v, float pz) -> bool {
                 const uint32_t tag = s_item[bi];
                 const uint32_t w = tag & 3u;
                 const uint32_t lead = bi - w;
@@ -806,40 +861,32 @@ __global__ void __launch_bounds__(kCamThreads, 14) k_raster(const FrameParams* _
                     const uint32_t item = (tag >> 2) & 0x3FFu;
                     if (pending != kInvalid && item > pending) {
                         end_of_item();
-                        if (done) break;
+                        if (done) return false;
                     }
                     cur_lead = lead;
                     pending = item;
                 }
-                pos = bi + 1u;
-                const float ax = sp0x[bi], ay = sp0y[bi], bx = sp1x[bi], by = sp1y[bi];
-                const float rmax = srmax[bi];
-                const bool in_box = !((pcx < wmin(ax, bx) - rmax || pcy < wmin(ay, by) - rmax) ||
-                                      (pcx > wmax(ax, bx) + rmax || pcy > wmax(ay, by) + rmax));
-                const float abx = bx - ax, aby = by - ay;
-                const float t = ((pcx - ax) * abx + (pcy - ay) * aby) * sinv[bi];
-                const float fx = ax + abx * t, fy = ay + aby * t;
-                const float pz = wmix(sz0[bi], sz1[bi], t);
-                const float rr = wmix(srmin[bi], rmax, wclamp(normalize_depth01(pz), 0.0f, 1.0f));
-                const float dx = pcx - fx, dy = pcy - fy;
-                const float d2 = dx * dx + dy * dy;
-                if (!(in_box && t >= 0.0f && t <= 1.0f && d2 < rr * rr)) continue;
-                const float cov = wclamp(1.0f - sqrtf(d2) / rr, 0.0f, 1.0f);
-                // perspective_correct_line_t (:149-154)
-                const float aw0 = wmax(fabsf(sw0[bi]), 1e-6f), aw1 = wmax(fabsf(sw1[bi]), 1e-6f);
-                const float tw = (t * aw0) / ((1.0f - t) * aw1 + t * aw0);
-                const float4 c0 = load_half4(reinterpret_cast<const __half*>(&ss0[bi]));
-                const float4 c1 = load_half4(reinterpret_cast<const __half*>(&ss1[bi]));
-                const float sr = wmix(c0.x, c1.x, tw), sg = wmix(c0.y, c1.y, tw);
-                const float sbl = wmix(c0.z, c1.z, tw), sa = wmix(c0.w, c1.w, tw);
-                const float alpha = sa * cov;
-                const float vsb = svis[bi];
-                const float4 v = make_float4(sr * vsb * alpha, sg * vsb * alpha, sbl * vsb * alpha, alpha);
-                if (w == 0u) { g0 = v; e0 = pz; }
-                else if (w == 1u) { g1 = v; e1 = pz; }
-                else if (w == 2u) { g2 = v; e2 = pz; }
-                else { g3 = v; e3 = pz; }
-                ++frags;
+                if (covered) {
+                    if (w == 0u) { g0 = v; e0 = pz; }
+                    else if (w == 1u) { g1 = v; e1 = pz; }
+                    else if (w == 2u) { g2 = v; e2 = pz; }
+                    else { g3 = v; e3 = pz; }
+                    ++frags;
+                }
+                return true;
+            };
+            while (!done) {
+                const uint32_t b0 = next();
+                if (b0 == kInvalid) break;
+                const uint32_t b1 = next();
+                const bool two = b1 != kInvalid;
+                const uint32_t c1 = two ? b1 : b0;
+                float4 v0, v1;
+                float z0, z1;
+                const bool h0 = eval(b0, v0, z0);
+                const bool h1 = eval(c1, v1, z1);
+                if (!land(b0, h0, v0, z0) || !two) break;
+                if (!land(c1, h1, v1, z1)) break;
             }
             flush_group();
             // The last item blended into ends in this round unless the round
