@@ -607,11 +607,12 @@ def served_section(args) -> dict:
 def batched_section(args, reps: int = 5) -> dict:
     """The batched configuration: independent views (strands log-uniform in
     [1k, 200k] at 16 or 32 points, 256^2 to 1080p, one light with a 512^2 to
-    2048^2 deep-opacity map) rendered two ways: one multi-view frame whose
-    kernels cover every view (fiber_frame_begin_views, replayed from one
-    graph), and one graph launch of the views' own frames over concurrent
-    branches after the autotuner picked the branch count and view order; the
-    faster is the batch. Compared with the same views as a loop of plain frames
+    2048^2 deep-opacity map) rendered two ways: multi-view frames whose kernels
+    cover every view of the frame (fiber_frame_begin_views, replayed from one
+    graph; the tuner picks 1, 2 or 4 such frames on concurrent streams), and
+    one graph launch of the views' own frames over concurrent branches after
+    the autotuner picked the branch count and view order; the faster is the
+    batch. Compared with the same views as a loop of plain frames
     (per view: frame tables, then its own frame graph). All are timed with CUDA
     events on one stream over `reps` passes, after a warm-up pass, inputs
     resident on the device."""
@@ -653,12 +654,17 @@ def batched_section(args, reps: int = 5) -> dict:
     batch.close()
     for p in plugins:
         p.close()
-    # One multi-view frame: every kernel covers all 64 views.
+    # Multi-view frames: every kernel of a frame covers all of its views; the
+    # tuner times the views as 1, 2 and 4 such frames on concurrent streams.
     t = time.time()
-    merged = batched.MultiViewFrame(specs, packed)
+    group_ms = {}
+    for g in (1, 2, 4):
+        merged = batched.MultiViewGroups(specs, packed, g)
+        group_ms[g] = timed(lambda: merged.launch(stream))
+        merged.close()
     merged_setup_s = time.time() - t
-    merged_ms = timed(lambda: merged.launch(stream))
-    merged.close()
+    groups = min(group_ms, key=group_ms.get)
+    merged_ms = group_ms[groups]
     n = len(specs)
 
     def rates(ms):
@@ -672,7 +678,8 @@ def batched_section(args, reps: int = 5) -> dict:
             "scene_gen_s": gen_s, "setup_s": setup_s, "tune_s": tune_s, "merged_setup_s": merged_setup_s,
             "passes": reps,
             "plain": rates(plain_ms),
-            "multi_view_frame": rates(merged_ms),
+            "multi_view_frame": dict(rates(merged_ms), groups=groups,
+                                     ms_by_groups={str(k): v for k, v in group_ms.items()}),
             "graph_branches": dict(rates(branches_ms), tuning={"branches": int(best.branches),
                                                                "order": "lpt" if best.order else "index",
                                                                "tuned_ms": float(best.ms)}),

@@ -114,6 +114,55 @@ class MultiViewFrame:
         self.plugin.close()
 
 
+def view_cost(spec: ViewSpec, packed: PackedStrandBuffers) -> float:
+    """A view's work estimate for grouping: its segments plus its camera and
+    deep-opacity pixels."""
+    segs = float(np.maximum(packed.meta["count"].astype(np.int64) - 1, 0).sum())
+    return segs + spec.camera_cfg.screen_width * spec.camera_cfg.screen_height + spec.light_cfg.screen_width ** 2
+
+
+def group_views(costs, groups: int) -> list[list[int]]:
+    """Views split into `groups` sets of near-equal cost: longest first, each to
+    the set with the least cost so far; each set keeps increasing view order."""
+    sets = [[] for _ in range(max(1, groups))]
+    load = [0.0] * len(sets)
+    for k in sorted(range(len(costs)), key=lambda i: (-costs[i], i)):
+        j = min(range(len(sets)), key=lambda i: (load[i], i))
+        sets[j].append(k)
+        load[j] += costs[k]
+    return [sorted(g) for g in sets if g]
+
+
+class MultiViewGroups:
+    """The views as `groups` multi-view frames on concurrent streams (one
+    context and one stream each), launched together from `stream`: the work of
+    one group's small launches overlaps another's large ones. groups = 1 is one
+    MultiViewFrame. Each view's image is the one it renders alone."""
+
+    def __init__(self, specs: list[ViewSpec], packed: list[PackedStrandBuffers], groups: int, device: int = 0,
+                 **kw):
+        import torch
+        self.sets = group_views([view_cost(s, p) for s, p in zip(specs, packed)], groups)
+        self.frames = [MultiViewFrame([specs[k] for k in g], [packed[k] for k in g], device, **kw) for g in self.sets]
+        self.streams = [torch.cuda.Stream(device) for _ in self.frames]
+
+    def launch(self, stream):
+        import torch
+        start = torch.cuda.Event()
+        start.record(stream)
+        for f, s in zip(self.frames, self.streams):
+            s.wait_event(start)
+            f.launch(s)
+        for s in self.streams:
+            done = torch.cuda.Event()
+            done.record(s)
+            stream.wait_event(done)
+
+    def close(self):
+        for f in self.frames:
+            f.close()
+
+
 class FiberBatch:
     """fiber_batch over the contexts of `plugins` (which must outlive it)."""
 

@@ -22,6 +22,18 @@ def test_plan_lpt_balances_loads():
     assert a[1] == 0 and a[7] == 1 and a[3] == 2
 
 
+def test_group_views_balances_and_keeps_order():
+    from bevy_strand_rasterizer_b200.batched import group_views
+    costs = [9.0, 1.0, 3.0, 7.0, 5.0, 5.0, 2.0, 8.0]
+    sets = group_views(costs, 3)
+    assert sorted(k for g in sets for k in g) == list(range(8))
+    assert all(g == sorted(g) for g in sets)
+    loads = sorted(sum(costs[k] for k in g) for g in sets)
+    assert loads == [13.0, 13.0, 14.0]
+    assert group_views(costs, 1) == [list(range(8))]
+    assert len(group_views([1.0, 2.0], 4)) == 2  # no empty group
+
+
 def test_plan_rejects_bad_arguments():
     lib = abi.load_library()
     assert lib.fiber_batch_plan(None, 3, 2, 0, None) == abi.EINVAL

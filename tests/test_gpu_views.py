@@ -125,3 +125,35 @@ def test_frame_begin_views_rejects_bad_views():
     with pytest.raises(abi.FiberError):  # and cover the instance table
         p.frame_begin_views([(c0, m0, l0, s0, 0, 1)] * 1 + [(c1, m1, l1, s1, 1, 0)])
     p.close()
+
+
+def test_view_groups_match_one_multi_view_frame():
+    """The views split into two multi-view frames on concurrent streams
+    (batched.MultiViewGroups) render each view as one multi-view frame of all
+    of them does, bit for bit."""
+    import torch
+
+    from bevy_strand_rasterizer_b200 import batched
+    specs = batched.batched_views(6, seed=77, strand_range=(500, 3000))
+    packed = [batched.view_strands(v) for v in specs]
+    stream = torch.cuda.Stream()
+    one = batched.MultiViewFrame(specs, packed)
+    bases = one.launch(stream)
+    stream.synchronize()
+    want = {w: one.plugin.dump(w).copy() for w in (abi.DUMP_COLOR, abi.DUMP_FRAGMENTS)}
+    one.close()
+    two = batched.MultiViewGroups(specs, packed, 2)
+    assert len(two.frames) == 2
+    two.launch(stream)
+    stream.synchronize()
+    for g, f in zip(two.sets, two.frames):
+        gb = f.launch(stream)
+        stream.synchronize()
+        color, frags = f.plugin.dump(abi.DUMP_COLOR), f.plugin.dump(abi.DUMP_FRAGMENTS)
+        for j, k in enumerate(g):
+            n = specs[k].camera_cfg.screen_width * specs[k].camera_cfg.screen_height
+            a, b = bases[k], gb[j]
+            assert np.array_equal(color[4 * b: 4 * (b + n)].view(np.uint16),
+                                  want[abi.DUMP_COLOR][4 * a: 4 * (a + n)].view(np.uint16)), f"view {k}"
+            assert np.array_equal(frags[b: b + n], want[abi.DUMP_FRAGMENTS][a: a + n]), f"view {k}"
+    two.close()
