@@ -7,12 +7,12 @@
 // 64 slots; its 4 depth workers per pixel become the order in which one
 // thread applies the same operations). Blocks claim runs from a counter. The
 // run's references are staged into shared memory a round at a time
-// (per-reference projection, radii, shading texels); a round holds whole work
-// items, or one CAP-sized chunk of an item longer than CAP (CAP is a multiple
-// of 16, so the reference's groups of 4 never straddle a round). Each round
-// also builds per-pixel coverage-candidate bits from a conservative band
-// test, and each pixel walks only its candidates. Block barriers happen only
-// between rounds. The blend order is the reference's: work items near to far,
+// (per-reference projection, radii, shading texels, by asynchronous copies);
+// a round holds whole work items, or one CAP-sized chunk of an item longer
+// than CAP (CAP is a multiple of 16, so the reference's groups of 4 never
+// straddle a round). Each round also builds per-pixel coverage-candidate bits
+// from a conservative band test, and each pixel walks only its candidates,
+// two at a time. Block barriers happen only between rounds. The blend order is the reference's: work items near to far,
 // references in groups of 4 from each item's start, (w0 over w1) over (w2 over
 // w3), early out after each item once alpha > 0.98.
 #include "fiber_kernels.cuh"
@@ -648,12 +648,14 @@ void launch_dom_paging(const LaunchCtx& L, const RenderArgs& R, uint32_t table_e
 // K19 camera colour raster.
 //
 // One 64-thread block per camera tile run, one thread per pixel. Each pixel
-// walks, in order, the groups of 4 (an item's entries 4g .. 4g+3 from the item
-// start) that hold a coverage candidate for it, and blends each group as the
-// reference's four workers do: (w0 over w1) over (w2 over w3), then final over
-// group, the same float operations in the same order, computed in one thread.
-// A group without a candidate contributes transparent black and depth 0,
-// which leaves the blend unchanged, so skipping it keeps the result.
+// walks its candidate entries in order, one entry (two per step) at a time;
+// an entry lands in its worker's part of its group of 4 (an item's entries
+// 4g .. 4g+3 from the item start), and a group is blended when the walk
+// reaches the next one, as the reference's four workers do: (w0 over w1) over
+// (w2 over w3), then final over group, the same float operations in the same
+// order, computed in one thread. A group without a candidate contributes
+// transparent black and depth 0, which leaves the blend unchanged, so skipping
+// it keeps the result.
 // ===========================================================================
 constexpr uint32_t kCamThreads = 64;  // = kPixelSlots
 constexpr uint32_t kCamCap = 128;
