@@ -111,18 +111,19 @@ __device__ __forceinline__ float gaussian_detector(const Detector& g, float phi_
         float m = phi_delta - two_pi * truncf(phi_delta / two_pi);
         return fabsf(m) < 1e-3f ? 0.0f : 1e6f;
     }
-    // Three nearest terms: with k_c the nearest wrap (|phi - 2 pi k_c| <= pi),
-    // every other k has |phi - 2 pi k| >= 3 pi, so its term is below
-    // exp(-9 pi^2 / (2 var)) < 2.3e-10 for var < 2; the at most 18 such terms
-    // change the detector by less than 4.2e-9 norm, far inside the shading
-    // tolerance. Summed in increasing k, as the full loop does.
-    // With var < 0.26 every term but the nearest is below exp(-pi^2 / (2 var))
-    // < 5.8e-9 (|phi - 2 pi k| >= pi), and the 20 of them change the detector
-    // by less than 1.2e-8 norm: the nearest term alone is summed.
+    // Let k_c be the wrap nearest to phi (|phi - 2 pi k_c| <= pi; |phi| < 56
+    // keeps k_c +- 1 inside k = -10..10). Nearest term alone: with var < 0.26
+    // every other term is below exp(-pi^2 / (2 var)) < 5.8e-9 (|phi - 2 pi k|
+    // >= pi), and the 20 of them change the detector by less than 1.2e-8 norm.
     if (g.near1 && fabsf(phi_delta) < 56.0f) {
         const float a = phi_delta - (2.0f * kPi) * rintf(phi_delta * (1.0f / (2.0f * kPi)));
         return g.norm * __expf((a * a) * g.neg_inv_two_var);
     }
+    // Three nearest terms: every k other than k_c and k_c +- 1 has
+    // |phi - 2 pi k| >= 3 pi, so its term is below exp(-9 pi^2 / (2 var)) <
+    // 2.3e-10 for var < 2; the at most 18 such terms change the detector by
+    // less than 4.2e-9 norm, far inside the shading tolerance. Summed in
+    // increasing k, as the full loop does.
     if (g.near3 && fabsf(phi_delta) < 56.0f) {
         const float two_pi = 2.0f * kPi;
         const float kc = rintf(phi_delta * (1.0f / two_pi));
